@@ -1,0 +1,261 @@
+/*
+ * rvsb.h - C ABI of the B200 backend for the RVS per-frame view-synthesis path.
+ *
+ * The reference (RVS, the MPEG Reference View Synthesizer, with its CUDA fork)
+ * synthesises one virtual view per frame in Pipeline::computeView
+ * (rvs/src/Pipeline.cpp:169-345).  For each input view it calls
+ * SynthesizedView::compute (rvs/src/SynthesizedView.cpp:374-380: unproject,
+ * R*x+t, project, triangle raster), then BlendedView::blend
+ * (rvs/src/BlendedView.cpp:256-262), and after the last view the inpainter
+ * (rvs/src/inpainting.cpp:213-235) and the YUV420 writer
+ * (rvs/src/image_writing.cpp:182-225).  The CUDA fork exposes the same steps
+ * as C++ free functions with OpenCV types (the .cuh headers under rvs_cuda_lib/src).
+ *
+ * This header replaces both layers with plain C: cameras are plain structs,
+ * images are raw plane pointers plus the sizes in the camera struct, streams
+ * are passed as void* (a cudaStream_t), and errors are status codes instead
+ * of exceptions.  Each entry point names the reference interface it replaces.
+ *
+ * Threading: a context may be used from one host thread at a time; scenes
+ * and servers created from it share its device.  All device work is issued on
+ * the stream passed in (NULL = the legacy default stream).
+ */
+#ifndef RVSB_H
+#define RVSB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RVSB_ABI_VERSION 1
+
+/* Status codes.  The reference throws std::runtime_error / std::logic_error
+ * (e.g. rvs_cuda_lib/src/transform_triangle.cu:376-379,
+ * rvs/src/Parameters.cpp:330-339) and its call sites print and continue
+ * (rvs/src/SynthesizedView.cpp:461-464); here every failure is returned. */
+typedef enum rvsb_status {
+    RVSB_OK = 0,
+    RVSB_E_ARG = 1,          /* null pointer, size or index out of range */
+    RVSB_E_CONFIG = 2,       /* JSON / camera parameters rejected */
+    RVSB_E_IO = 3,           /* file missing or shorter than one frame */
+    RVSB_E_OOM_BUDGET = 4,   /* request does not fit the HBM budget */
+    RVSB_E_CUDA = 5,         /* CUDA runtime error */
+    RVSB_E_TIMEOUT = 6,      /* a bounded wait expired */
+    RVSB_E_UNSUPPORTED = 7,  /* a reference option this build does not take */
+    RVSB_E_BUSY = 8,         /* queue full */
+    RVSB_E_NOT_FOUND = 9     /* unknown ticket / camera name */
+} rvsb_status;
+
+typedef enum rvsb_projection {
+    RVSB_PROJ_PERSPECTIVE = 0,      /* "Perspective" */
+    RVSB_PROJ_EQUIRECTANGULAR = 1   /* "Equirectangular" */
+} rvsb_projection;
+
+typedef enum rvsb_color_format {
+    RVSB_FMT_YUV420 = 0,            /* "YUV420" */
+    RVSB_FMT_YUV400 = 1             /* "YUV400" (depth only) */
+} rvsb_color_format;
+
+/* One camera of an RVS camera-parameter file.  Field meanings follow
+ * Parameters::readFrom (rvs/src/Parameters.cpp:104-129) and the setters at
+ * rvs/src/Parameters.cpp:316-463.  Crop_region is not supported (the crop
+ * equals the full resolution). */
+typedef struct rvsb_camera {
+    int32_t projection;          /* rvsb_projection ("Projection") */
+    int32_t width;               /* "Resolution"[0] */
+    int32_t height;              /* "Resolution"[1] */
+    int32_t bit_depth_color;     /* "BitDepthColor" (1..16) */
+    int32_t bit_depth_depth;     /* "BitDepthDepth" (1..16) */
+    int32_t depth_color_format;  /* rvsb_color_format ("DepthColorSpace") */
+    int32_t has_invalid_depth;   /* "HasInvalidDepth", default 1 */
+    int32_t full_hor_range;      /* "Hor_range" equals [-180, 180] as integers */
+    float position[3];           /* "Position" (x forward, y left, z up) */
+    float rotation[3];           /* "Rotation": yaw, pitch, roll in degrees */
+    float depth_range[2];        /* "Depth_range": near, far (far >= 1000 = infinity) */
+    float focal[2];              /* "Focal" (perspective) */
+    float principle_point[2];    /* "Principle_point" (perspective) */
+    float hor_range[2];          /* "Hor_range" in degrees (equirectangular) */
+    float ver_range[2];          /* "Ver_range" in degrees (equirectangular) */
+} rvsb_camera;
+
+/* Raw planes of one input view, as stored in the reference's .yuv files
+ * (read_color_YUV / read_depth_YUV, rvs/src/image_loading.cpp:74-211):
+ * samples are little-endian uint16 for bit depths 9..16.
+ *   y:     width*height colour luma samples
+ *   u, v:  (width/2)*(height/2) chroma samples each
+ *   depth: width*height samples of the depth map's luma plane */
+typedef struct rvsb_view_planes {
+    const uint16_t* y;
+    const uint16_t* u;
+    const uint16_t* v;
+    const uint16_t* depth;
+} rvsb_view_planes;
+
+/* YUV420 output planes (write_color, rvs/src/image_writing.cpp:182-225):
+ * y: width*height, u and v: (width/2)*(height/2) uint16 samples each. */
+typedef struct rvsb_yuv420 {
+    uint16_t* y;
+    uint16_t* u;
+    uint16_t* v;
+} rvsb_yuv420;
+
+/* Synthesis options (Config, rvs/src/Config.hpp:172-205). */
+typedef struct rvsb_synth_params {
+    float blending_factor;    /* "BlendingFactor" (default 5); must be > 0 */
+    float precision;          /* "Precision"; only 1 is supported */
+    int32_t reserved[2];
+} rvsb_synth_params;
+
+/* ----------------------------------------------------------------------- */
+/* Context                                                                  */
+/* ----------------------------------------------------------------------- */
+
+typedef struct rvsb_context rvsb_context;
+
+/* Creates a context on CUDA device `device`.  `hbm_budget_bytes` caps the
+ * device memory the context's scenes and work buffers may hold (0 = 60 GB).
+ * Replaces the per-call cudaMalloc/cudaFree of the reference wrappers
+ * (e.g. rvs_cuda_lib/src/transform_triangle.cu:327-380) with arenas owned
+ * by the context. */
+rvsb_status rvsb_create(int device, size_t hbm_budget_bytes, rvsb_context** out);
+void rvsb_destroy(rvsb_context* ctx);
+
+/* Last error message of the context (never NULL). */
+const char* rvsb_last_error(const rvsb_context* ctx);
+const char* rvsb_status_string(rvsb_status status);
+
+/* Bytes of device memory currently held by the context. */
+size_t rvsb_memory_in_use(const rvsb_context* ctx);
+
+/* ----------------------------------------------------------------------- */
+/* Front end: RVS JSON, camera JSON, pose trace                             */
+/* ----------------------------------------------------------------------- */
+
+/* Parses one camera object of a camera-parameter file (JSON text of the
+ * object itself).  Replaces Parameters::readFrom
+ * (rvs/src/Parameters.cpp:104-129) including its validation
+ * (Depth_range order and far <= 1000, Depthmap == 1, ColorSpace YUV420).
+ * On failure returns RVSB_E_CONFIG and writes a message into err. */
+rvsb_status rvsb_camera_from_json(const char* json_object_text, rvsb_camera* out,
+                                  char* err, size_t err_len);
+
+typedef struct rvsb_config rvsb_config;
+
+/* Loads an RVS configuration file and the camera files it names.  Replaces
+ * Config::loadFromFile (rvs/src/Config.cpp:72-120) with
+ * loadCamerasParametersFromFile (rvs/src/Config.cpp:122-175), the
+ * InputOverrides/VirtualOverrides rule (rvs/src/JsonParser.cpp:199-219) and
+ * the pose trace (rvs/src/PoseTraces.cpp:54-109).  Relative paths are
+ * resolved against the working directory, as the reference does. */
+rvsb_status rvsb_config_load(const char* rvs_json_path, rvsb_config** out,
+                             char* err, size_t err_len);
+void rvsb_config_free(rvsb_config* cfg);
+
+int rvsb_config_num_inputs(const rvsb_config* cfg);
+int rvsb_config_num_virtual(const rvsb_config* cfg);
+rvsb_status rvsb_config_input_camera(const rvsb_config* cfg, int i, rvsb_camera* out);
+rvsb_status rvsb_config_virtual_camera(const rvsb_config* cfg, int i, rvsb_camera* out);
+/* Texture and depth file paths of input i; output path of virtual view i. */
+const char* rvsb_config_texture_path(const rvsb_config* cfg, int i);
+const char* rvsb_config_depth_path(const rvsb_config* cfg, int i);
+const char* rvsb_config_output_path(const rvsb_config* cfg, int i);
+/* StartFrame, NumberOfFrames, NumberOfOutputFrames, BlendingFactor, Precision. */
+void rvsb_config_frames(const rvsb_config* cfg, int* start_frame, int* number_of_frames,
+                        int* number_of_output_frames);
+void rvsb_config_synth_params(const rvsb_config* cfg, rvsb_synth_params* out);
+/* Virtual camera i for output frame `frame` after applying the pose trace
+ * the way Pipeline::computeView does (rvs/src/Pipeline.cpp:173-181:
+ * position += trace position, rotation = trace rotation). */
+rvsb_status rvsb_config_virtual_camera_at(const rvsb_config* cfg, int i, int frame, rvsb_camera* out);
+
+/* Relative pose of an input camera seen from the virtual camera:
+ * R = R_virt^T * R_in, t = -R_virt^T * (t_virt - t_in), in float with the
+ * reference's operation order.  Replaces SpaceTransformer::get_rotation /
+ * get_translation (rvs/src/SpaceTransformer.cpp:77-92) and
+ * Parameters::getRotationMatrix (rvs/src/Parameters.cpp:151-155). */
+rvsb_status rvsb_relative_pose(const rvsb_camera* input, const rvsb_camera* virt,
+                               float R[9], float t[3]);
+
+/* ----------------------------------------------------------------------- */
+/* Scenes: input views resident in device memory                           */
+/* ----------------------------------------------------------------------- */
+
+typedef struct rvsb_scene rvsb_scene;
+
+/* Creates a scene of n_inputs input cameras (the InputCameraNames order,
+ * which is also the blend order, rvs/src/Pipeline.cpp:202-266) and reserves
+ * device memory for their raw planes under the context's HBM budget. */
+rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs,
+                              rvsb_scene** out);
+void rvsb_scene_destroy(rvsb_scene* scene);
+
+/* Uploads (host pointers, planes_on_device = 0) or copies (device pointers,
+ * planes_on_device = 1) the raw planes of input view `view` into the scene.
+ * Replaces InputView::load -> read_color / read_depth and their loader
+ * kernels (rvs/src/View.cpp:233-257, rvs/src/image_loading.cpp:74-211,
+ * rvs_cuda_lib/src/process_input_frame.cu:95-467); the decode itself is
+ * fused into the synthesis kernels. */
+rvsb_status rvsb_scene_upload(rvsb_scene* scene, int view, const rvsb_view_planes* planes,
+                              int planes_on_device, void* stream);
+
+/* ----------------------------------------------------------------------- */
+/* Synthesis                                                                */
+/* ----------------------------------------------------------------------- */
+
+/* Synthesises the virtual camera `virt` from all views of `scene` into the
+ * device planes `out` (YUV420, virt->bit_depth_color bits in uint16).
+ * Replaces one pass of Pipeline::computeView (rvs/src/Pipeline.cpp:169-298):
+ * SynthesizedView::compute + BlendedView::blend per input view, inpainting,
+ * then the quantisation of write_color.  Asynchronous on `stream`. */
+rvsb_status rvsb_synthesize(rvsb_scene* scene, const rvsb_camera* virt,
+                            const rvsb_synth_params* params, const rvsb_yuv420* out,
+                            void* stream);
+
+/* The same call with host buffers on both sides (the reference's plain
+ * per-frame path): uploads the n raw input views from host memory,
+ * synthesises, and copies the YUV420 result back into host memory.  Blocks
+ * until the result is in `out_host`. */
+rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs,
+                                 const rvsb_view_planes* host_planes, const rvsb_camera* virt,
+                                 const rvsb_synth_params* params, const rvsb_yuv420* out_host,
+                                 void* stream);
+
+/* Intermediate results of one synthesis, for stage-by-stage checks against
+ * the reference's CPU path.  Every pointer is a device pointer and may be
+ * NULL; n = number of input views, W,H = input size, Wo,Ho = output size.
+ *   warped_uvz:    n*H*W*4 floats, (u, v, virtual depth, 0) per input pixel
+ *                  (SynthesizedView::computeBasicMode, SynthesizedView.cpp:320-331)
+ *   view_color:    n*Ho*Wo*3 floats, raster colour of each view
+ *   view_depth:    n*Ho*Wo floats (+inf where uncovered)
+ *   view_validity: n*Ho*Wo floats (triangle quality, 0 where uncovered)
+ *                  (transform_trianglesMethod, rvs/src/transform.cpp:148-181)
+ *   blend_color:   Ho*Wo*3 floats, blended colour before inpainting
+ *   blend_quality: Ho*Wo floats, blended quality (BlendedView.cpp:180-212)
+ *   inpaint_source: Ho*Wo int32 pairs (x, y) of the pixel each hole copies
+ *                  (compute_nearest, rvs/src/inpainting.cpp:104-136) */
+typedef struct rvsb_debug_out {
+    float* warped_uvz;
+    float* view_color;
+    float* view_depth;
+    float* view_validity;
+    float* blend_color;
+    float* blend_quality;
+    int32_t* inpaint_source;
+} rvsb_debug_out;
+
+rvsb_status rvsb_synthesize_debug(rvsb_scene* scene, const rvsb_camera* virt,
+                                  const rvsb_synth_params* params, const rvsb_yuv420* out,
+                                  const rvsb_debug_out* dbg, void* stream);
+
+/* Kernel launches issued by the most recent synthesis call of the scene
+ * (for launch accounting). */
+int rvsb_scene_last_launch_count(const rvsb_scene* scene);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RVSB_H */

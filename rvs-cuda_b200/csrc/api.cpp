@@ -1,0 +1,608 @@
+// C ABI of the B200 synthesis backend (include/rvsb.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "camera.hpp"
+#include "frontend.hpp"
+#include "kernels.hpp"
+#include "rvsb.h"
+
+using namespace rvsb;
+
+struct rvsb_context {
+    int device = 0;
+    size_t budget = 0;
+    size_t in_use = 0;
+    std::string last_error;
+    std::mutex mu;
+    rvsb_scene* host_scene = nullptr;  // scene reused by rvsb_synthesize_host
+    void* host_out = nullptr;          // device output staging of rvsb_synthesize_host
+    size_t host_out_bytes = 0;
+};
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct BudgetError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ArgError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Device allocation counted against the context's HBM budget.
+struct DevMem {
+    rvsb_context* ctx = nullptr;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    ~DevMem() { release(); }
+
+    void alloc(rvsb_context* c, size_t n) {
+        release();
+        if (n == 0) n = 16;
+        if (c->in_use + n > c->budget)
+            throw BudgetError("request of " + std::to_string(n) + " bytes exceeds the HBM budget (" +
+                              std::to_string(c->in_use) + " of " + std::to_string(c->budget) + " in use)");
+        check(cudaMalloc(&ptr, n), "cudaMalloc");
+        ctx = c;
+        bytes = n;
+        c->in_use += n;
+    }
+    void release() {
+        if (ptr) {
+            cudaFree(ptr);
+            ctx->in_use -= bytes;
+        }
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+struct Workspace {
+    int wo = 0, ho = 0;
+    DevMem views, target, status, counts, offsets, cursor, list, codes, scan[4], vert, bbox;
+    SynthBuffers b;
+    LaunchShape shape{};
+    std::vector<DevView> host_views;
+    std::vector<int64_t> vert_off, bbox_off;
+};
+
+}  // namespace
+
+struct rvsb_scene {
+    rvsb_context* ctx = nullptr;
+    std::vector<rvsb_camera> cams;
+    std::vector<std::unique_ptr<DevMem>> planes;  // 4 per view: y, u, v, depth
+    std::vector<std::unique_ptr<DevMem>> erp;     // 2 per view: rows, cols (ERP inputs)
+    std::vector<bool> uploaded;
+    std::unique_ptr<Workspace> ws;
+    int last_launches = 0;
+};
+
+namespace {
+
+rvsb_status fail(rvsb_context* ctx, rvsb_status s, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return s;
+}
+
+template <class F>
+rvsb_status guarded(rvsb_context* ctx, F&& f) {
+    try {
+        return f();
+    } catch (const ArgError& e) {
+        return fail(ctx, RVSB_E_ARG, e.what());
+    } catch (const ConfigError& e) {
+        return fail(ctx, RVSB_E_CONFIG, e.what());
+    } catch (const Unsupported& e) {
+        return fail(ctx, RVSB_E_UNSUPPORTED, e.what());
+    } catch (const IoError& e) {
+        return fail(ctx, RVSB_E_IO, e.what());
+    } catch (const BudgetError& e) {
+        return fail(ctx, RVSB_E_OOM_BUDGET, e.what());
+    } catch (const CudaError& e) {
+        return fail(ctx, RVSB_E_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, RVSB_E_OOM_BUDGET, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(ctx, RVSB_E_ARG, e.what());
+    }
+}
+
+size_t plane_bytes(const rvsb_camera& c, int k) {
+    const size_t n = (size_t)c.width * c.height;
+    return (k == 1 || k == 2) ? (size_t)(c.width / 2) * (c.height / 2) * 2 : n * 2;
+}
+
+int nblocks_x(int w) { return (w - 1 + BLOCK_W - 1) / BLOCK_W; }
+int nblocks_y(int h) { return (h - 1 + BLOCK_H - 1) / BLOCK_H; }
+
+void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
+    if (sc->ws && sc->ws->wo == wo && sc->ws->ho == ho) return;
+    sc->ws.reset();
+    auto ws = std::make_unique<Workspace>();
+    rvsb_context* ctx = sc->ctx;
+    const int n = (int)sc->cams.size();
+    ws->wo = wo;
+    ws->ho = ho;
+    int64_t nvert = 0, nbb = 0;
+    int max_w = 0, max_h = 0, max_blocks = 0;
+    for (const auto& c : sc->cams) {
+        ws->vert_off.push_back(nvert);
+        ws->bbox_off.push_back(nbb);
+        nvert += (int64_t)c.width * c.height;
+        const int nb = nblocks_x(c.width) * nblocks_y(c.height);
+        nbb += nb;
+        max_w = std::max(max_w, c.width);
+        max_h = std::max(max_h, c.height);
+        max_blocks = std::max(max_blocks, nb);
+    }
+    const int ntx = (wo + TILE - 1) / TILE, nty = (ho + TILE - 1) / TILE;
+    const size_t nbins = (size_t)ntx * nty * n;
+    const int capacity = (int)std::min<int64_t>(INT32_MAX / 2, std::max<int64_t>(1 << 16, nbb * 8 + nbins));
+    ws->vert.alloc(ctx, (size_t)nvert * sizeof(float4));
+    ws->bbox.alloc(ctx, (size_t)nbb * sizeof(int4));
+    ws->views.alloc(ctx, sizeof(DevView) * n);
+    ws->target.alloc(ctx, sizeof(DevTarget));
+    ws->status.alloc(ctx, sizeof(DevStatus));
+    ws->counts.alloc(ctx, nbins * sizeof(int));
+    ws->offsets.alloc(ctx, nbins * sizeof(int));
+    ws->cursor.alloc(ctx, nbins * sizeof(int));
+    ws->list.alloc(ctx, (size_t)capacity * sizeof(int));
+    const size_t npix = (size_t)wo * ho;
+    ws->codes.alloc(ctx, npix * sizeof(uint64_t));
+    for (auto& s : ws->scan) s.alloc(ctx, npix * sizeof(uint64_t));
+    SynthBuffers& b = ws->b;
+    b.views = ws->views.as<DevView>();
+    b.target = ws->target.as<DevTarget>();
+    b.status = ws->status.as<DevStatus>();
+    b.counts = ws->counts.as<int>();
+    b.offsets = ws->offsets.as<int>();
+    b.cursor = ws->cursor.as<int>();
+    b.list = ws->list.as<int>();
+    b.capacity = capacity;
+    b.codes = ws->codes.as<uint64_t>();
+    b.scan_a = ws->scan[0].as<uint64_t>();
+    b.scan_b = ws->scan[1].as<uint64_t>();
+    b.scan_c = ws->scan[2].as<uint64_t>();
+    b.scan_d = ws->scan[3].as<uint64_t>();
+    LaunchShape& sh = ws->shape;
+    sh.n_views = n;
+    sh.max_w = max_w;
+    sh.max_h = max_h;
+    sh.max_blocks = max_blocks;
+    sh.wo = wo;
+    sh.ho = ho;
+    sh.ntx = ntx;
+    sh.nty = nty;
+    for (int v = 0; v < n && v < 64; ++v) {
+        sh.input_w[v] = sc->cams[v].width;
+        sh.input_h[v] = sc->cams[v].height;
+        sh.vert_offset[v] = ws->vert_off[v];
+    }
+    ws->host_views.resize(n);
+    sc->ws = std::move(ws);
+}
+
+void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_params& p, DevTarget& T) {
+    Workspace& ws = *sc->ws;
+    const int n = (int)sc->cams.size();
+    for (int v = 0; v < n; ++v) {
+        const rvsb_camera& c = sc->cams[v];
+        DevView& V = ws.host_views[v];
+        std::memset(&V, 0, sizeof(V));
+        V.w = c.width;
+        V.h = c.height;
+        V.proj = c.projection;
+        V.bits_color = c.bit_depth_color;
+        V.f0 = c.focal[0];
+        V.f1 = c.focal[1];
+        V.p0 = c.principle_point[0];
+        V.p1 = c.principle_point[1];
+        V.near_ = c.depth_range[0];
+        V.far_ = c.depth_range[1];
+        V.depth_scale = 1.0f / (float)((1u << c.bit_depth_depth) - 1u);
+        V.has_invalid = c.has_invalid_depth;
+        V.color_scale = 1.0f / (float)((1u << c.bit_depth_color) - 1u);
+        V.cw = c.width / 2;
+        V.ch = c.height / 2;
+        V.chroma_sx = (float)V.cw / c.width;
+        V.chroma_sy = (float)V.ch / c.height;
+        relative_pose(c, virt, V.R, V.t);
+        V.py = sc->planes[v * 4 + 0]->as<uint16_t>();
+        V.pu = sc->planes[v * 4 + 1]->as<uint16_t>();
+        V.pv = sc->planes[v * 4 + 2]->as<uint16_t>();
+        V.pd = sc->planes[v * 4 + 3]->as<uint16_t>();
+        if (c.projection == RVSB_PROJ_EQUIRECTANGULAR) {
+            V.erp_row = sc->erp[v * 2 + 0]->as<float>();
+            V.erp_col = sc->erp[v * 2 + 1]->as<float>();
+        }
+        V.vert = ws.vert.as<float4>() + ws.vert_off[v];
+        V.bbox = ws.bbox.as<int4>() + ws.bbox_off[v];
+        V.nbx = nblocks_x(c.width);
+        V.nby = nblocks_y(c.height);
+    }
+    std::memset(&T, 0, sizeof(T));
+    T.wo = virt.width;
+    T.ho = virt.height;
+    T.proj = virt.projection;
+    T.wrap = (virt.projection == RVSB_PROJ_EQUIRECTANGULAR && virt.full_hor_range) ? 1 : 0;
+    T.f0 = virt.focal[0];
+    T.f1 = virt.focal[1];
+    T.p0 = virt.principle_point[0];
+    T.p1 = virt.principle_point[1];
+    if (virt.projection == RVSB_PROJ_EQUIRECTANGULAR) erp_projector_constants(virt, T.u0, T.v0, T.du_dphi, T.dv_dtheta);
+    T.bits = virt.bit_depth_color;
+    T.max_val = (1u << virt.bit_depth_color) - 1u;
+    T.blend_exp = p.blending_factor;
+    T.inv_blend_exp = 1.0f / p.blending_factor;
+    T.ntx = ws.shape.ntx;
+    T.nty = ws.shape.nty;
+    T.n_views = n;
+    T.bin_capacity = ws.b.capacity;
+}
+
+void validate_params(const rvsb_synth_params* p) {
+    if (!p) throw ArgError("null synthesis parameters");
+    if (!(p->blending_factor > 0.f) || !std::isfinite(p->blending_factor))
+        throw Unsupported("BlendingFactor must be a positive finite number");
+    if (p->precision != 1.f) throw Unsupported("Precision other than 1 is not supported");
+}
+
+rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_synth_params* params,
+                            const rvsb_yuv420* out, const rvsb_debug_out* dbg_out, void* stream) {
+    if (!sc) return RVSB_E_ARG;
+    rvsb_context* ctx = sc->ctx;
+    return guarded(ctx, [&]() -> rvsb_status {
+        if (!virt || !out || !out->y || !out->u || !out->v) throw ArgError("null camera or output planes");
+        validate_params(params);
+        if (const char* why = camera_problem(*virt, true)) throw ArgError(std::string("virtual camera: ") + why);
+        for (size_t v = 0; v < sc->cams.size(); ++v)
+            if (!sc->uploaded[v]) throw ArgError("input view " + std::to_string(v) + " was not uploaded");
+        check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        ensure_workspace(sc, virt->width, virt->height);
+        Workspace& ws = *sc->ws;
+        DevTarget T;
+        fill_tables(sc, *virt, *params, T);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check(cudaMemcpyAsync(ws.b.views, ws.host_views.data(), sizeof(DevView) * ws.host_views.size(),
+                              cudaMemcpyHostToDevice, s),
+              "upload view table");
+        check(cudaMemcpyAsync(ws.b.target, &T, sizeof(T), cudaMemcpyHostToDevice, s), "upload target");
+        DebugPtrs dbg;
+        if (dbg_out) {
+            dbg.warped_uvz = dbg_out->warped_uvz;
+            dbg.view_color = dbg_out->view_color;
+            dbg.view_depth = dbg_out->view_depth;
+            dbg.view_validity = dbg_out->view_validity;
+            dbg.blend_color = dbg_out->blend_color;
+            dbg.blend_quality = dbg_out->blend_quality;
+            dbg.inpaint_source = dbg_out->inpaint_source;
+        }
+        int launches = launch_synthesis(ws.b, ws.shape, dbg, out->y, out->u, out->v, s);
+        if (launches < 0) check(cudaGetLastError(), "kernel launch");
+        if (dbg.warped_uvz) {
+            size_t off = 0;
+            for (size_t v = 0; v < sc->cams.size(); ++v) {
+                const size_t nv = (size_t)sc->cams[v].width * sc->cams[v].height;
+                check(cudaMemcpyAsync(dbg.warped_uvz + off * 4, ws.vert.as<float4>() + ws.vert_off[v],
+                                      nv * sizeof(float4), cudaMemcpyDeviceToDevice, s),
+                      "copy warped vertices");
+                off += nv;
+            }
+        }
+        sc->last_launches = launches;
+        return RVSB_OK;
+    });
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rvsb_status_string(rvsb_status s) {
+    switch (s) {
+        case RVSB_OK: return "ok";
+        case RVSB_E_ARG: return "invalid argument";
+        case RVSB_E_CONFIG: return "configuration rejected";
+        case RVSB_E_IO: return "i/o error";
+        case RVSB_E_OOM_BUDGET: return "HBM budget exceeded";
+        case RVSB_E_CUDA: return "CUDA error";
+        case RVSB_E_TIMEOUT: return "timeout";
+        case RVSB_E_UNSUPPORTED: return "unsupported option";
+        case RVSB_E_BUSY: return "busy";
+        case RVSB_E_NOT_FOUND: return "not found";
+    }
+    return "unknown status";
+}
+
+rvsb_status rvsb_create(int device, size_t hbm_budget_bytes, rvsb_context** out) {
+    if (!out) return RVSB_E_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return RVSB_E_CUDA;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return RVSB_E_CUDA;
+    auto* ctx = new (std::nothrow) rvsb_context;
+    if (!ctx) return RVSB_E_OOM_BUDGET;
+    ctx->device = device;
+    ctx->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)60 << 30;
+    *out = ctx;
+    return RVSB_OK;
+}
+
+void rvsb_destroy(rvsb_context* ctx) {
+    if (!ctx) return;
+    if (ctx->host_scene) rvsb_scene_destroy(ctx->host_scene);
+    if (ctx->host_out) {
+        cudaSetDevice(ctx->device);
+        cudaFree(ctx->host_out);
+    }
+    delete ctx;
+}
+
+const char* rvsb_last_error(const rvsb_context* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+size_t rvsb_memory_in_use(const rvsb_context* ctx) { return ctx ? ctx->in_use : 0; }
+
+rvsb_status rvsb_relative_pose(const rvsb_camera* input, const rvsb_camera* virt, float R[9], float t[3]) {
+    if (!input || !virt || !R || !t) return RVSB_E_ARG;
+    relative_pose(*input, *virt, R, t);
+    return RVSB_OK;
+}
+
+rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs, rvsb_scene** out) {
+    if (!ctx || !inputs || !out || n_inputs <= 0 || n_inputs > 64) return RVSB_E_ARG;
+    *out = nullptr;
+    return guarded(ctx, [&]() -> rvsb_status {
+        check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        auto sc = std::make_unique<rvsb_scene>();
+        sc->ctx = ctx;
+        for (int v = 0; v < n_inputs; ++v) {
+            if (const char* why = camera_problem(inputs[v], false))
+                throw ArgError("input camera " + std::to_string(v) + ": " + why);
+            sc->cams.push_back(inputs[v]);
+        }
+        for (int v = 0; v < n_inputs; ++v) {
+            for (int k = 0; k < 4; ++k) {
+                auto m = std::make_unique<DevMem>();
+                m->alloc(ctx, plane_bytes(inputs[v], k));
+                sc->planes.push_back(std::move(m));
+            }
+            auto r = std::make_unique<DevMem>();
+            auto c = std::make_unique<DevMem>();
+            if (inputs[v].projection == RVSB_PROJ_EQUIRECTANGULAR) {
+                std::vector<float> rows, cols;
+                erp_tables(inputs[v], rows, cols);
+                r->alloc(ctx, rows.size() * sizeof(float));
+                c->alloc(ctx, cols.size() * sizeof(float));
+                check(cudaMemcpy(r->ptr, rows.data(), rows.size() * sizeof(float), cudaMemcpyHostToDevice),
+                      "upload ERP rows");
+                check(cudaMemcpy(c->ptr, cols.data(), cols.size() * sizeof(float), cudaMemcpyHostToDevice),
+                      "upload ERP columns");
+            }
+            sc->erp.push_back(std::move(r));
+            sc->erp.push_back(std::move(c));
+        }
+        sc->uploaded.assign(n_inputs, false);
+        *out = sc.release();
+        return RVSB_OK;
+    });
+}
+
+void rvsb_scene_destroy(rvsb_scene* scene) {
+    if (!scene) return;
+    cudaSetDevice(scene->ctx->device);
+    cudaDeviceSynchronize();
+    delete scene;
+}
+
+rvsb_status rvsb_scene_upload(rvsb_scene* sc, int view, const rvsb_view_planes* planes, int planes_on_device,
+                              void* stream) {
+    if (!sc) return RVSB_E_ARG;
+    return guarded(sc->ctx, [&]() -> rvsb_status {
+        if (!planes || view < 0 || view >= (int)sc->cams.size()) throw ArgError("bad view index or planes");
+        const void* src[4] = {planes->y, planes->u, planes->v, planes->depth};
+        for (int k = 0; k < 4; ++k)
+            if (!src[k]) throw ArgError("null plane");
+        check(cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const rvsb_camera& c = sc->cams[view];
+        for (int k = 0; k < 4; ++k)
+            check(cudaMemcpyAsync(sc->planes[view * 4 + k]->ptr, src[k], plane_bytes(c, k),
+                                  planes_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s),
+                  "upload plane");
+        sc->uploaded[view] = true;
+        return RVSB_OK;
+    });
+}
+
+rvsb_status rvsb_synthesize(rvsb_scene* scene, const rvsb_camera* virt, const rvsb_synth_params* params,
+                            const rvsb_yuv420* out, void* stream) {
+    return synthesize_impl(scene, virt, params, out, nullptr, stream);
+}
+
+rvsb_status rvsb_synthesize_debug(rvsb_scene* scene, const rvsb_camera* virt, const rvsb_synth_params* params,
+                                  const rvsb_yuv420* out, const rvsb_debug_out* dbg, void* stream) {
+    return synthesize_impl(scene, virt, params, out, dbg, stream);
+}
+
+int rvsb_scene_last_launch_count(const rvsb_scene* scene) { return scene ? scene->last_launches : 0; }
+
+rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs,
+                                 const rvsb_view_planes* host_planes, const rvsb_camera* virt,
+                                 const rvsb_synth_params* params, const rvsb_yuv420* out_host, void* stream) {
+    if (!ctx || !inputs || !host_planes || !virt || !out_host || n_inputs <= 0) return RVSB_E_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    // Reuse the scene of the previous call when the input cameras match.
+    rvsb_scene* sc = ctx->host_scene;
+    if (!sc || sc->cams.size() != (size_t)n_inputs ||
+        std::memcmp(sc->cams.data(), inputs, sizeof(rvsb_camera) * n_inputs) != 0) {
+        if (sc) rvsb_scene_destroy(sc);
+        ctx->host_scene = nullptr;
+        rvsb_status st = rvsb_scene_create(ctx, inputs, n_inputs, &sc);
+        if (st != RVSB_OK) return st;
+        ctx->host_scene = sc;
+    }
+    for (int v = 0; v < n_inputs; ++v) {
+        rvsb_status st = rvsb_scene_upload(sc, v, &host_planes[v], 0, stream);
+        if (st != RVSB_OK) return st;
+    }
+    return guarded(ctx, [&]() -> rvsb_status {
+        if (!out_host->y || !out_host->u || !out_host->v) throw ArgError("null output planes");
+        const size_t ny = (size_t)virt->width * virt->height * 2;
+        const size_t nc = (size_t)(virt->width / 2) * (virt->height / 2) * 2;
+        // Device output staging owned by the context.
+        if (ctx->host_out_bytes < ny + 2 * nc) {
+            if (ctx->host_out) {
+                cudaFree(ctx->host_out);
+                ctx->in_use -= ctx->host_out_bytes;
+                ctx->host_out = nullptr;
+                ctx->host_out_bytes = 0;
+            }
+            if (ctx->in_use + ny + 2 * nc > ctx->budget) throw BudgetError("output staging exceeds the HBM budget");
+            check(cudaMalloc(&ctx->host_out, ny + 2 * nc), "cudaMalloc");
+            ctx->host_out_bytes = ny + 2 * nc;
+            ctx->in_use += ny + 2 * nc;
+        }
+        rvsb_yuv420 dev;
+        char* base = static_cast<char*>(ctx->host_out);
+        dev.y = reinterpret_cast<uint16_t*>(base);
+        dev.u = reinterpret_cast<uint16_t*>(base + ny);
+        dev.v = reinterpret_cast<uint16_t*>(base + ny + nc);
+        rvsb_status st = synthesize_impl(sc, virt, params, &dev, nullptr, stream);
+        if (st != RVSB_OK) return st;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        check(cudaMemcpyAsync(out_host->y, dev.y, ny, cudaMemcpyDeviceToHost, s), "download Y");
+        check(cudaMemcpyAsync(out_host->u, dev.u, nc, cudaMemcpyDeviceToHost, s), "download U");
+        check(cudaMemcpyAsync(out_host->v, dev.v, nc, cudaMemcpyDeviceToHost, s), "download V");
+        check(cudaStreamSynchronize(s), "synchronize");
+        return RVSB_OK;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Front end
+// ---------------------------------------------------------------------------
+
+struct rvsb_config {
+    Config cfg;
+};
+
+static void copy_err(char* err, size_t len, const char* msg) {
+    if (err && len) {
+        std::strncpy(err, msg, len - 1);
+        err[len - 1] = 0;
+    }
+}
+
+rvsb_status rvsb_camera_from_json(const char* text, rvsb_camera* out, char* err, size_t err_len) {
+    if (!text || !out) return RVSB_E_ARG;
+    try {
+        *out = parse_camera(json::Node::parse(text));
+        return RVSB_OK;
+    } catch (const Unsupported& e) {
+        copy_err(err, err_len, e.what());
+        return RVSB_E_UNSUPPORTED;
+    } catch (const std::exception& e) {
+        copy_err(err, err_len, e.what());
+        return RVSB_E_CONFIG;
+    }
+}
+
+rvsb_status rvsb_config_load(const char* path, rvsb_config** out, char* err, size_t err_len) {
+    if (!path || !out) return RVSB_E_ARG;
+    *out = nullptr;
+    try {
+        auto c = std::make_unique<rvsb_config>();
+        c->cfg = load_config(path);
+        *out = c.release();
+        return RVSB_OK;
+    } catch (const IoError& e) {
+        copy_err(err, err_len, e.what());
+        return RVSB_E_IO;
+    } catch (const Unsupported& e) {
+        copy_err(err, err_len, e.what());
+        return RVSB_E_UNSUPPORTED;
+    } catch (const std::exception& e) {
+        copy_err(err, err_len, e.what());
+        return RVSB_E_CONFIG;
+    }
+}
+
+void rvsb_config_free(rvsb_config* cfg) { delete cfg; }
+int rvsb_config_num_inputs(const rvsb_config* c) { return c ? (int)c->cfg.params_real.size() : 0; }
+int rvsb_config_num_virtual(const rvsb_config* c) { return c ? (int)c->cfg.params_virtual.size() : 0; }
+
+rvsb_status rvsb_config_input_camera(const rvsb_config* c, int i, rvsb_camera* out) {
+    if (!c || !out || i < 0 || i >= (int)c->cfg.params_real.size()) return RVSB_E_ARG;
+    *out = c->cfg.params_real[i];
+    return RVSB_OK;
+}
+
+rvsb_status rvsb_config_virtual_camera(const rvsb_config* c, int i, rvsb_camera* out) {
+    if (!c || !out || i < 0 || i >= (int)c->cfg.params_virtual.size()) return RVSB_E_ARG;
+    *out = c->cfg.params_virtual[i];
+    return RVSB_OK;
+}
+
+const char* rvsb_config_texture_path(const rvsb_config* c, int i) {
+    return (c && i >= 0 && i < (int)c->cfg.texture_names.size()) ? c->cfg.texture_names[i].c_str() : nullptr;
+}
+const char* rvsb_config_depth_path(const rvsb_config* c, int i) {
+    return (c && i >= 0 && i < (int)c->cfg.depth_names.size()) ? c->cfg.depth_names[i].c_str() : nullptr;
+}
+const char* rvsb_config_output_path(const rvsb_config* c, int i) {
+    return (c && i >= 0 && i < (int)c->cfg.outfilenames.size()) ? c->cfg.outfilenames[i].c_str() : nullptr;
+}
+
+void rvsb_config_frames(const rvsb_config* c, int* start, int* n, int* nout) {
+    if (!c) return;
+    if (start) *start = c->cfg.start_frame;
+    if (n) *n = c->cfg.number_of_frames;
+    if (nout) *nout = c->cfg.number_of_output_frames;
+}
+
+void rvsb_config_synth_params(const rvsb_config* c, rvsb_synth_params* out) {
+    if (!c || !out) return;
+    std::memset(out, 0, sizeof(*out));
+    out->blending_factor = c->cfg.blending_factor;
+    out->precision = c->cfg.precision;
+}
+
+rvsb_status rvsb_config_virtual_camera_at(const rvsb_config* c, int i, int frame, rvsb_camera* out) {
+    if (!c || !out || i < 0 || i >= (int)c->cfg.params_virtual.size() || frame < 0) return RVSB_E_ARG;
+    *out = c->cfg.params_virtual[i];
+    if (!c->cfg.pose_trace.empty()) {
+        if (frame >= (int)c->cfg.pose_trace.size()) return RVSB_E_ARG;
+        const Pose& p = c->cfg.pose_trace[frame];
+        for (int k = 0; k < 3; ++k) out->position[k] = out->position[k] + p.position[k];
+        for (int k = 0; k < 3; ++k) out->rotation[k] = p.rotation[k];
+    }
+    return RVSB_OK;
+}
+
+}  // extern "C"

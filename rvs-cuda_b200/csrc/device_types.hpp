@@ -1,0 +1,65 @@
+// Parameter blocks shared by the host launch code and the kernels.
+#pragma once
+
+#include <cstdint>
+
+namespace rvsb {
+
+// Tiling constants.  A binning block is BLOCK_W x BLOCK_H quads of an input
+// view (each quad = two triangles, transform.cpp:159-176); an output tile is
+// TILE x TILE pixels whose 64-bit z-buffer lives in shared memory.
+constexpr int BLOCK_W = 16;
+constexpr int BLOCK_H = 8;
+constexpr int TILE = 32;
+constexpr int TILE_THREADS = 256;
+
+// Per input view parameters of one synthesis (device copy in a table).
+struct DevView {
+    int w, h;          // input size
+    int proj;          // 0 perspective, 1 equirectangular
+    int bits_color;
+    float f0, f1, p0, p1;                 // perspective intrinsics
+    float near_, far_, depth_scale;       // depth decode (process_input_frame.cu:369-376)
+    int has_invalid;
+    float color_scale;                    // 1 / (2^bits - 1)
+    float chroma_sx, chroma_sy;           // (w/2)/w, (h/2)/h as float
+    int cw, ch;                           // chroma plane size
+    float R[9], t[3];                     // relative pose (SpaceTransformer.cpp:77-92)
+    const uint16_t* py;
+    const uint16_t* pu;
+    const uint16_t* pv;
+    const uint16_t* pd;
+    const float* erp_row;                 // ERP: per row (cos theta, sin theta), 2*h floats
+    const float* erp_col;                 // ERP: per column (cos phi, sin phi), 2*w floats
+    float4* vert;                         // h*w warped vertices (u, v, z, 0)
+    int4* bbox;                           // per binning block: x0, y0, x1, y1 (x0 > x1: empty)
+    int nbx, nby;                         // binning blocks
+    int pad[2];
+};
+
+// Virtual camera of one synthesis.
+struct DevTarget {
+    int wo, ho;
+    int proj;
+    int wrap;                             // horizontal wrap (ERP output, full range)
+    float f0, f1, p0, p1;                 // perspective
+    float u0, v0, du_dphi, dv_dtheta;     // equirectangular
+    int bits;                             // output bit depth
+    unsigned max_val;                     // 2^bits - 1
+    float blend_exp;                      // BlendingFactor
+    float inv_blend_exp;                  // 1.0f / BlendingFactor
+    int ntx, nty;                         // output tiles
+    int n_views;
+    int bin_capacity;
+};
+
+// Status words written by the kernels (device memory, zeroed per call).
+struct DevStatus {
+    int bin_total;      // number of (tile, view, block) entries
+    int bin_overflow;   // 1 when bin_total exceeded the list capacity
+    int hole_x0, hole_y0, hole_x1, hole_y1;   // bounding box of holes (x0 > x1: none)
+    int n_holes;
+    int pad;
+};
+
+}  // namespace rvsb

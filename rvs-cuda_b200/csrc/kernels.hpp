@@ -1,0 +1,60 @@
+// Host-side interface of the synthesis kernels (kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_types.hpp"
+
+namespace rvsb {
+
+// Device buffers of one synthesis workspace.
+struct SynthBuffers {
+    DevView* views = nullptr;      // n_views entries (device)
+    DevTarget* target = nullptr;   // 1 entry (device)
+    DevStatus* status = nullptr;   // 1 entry (device)
+    int* counts = nullptr;         // ntiles * n_views
+    int* offsets = nullptr;        // ntiles * n_views
+    int* cursor = nullptr;         // ntiles * n_views
+    int* list = nullptr;           // bin list, `capacity` entries
+    int capacity = 0;
+    uint64_t* codes = nullptr;     // Wo*Ho packed output codes + hole bit
+    uint64_t* scan_a = nullptr;    // Wo*Ho inpainting scratch
+    uint64_t* scan_b = nullptr;
+    uint64_t* scan_c = nullptr;
+    uint64_t* scan_d = nullptr;
+};
+
+// Optional intermediate outputs (device pointers, may be null).
+struct DebugPtrs {
+    float* warped_uvz = nullptr;
+    float* view_color = nullptr;
+    float* view_depth = nullptr;
+    float* view_validity = nullptr;
+    float* blend_color = nullptr;
+    float* blend_quality = nullptr;
+    int32_t* inpaint_source = nullptr;
+    bool any() const {
+        return warped_uvz || view_color || view_depth || view_validity || blend_color ||
+               blend_quality || inpaint_source;
+    }
+};
+
+// Sizes the launch code needs on the host.
+struct LaunchShape {
+    int n_views;
+    int max_w, max_h;        // largest input view
+    int max_blocks;          // largest nbx * nby
+    int wo, ho;
+    int ntx, nty;
+    int input_w[64];         // per view (for the debug copy of warped vertices)
+    int input_h[64];
+    int64_t vert_offset[64]; // element offset of each view's vertices in the vertex arena
+};
+
+// Issues the whole synthesis on `stream`; returns the number of kernel
+// launches, or -1 on a launch error (cudaGetLastError holds the cause).
+int launch_synthesis(const SynthBuffers& b, const LaunchShape& shape, const DebugPtrs& dbg,
+                     uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t stream);
+
+}  // namespace rvsb

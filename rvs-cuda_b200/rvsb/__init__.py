@@ -1,0 +1,288 @@
+"""Python binding (ctypes) of the B200 RVS synthesis backend, librvsb.so.
+
+The library is the product: every call goes through the C ABI declared in
+include/rvsb.h.  Loading fails loudly when the library is missing; there is
+no fallback implementation.
+
+Device buffers are passed as raw pointers (e.g. torch tensors' data_ptr()),
+streams as cudaStream_t handles (torch.cuda.Stream.cuda_stream).
+"""
+import ctypes
+import os
+
+from .abi import (Camera, DebugOut, SynthParams, ViewPlanes, Yuv420, make_camera, PERSPECTIVE,
+                  EQUIRECTANGULAR, YUV420, YUV400, RVSB_OK)
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "librvsb.so")
+
+# Every entry point include/rvsb.h declares.
+EXPORTED = [
+    "rvsb_create", "rvsb_destroy", "rvsb_last_error", "rvsb_status_string", "rvsb_memory_in_use",
+    "rvsb_camera_from_json", "rvsb_config_load", "rvsb_config_free", "rvsb_config_num_inputs",
+    "rvsb_config_num_virtual", "rvsb_config_input_camera", "rvsb_config_virtual_camera",
+    "rvsb_config_texture_path", "rvsb_config_depth_path", "rvsb_config_output_path", "rvsb_config_frames",
+    "rvsb_config_synth_params", "rvsb_config_virtual_camera_at", "rvsb_relative_pose", "rvsb_scene_create",
+    "rvsb_scene_destroy", "rvsb_scene_upload", "rvsb_synthesize", "rvsb_synthesize_host",
+    "rvsb_synthesize_debug", "rvsb_scene_last_launch_count",
+]
+
+_lib = None
+
+
+class RvsbError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"rvsb status {status}: {msg}")
+        self.status = status
+
+
+def load():
+    """Loads librvsb.so (built by rvs-cuda_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"native library missing: {LIB_PATH} (run rvs-cuda_b200/build.py)")
+    L = ctypes.CDLL(LIB_PATH)
+    c_p = ctypes.c_void_p
+    P = ctypes.POINTER
+    L.rvsb_create.argtypes = [ctypes.c_int, ctypes.c_size_t, P(c_p)]
+    L.rvsb_destroy.argtypes = [c_p]
+    L.rvsb_destroy.restype = None
+    L.rvsb_last_error.argtypes = [c_p]
+    L.rvsb_last_error.restype = ctypes.c_char_p
+    L.rvsb_status_string.argtypes = [ctypes.c_int]
+    L.rvsb_status_string.restype = ctypes.c_char_p
+    L.rvsb_memory_in_use.argtypes = [c_p]
+    L.rvsb_memory_in_use.restype = ctypes.c_size_t
+    L.rvsb_camera_from_json.argtypes = [ctypes.c_char_p, P(Camera), ctypes.c_char_p, ctypes.c_size_t]
+    L.rvsb_config_load.argtypes = [ctypes.c_char_p, P(c_p), ctypes.c_char_p, ctypes.c_size_t]
+    L.rvsb_config_free.argtypes = [c_p]
+    L.rvsb_config_free.restype = None
+    L.rvsb_config_num_inputs.argtypes = [c_p]
+    L.rvsb_config_num_virtual.argtypes = [c_p]
+    L.rvsb_config_input_camera.argtypes = [c_p, ctypes.c_int, P(Camera)]
+    L.rvsb_config_virtual_camera.argtypes = [c_p, ctypes.c_int, P(Camera)]
+    for f in ("rvsb_config_texture_path", "rvsb_config_depth_path", "rvsb_config_output_path"):
+        getattr(L, f).argtypes = [c_p, ctypes.c_int]
+        getattr(L, f).restype = ctypes.c_char_p
+    L.rvsb_config_frames.argtypes = [c_p, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+    L.rvsb_config_frames.restype = None
+    L.rvsb_config_synth_params.argtypes = [c_p, P(SynthParams)]
+    L.rvsb_config_synth_params.restype = None
+    L.rvsb_config_virtual_camera_at.argtypes = [c_p, ctypes.c_int, ctypes.c_int, P(Camera)]
+    L.rvsb_relative_pose.argtypes = [P(Camera), P(Camera), P(ctypes.c_float), P(ctypes.c_float)]
+    L.rvsb_scene_create.argtypes = [c_p, P(Camera), ctypes.c_int, P(c_p)]
+    L.rvsb_scene_destroy.argtypes = [c_p]
+    L.rvsb_scene_destroy.restype = None
+    L.rvsb_scene_upload.argtypes = [c_p, ctypes.c_int, P(ViewPlanes), ctypes.c_int, c_p]
+    L.rvsb_synthesize.argtypes = [c_p, P(Camera), P(SynthParams), P(Yuv420), c_p]
+    L.rvsb_synthesize_host.argtypes = [c_p, P(Camera), ctypes.c_int, P(ViewPlanes), P(Camera),
+                                       P(SynthParams), P(Yuv420), c_p]
+    L.rvsb_synthesize_debug.argtypes = [c_p, P(Camera), P(SynthParams), P(Yuv420), P(DebugOut), c_p]
+    L.rvsb_scene_last_launch_count.argtypes = [c_p]
+    _lib = L
+    return L
+
+
+def status_string(status):
+    return load().rvsb_status_string(status).decode()
+
+
+def params(blending_factor=5.0, precision=1.0):
+    p = SynthParams()
+    p.blending_factor = blending_factor
+    p.precision = precision
+    return p
+
+
+class Context:
+    """rvsb_context: one CUDA device and an HBM budget."""
+
+    def __init__(self, device=0, hbm_budget=0):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        st = self.lib.rvsb_create(int(device), int(hbm_budget), ctypes.byref(h))
+        if st != RVSB_OK:
+            raise RvsbError(st, "rvsb_create failed: " + status_string(st))
+        self.h = h
+
+    def check(self, st):
+        if st != RVSB_OK:
+            raise RvsbError(st, self.last_error())
+        return st
+
+    def last_error(self):
+        return self.lib.rvsb_last_error(self.h).decode()
+
+    def memory_in_use(self):
+        return self.lib.rvsb_memory_in_use(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.rvsb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synthesize_host(self, cams, host_planes, virt, p, out_planes, stream=None):
+        """Plain per-view call with host buffers (numpy or pinned torch)."""
+        n = len(cams)
+        arr = (Camera * n)(*cams)
+        vp = (ViewPlanes * n)()
+        for i, planes in enumerate(host_planes):
+            vp[i].y, vp[i].u, vp[i].v, vp[i].depth = (_ptr(a) for a in planes)
+        out = Yuv420(*(_ptr(a) for a in out_planes))
+        return self.check(self.lib.rvsb_synthesize_host(self.h, arr, n, vp, ctypes.byref(virt),
+                                                        ctypes.byref(p), ctypes.byref(out),
+                                                        _stream(stream)))
+
+
+class Scene:
+    """rvsb_scene: input views resident in device memory."""
+
+    def __init__(self, ctx, cams):
+        self.ctx = ctx
+        self.cams = list(cams)
+        n = len(self.cams)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.rvsb_scene_create(ctx.h, (Camera * n)(*self.cams), n, ctypes.byref(h)))
+        self.h = h
+
+    def upload(self, view, planes, on_device, stream=None):
+        vp = ViewPlanes(*(_ptr(a) for a in planes))
+        return self.ctx.check(self.ctx.lib.rvsb_scene_upload(self.h, int(view), ctypes.byref(vp),
+                                                             1 if on_device else 0, _stream(stream)))
+
+    def synthesize(self, virt, p, out_planes, stream=None):
+        out = Yuv420(*(_ptr(a) for a in out_planes))
+        return self.ctx.check(self.ctx.lib.rvsb_synthesize(self.h, ctypes.byref(virt), ctypes.byref(p),
+                                                           ctypes.byref(out), _stream(stream)))
+
+    def synthesize_debug(self, virt, p, out_planes, dbg, stream=None):
+        out = Yuv420(*(_ptr(a) for a in out_planes))
+        d = DebugOut(*(_ptr(dbg.get(k)) for k in ("warped_uvz", "view_color", "view_depth",
+                                                   "view_validity", "blend_color", "blend_quality",
+                                                   "inpaint_source")))
+        return self.ctx.check(self.ctx.lib.rvsb_synthesize_debug(self.h, ctypes.byref(virt), ctypes.byref(p),
+                                                                 ctypes.byref(out), ctypes.byref(d),
+                                                                 _stream(stream)))
+
+    def last_launch_count(self):
+        return self.ctx.lib.rvsb_scene_last_launch_count(self.h)
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.rvsb_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ptr(a):
+    """Raw address of a numpy array, torch tensor or int (None -> NULL)."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if hasattr(a, "ctypes"):
+        return a.ctypes.data
+    raise TypeError(f"cannot take the address of {type(a)}")
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+def relative_pose(cin, cvirt):
+    L = load()
+    R = (ctypes.c_float * 9)()
+    t = (ctypes.c_float * 3)()
+    L.rvsb_relative_pose(ctypes.byref(cin), ctypes.byref(cvirt), R, t)
+    return list(R), list(t)
+
+
+def camera_from_json(text):
+    L = load()
+    c = Camera()
+    err = ctypes.create_string_buffer(1024)
+    st = L.rvsb_camera_from_json(text.encode(), ctypes.byref(c), err, 1024)
+    if st != RVSB_OK:
+        raise RvsbError(st, err.value.decode())
+    return c
+
+
+class Config:
+    """rvsb_config: an RVS configuration file and its camera files."""
+
+    def __init__(self, path):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(1024)
+        st = self.lib.rvsb_config_load(str(path).encode(), ctypes.byref(h), err, 1024)
+        if st != RVSB_OK:
+            raise RvsbError(st, err.value.decode())
+        self.h = h
+
+    def inputs(self):
+        n = self.lib.rvsb_config_num_inputs(self.h)
+        out = []
+        for i in range(n):
+            c = Camera()
+            self.lib.rvsb_config_input_camera(self.h, i, ctypes.byref(c))
+            out.append(c)
+        return out
+
+    def virtual(self, i=0, frame=None):
+        c = Camera()
+        if frame is None:
+            st = self.lib.rvsb_config_virtual_camera(self.h, i, ctypes.byref(c))
+        else:
+            st = self.lib.rvsb_config_virtual_camera_at(self.h, i, frame, ctypes.byref(c))
+        if st != RVSB_OK:
+            raise RvsbError(st, "no such virtual camera / frame")
+        return c
+
+    def frames(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self.lib.rvsb_config_frames(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+    def synth_params(self):
+        p = SynthParams()
+        self.lib.rvsb_config_synth_params(self.h, ctypes.byref(p))
+        return p
+
+    def paths(self, i):
+        f = lambda g: (g(self.h, i) or b"").decode()
+        return f(self.lib.rvsb_config_texture_path), f(self.lib.rvsb_config_depth_path)
+
+    def output_path(self, i=0):
+        r = self.lib.rvsb_config_output_path(self.h, i)
+        return r.decode() if r else None
+
+    def close(self):
+        if self.h:
+            self.lib.rvsb_config_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

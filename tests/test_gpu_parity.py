@@ -1,0 +1,116 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bar (per the synthesis spec): Y/U/V PSNR >= 50 dB against the oracle's
+output, <= 0.5% of samples differing by more than 2 codes, and an identical
+hole mask.  Stage checks are stricter: warped (u, v, depth) are bit-exact,
+per-view coverage and the hole mask are identical, and inpainting copies the
+same source pixel.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import rvsb
+from rvsb import scenes
+from helpers import assert_parity, gpu_synthesize, parity_report
+
+pytestmark = pytest.mark.gpu
+
+SMALL_CASES = [
+    dict(n_views=2, w=64, h=36, seed=1),
+    dict(n_views=3, w=96, h=54, seed=2),
+    dict(n_views=4, w=80, h=48, seed=3),
+    dict(n_views=2, w=128, h=64, seed=4, erp_in=True),
+    dict(n_views=3, w=128, h=64, seed=5, erp_in=True, erp_out=True),
+    dict(n_views=1, w=64, h=36, seed=6),
+]
+
+
+def _oracle_stages(wl, target, exponent):
+    """CPU oracle stage by stage: warped uv/z, per-view raster, blend."""
+    warped, views = [], []
+    for cam, (y, u, v, d) in zip(wl.inputs, wl.planes):
+        col = O.decode_color(y, u, v, cam.bit_depth_color)
+        dep = O.decode_depth(d, cam)
+        uv, vd, wrap = O.warp(cam, target, dep)
+        warped.append((uv, vd))
+        oc, od, ov = O.raster(col, vd, uv, target.width, target.height, wrap)
+        views.append((oc, od, ov))
+    qual = [ov / od for (oc, od, ov) in views]
+    bc, bq = O.blend([v[0] for v in views], qual, [v[1] for v in views], exponent)
+    return warped, views, bc, bq
+
+
+@pytest.mark.parametrize("case", SMALL_CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+@pytest.mark.parametrize("exponent", [5.0, 1.0])
+def test_stages_small(ctx, case, exponent):
+    wl = scenes.random_pose_small(**case)
+    target = wl.targets[0]
+    yuv, dbg, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, exponent, debug=True)
+    warped, views, bc, bq = _oracle_stages(wl, target, exponent)
+    # 1. warp: bit-exact (NaN where the CPU writes NaN)
+    for v, (uv, vd) in enumerate(warped):
+        g = dbg["warped"][v]
+        np.testing.assert_array_equal(g[..., 0], uv[..., 0])
+        np.testing.assert_array_equal(g[..., 1], uv[..., 1])
+        np.testing.assert_array_equal(g[..., 2], vd)
+    # 2. raster: identical coverage, same winner colour/depth
+    for v, (oc, od, ov) in enumerate(views):
+        gcov = dbg["view_validity"][v] > 0
+        ccov = ov > 0
+        assert np.array_equal(gcov, ccov), f"view {v}: coverage differs at {np.argwhere(gcov != ccov)[:5]}"
+        same = np.isclose(dbg["view_depth"][v], od, rtol=1e-5) | (~ccov)
+        assert same.mean() > 0.995
+        np.testing.assert_allclose(dbg["view_color"][v][ccov], oc[ccov], atol=2e-3)
+    # 3. blend: identical hole mask, close colour
+    ghole = ~(dbg["blend_quality"] > 0)
+    chole = ~(bq > 0)
+    assert np.array_equal(ghole, chole)
+    np.testing.assert_allclose(dbg["blend_color"], bc, atol=2e-3)
+    # 4. end to end
+    cpu = O.synthesize(wl.inputs, wl.planes, target, exponent)
+    assert_parity(yuv, cpu)
+
+
+@pytest.mark.parametrize("seed", [11, 12, 13])
+def test_inpaint_sources_match(ctx, seed):
+    """Holes copy exactly the pixel the reference's sweeps choose."""
+    wl = scenes.random_pose_small(n_views=2, w=96, h=54, seed=seed)
+    target = wl.targets[0]
+    target.rotation[0] += 6.0  # rotate away to open border holes
+    yuv, dbg, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, debug=True)
+    q = dbg["blend_quality"]
+    hole = ~(q > 0)
+    assert hole.sum() > 20
+    _, src, _ = O.inpaint(dbg["blend_color"], q)
+    np.testing.assert_array_equal(dbg["inpaint_source"][hole], src[hole])
+
+
+def test_deterministic(ctx):
+    wl = scenes.random_pose_small(n_views=3, w=96, h=54, seed=21)
+    a, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, wl.targets[0], 5.0)
+    b, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, wl.targets[0], 5.0)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_plain_small_full_size(ctx):
+    """2 x 960x540 -> 960x540 (the CPU-runnable workload), full size."""
+    wl = scenes.plain_small()
+    target = wl.targets[0]
+    yuv, dbg, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, debug=True)
+    cpu, cq, _ = O.synthesize(wl.inputs, wl.planes, target, 5.0, want_intermediate=True)
+    assert np.array_equal(~(dbg["blend_quality"] > 0), ~(cq > 0))
+    r = assert_parity(yuv, cpu)
+    print(r)
+
+
+def test_plain_1080p_full_size(ctx):
+    """4 x 1920x1080 -> 1920x1080 (the headline workload), full size."""
+    wl = scenes.plain_1080p()
+    target = wl.targets[0]
+    yuv, dbg, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, debug=True)
+    cpu, cq, _ = O.synthesize(wl.inputs, wl.planes, target, 5.0, want_intermediate=True)
+    assert np.array_equal(~(dbg["blend_quality"] > 0), ~(cq > 0))
+    r = assert_parity(yuv, cpu)
+    print(r)
