@@ -1,0 +1,356 @@
+"""Benchmark of the B200 RVS synthesis path.
+
+Default workload (N=1): 4 perspective inputs 1920x1080 (10-bit YUV420, 16-bit
+depth) -> 1 perspective 1920x1080 view, seeded synthetic scene.  A step is
+one synthesis of the virtual view from the resident raw input planes.
+
+  value  views/s with the input planes resident in HBM (device-timed with
+         CUDA events around each synthesis; L2 flushed between steps).
+  e2e    the same metric through the reference-facing C-ABI call with host
+         buffers (rvsb_synthesize_host): pinned host -> device upload of the
+         raw planes, synthesis and download of the YUV420 result every step.
+  roofline  of the dominant kernel, with its algorithmic bytes per launch.
+  cpu_baseline  the CPU oracle (a restatement of the reference's CPU path)
+         on a bounded sample, 1 thread (the reference's loops are serial).
+
+Multi-GPU: pose-parallel replicas (each rank synthesises its own views;
+no collective on the data path), value = all ranks' views / max time.
+
+--impl reference times the reference's CPU path (the oracle port; the
+reference itself does not build here) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rvs-cuda_b200"))
+
+METRIC = "synth views/s + p50/p99 ms, batched-served vs plain on B200, ≥50 dB vs CPU"
+UNIT = "views/s"
+CACHE = os.path.join(ROOT, ".scene_cache")
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,utilization.gpu,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 10:
+                continue
+            rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [r for r in rows if r[3].isdigit() and int(r[3]) > 0] or rows
+        sm = [float(r[1]) for r in load if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in load for k in range(4) if r[6 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows), "samples_under_load": len(load)}
+
+
+def percentile(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = (len(xs) - 1) * q / 100.0
+    f = int(k)
+    c = min(f + 1, len(xs) - 1)
+    return xs[f] + (xs[c] - xs[f]) * (k - f)
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def workload_plain():
+    from rvsb import scenes
+    wl = scenes.plain_1080p()
+    scenes.cache_planes(wl, CACHE)
+    return wl
+
+
+def cpu_baseline_port(wl, n_views=5):
+    """The CPU oracle on `n_views` syntheses of the workload, 1 thread."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    t0 = time.perf_counter()
+    for _ in range(n_views):
+        O.synthesize(wl.inputs, wl.planes, wl.targets[0], wl.blending_factor)
+    dt = time.perf_counter() - t0
+    return {"value": n_views / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n_views} syntheses of the 4x1920x1080 -> 1920x1080 view, 1 thread, "
+                      f"{dt:.1f} s; host has {os.cpu_count()} cores"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU synthesis (oracle port) on the
+    host cores, one view per thread per step."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    wl = workload_plain()
+    threads = max(1, min(32, os.cpu_count() or 1))
+
+    def one(_):
+        O.synthesize(wl.inputs, wl.planes, wl.targets[0], wl.blending_factor)
+
+    with ThreadPoolExecutor(threads) as ex:
+        for _ in range(args.warmup):
+            list(ex.map(one, range(threads)))
+        step_times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            list(ex.map(one, range(threads)))
+            step_times.append(time.perf_counter() - t0)
+    total = sum(step_times)
+    value = threads * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene, RVS file formats)",
+        "config": {"workload": "plain_1080p: 4 perspective 1920x1080 inputs -> 1 perspective 1920x1080 view",
+                   "step": f"{threads} views synthesised in parallel, one per host thread"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} steps x {threads} views of the 4x1080p workload; the "
+                                   "reference RVS needs OpenCV C++ and does not build here, so its CPU path "
+                                   "runs as the oracle restatement"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--e2e-steps", type=int, default=40)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+    import rvsb
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    wl = workload_plain()
+    target = wl.targets[0]
+    p = rvsb.params(wl.blending_factor)
+    ctx = rvsb.Context(local)
+    stream = torch.cuda.current_stream()
+
+    # Resident scene: raw planes uploaded once.
+    scene = rvsb.Scene(ctx, wl.inputs)
+    dev_planes = []
+    for i, planes in enumerate(wl.planes):
+        dp = [torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).reshape(-1).cuda() for a in planes]
+        dev_planes.append(dp)
+        scene.upload(i, dp, on_device=True, stream=stream)
+    wo, ho = target.width, target.height
+    out = [torch.empty(n, dtype=torch.int16, device="cuda")
+           for n in (wo * ho, (wo // 2) * (ho // 2), (wo // 2) * (ho // 2))]
+    scene.set_profiling(True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    for _ in range(args.warmup):
+        scene.synthesize(target, p, out, stream=stream)
+    torch.cuda.synchronize()
+    launches_per_step = scene.last_launch_count()
+
+    step_ms, stage_acc = [], {k: 0.0 for k in rvsb.STAGES}
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()  # L2 flush (256 MiB > 126 MB L2), outside the timed events
+        ev[k][0].record(stream)
+        scene.synthesize(target, p, out, stream=stream)
+        ev[k][1].record(stream)
+        ev[k][1].synchronize()
+        for name, ms in scene.stage_times().items():
+            stage_acc[name] += ms
+    torch.cuda.synchronize()
+    barrier(world)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_s = sum(step_ms) / 1000.0
+    max_total = allreduce_max(total_s, world)
+    value = world * args.steps / max_total
+
+    # e2e: reference-facing call with pinned host buffers.
+    host_planes = [[torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).reshape(-1).pin_memory()
+                    for a in planes] for planes in wl.planes]
+    host_out = [torch.empty(t.numel(), dtype=torch.int16).pin_memory() for t in out]
+    h2d = sum(t.numel() * 2 for planes in host_planes for t in planes)
+    d2h = sum(t.numel() * 2 for t in host_out)
+    for _ in range(3):
+        ctx.synthesize_host(wl.inputs, host_planes, target, p, host_out, stream=stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = []
+    for _ in range(args.e2e_steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.synthesize_host(wl.inputs, host_planes, target, p, host_out, stream=stream)
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    barrier(world)
+    e2e_total = allreduce_max(sum(e2e_ms) / 1000.0, world)
+    e2e_value = world * args.e2e_steps / e2e_total
+    clocks = sampler.stop()
+
+    # Roofline of the dominant kernel (per launch, averaged over the timed steps).
+    n_views = len(wl.inputs)
+    n_in = sum(c.width * c.height for c in wl.inputs)
+    n_out = wo * ho
+    stage_avg = {k: v / args.steps for k, v in stage_acc.items()}
+    algorithmic = {
+        # SURVEY-defined figures: warp 14 B per input pixel; blend (10N + 4) B
+        # per output pixel; the tile kernel also reads the warped mesh
+        # (12 B per input pixel) for its raster.
+        "warp": 14 * n_in,
+        "tile": 12 * n_in + (10 * n_views + 4) * n_out,
+    }
+    dominant = max(("warp", "tile", "inpaint", "bin"), key=lambda k: stage_avg[k])
+    peak, peak_kind = measured_peaks()
+    rk = dominant if dominant in algorithmic else "tile"
+    achieved = algorithmic[rk] / (stage_avg[rk] / 1000.0) / 1e9
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", "tile_kernel_traffic.json")
+    if os.path.exists(prof_path):
+        try:
+            traffic = json.load(open(prof_path)).get(rk)
+        except Exception:
+            traffic = None
+    roofline = {"kernel": {"tile": "tile_kernel", "warp": "warp_kernel"}[rk], "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": algorithmic[rk], "ms_per_launch": stage_avg[rk],
+                "dominant_stage": dominant}
+    stage_roof = {k: {"ms": stage_avg[k], "GBs": algorithmic[k] / (stage_avg[k] / 1000.0) / 1e9,
+                      "frac": algorithmic[k] / (stage_avg[k] / 1000.0) / 1e9 / peak}
+                  for k in algorithmic}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(wl)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene, RVS file formats: 10-bit YUV420, 16-bit depth)",
+            "config": {"workload": "plain_1080p: 4 perspective 1920x1080 inputs -> 1 perspective 1920x1080 view "
+                                   "(2x2 grid 0.15 m, f=1500, target +-10 cm / +-5 deg)",
+                       "global_batch": world, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "blending_factor": wl.blending_factor},
+            "p50_ms": percentile(step_ms, 50), "p99_ms": percentile(step_ms, 99),
+            "stage_ms": stage_avg, "stage_roofline": stage_roof,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "p50_ms": percentile(e2e_ms, 50), "p99_ms": percentile(e2e_ms, 99),
+                    "call": "rvsb_synthesize_host (pinned host buffers)"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches_per_step * args.steps,
+        }
+        print(json.dumps(line))
+    scene.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -18,9 +18,10 @@ INCLUDE = os.path.join(ROOT, "include")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-CU_SOURCES = ["kernels.cu"]
+CU_SOURCES = ["launch.cu", "warp.cu", "bin.cu", "tile.cu", "inpaint.cu"]
 CPP_SOURCES = ["api.cpp", "frontend.cpp", "camera.cpp"]
 CLI_SOURCES = ["rvsb_cli.cpp"]
+SCENEGEN_SOURCES = ["scenegen.cpp"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = GENCODE + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
@@ -29,6 +30,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
              "-Wno-unused-parameter"]
 
 LIB_PATH = os.path.join(LIB, "librvsb.so")
+SCENEGEN_PATH = os.path.join(LIB, "libscenegen.so")
 CLI_PATH = os.path.join(LIB, "rvsb")
 
 
@@ -92,6 +94,9 @@ def build(force=False, verbose=False):
     if force or _stale(CLI_PATH, [cli_obj, LIB_PATH]):
         _run(["g++", "-o", CLI_PATH, cli_obj, "-L", LIB, "-lrvsb", "-Wl,-rpath,$ORIGIN",
               "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart"])
+    sg = os.path.join(CSRC, SCENEGEN_SOURCES[0])
+    if force or _stale(SCENEGEN_PATH, [sg]):
+        _run(["g++", "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-shared", "-o", SCENEGEN_PATH, sg])
     return LIB_PATH
 
 

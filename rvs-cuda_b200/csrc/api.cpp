@@ -81,10 +81,10 @@ struct DevMem {
 
 struct Workspace {
     int wo = 0, ho = 0;
-    DevMem views, target, status, counts, offsets, cursor, list, codes, scan[4], vert, bbox;
+    DevMem status, counts, offsets, cursor, list, codes, scan[4], vert, bbox;
     SynthBuffers b;
     LaunchShape shape{};
-    std::vector<DevView> host_views;
+    ViewTable table{};
     std::vector<int64_t> vert_off, bbox_off;
 };
 
@@ -98,6 +98,13 @@ struct rvsb_scene {
     std::vector<bool> uploaded;
     std::unique_ptr<Workspace> ws;
     int last_launches = 0;
+    bool profiling = false;
+    bool profiled = false;
+    cudaEvent_t events[2 * NUM_STAGES] = {};
+    ~rvsb_scene() {
+        for (auto& e : events)
+            if (e) cudaEventDestroy(e);
+    }
 };
 
 namespace {
@@ -163,8 +170,6 @@ void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
     const int capacity = (int)std::min<int64_t>(INT32_MAX / 2, std::max<int64_t>(1 << 16, nbb * 8 + nbins));
     ws->vert.alloc(ctx, (size_t)nvert * sizeof(float4));
     ws->bbox.alloc(ctx, (size_t)nbb * sizeof(int4));
-    ws->views.alloc(ctx, sizeof(DevView) * n);
-    ws->target.alloc(ctx, sizeof(DevTarget));
     ws->status.alloc(ctx, sizeof(DevStatus));
     ws->counts.alloc(ctx, nbins * sizeof(int));
     ws->offsets.alloc(ctx, nbins * sizeof(int));
@@ -174,8 +179,6 @@ void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
     ws->codes.alloc(ctx, npix * sizeof(uint64_t));
     for (auto& s : ws->scan) s.alloc(ctx, npix * sizeof(uint64_t));
     SynthBuffers& b = ws->b;
-    b.views = ws->views.as<DevView>();
-    b.target = ws->target.as<DevTarget>();
     b.status = ws->status.as<DevStatus>();
     b.counts = ws->counts.as<int>();
     b.offsets = ws->offsets.as<int>();
@@ -196,21 +199,20 @@ void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
     sh.ho = ho;
     sh.ntx = ntx;
     sh.nty = nty;
-    for (int v = 0; v < n && v < 64; ++v) {
+    for (int v = 0; v < n && v < MAX_VIEWS; ++v) {
         sh.input_w[v] = sc->cams[v].width;
         sh.input_h[v] = sc->cams[v].height;
         sh.vert_offset[v] = ws->vert_off[v];
     }
-    ws->host_views.resize(n);
     sc->ws = std::move(ws);
 }
 
-void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_params& p, DevTarget& T) {
+void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_params& p) {
     Workspace& ws = *sc->ws;
     const int n = (int)sc->cams.size();
     for (int v = 0; v < n; ++v) {
         const rvsb_camera& c = sc->cams[v];
-        DevView& V = ws.host_views[v];
+        DevView& V = ws.table.v[v];
         std::memset(&V, 0, sizeof(V));
         V.w = c.width;
         V.h = c.height;
@@ -240,9 +242,12 @@ void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_param
         }
         V.vert = ws.vert.as<float4>() + ws.vert_off[v];
         V.bbox = ws.bbox.as<int4>() + ws.bbox_off[v];
+        V.tri_shift = 2;
+        while ((1 << (V.tri_shift - 2)) < c.width - 1) ++V.tri_shift;
         V.nbx = nblocks_x(c.width);
         V.nby = nblocks_y(c.height);
     }
+    DevTarget& T = ws.table.t;
     std::memset(&T, 0, sizeof(T));
     T.wo = virt.width;
     T.ho = virt.height;
@@ -257,6 +262,13 @@ void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_param
     T.max_val = (1u << virt.bit_depth_color) - 1u;
     T.blend_exp = p.blending_factor;
     T.inv_blend_exp = 1.0f / p.blending_factor;
+    T.blend_exp_int = 0;
+    if (p.blending_factor == std::floor(p.blending_factor) && p.blending_factor >= 2.f && p.blending_factor <= 16.f)
+        T.blend_exp_int = (int)p.blending_factor;
+    {
+        const float t = -1e-6f;
+        T.lambda_mid = ((double)t + (double)std::nextafter(t, -INFINITY)) / 2.0;
+    }
     T.ntx = ws.shape.ntx;
     T.nty = ws.shape.nty;
     T.n_views = n;
@@ -283,13 +295,8 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
         check(cudaSetDevice(ctx->device), "cudaSetDevice");
         ensure_workspace(sc, virt->width, virt->height);
         Workspace& ws = *sc->ws;
-        DevTarget T;
-        fill_tables(sc, *virt, *params, T);
+        fill_tables(sc, *virt, *params);
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        check(cudaMemcpyAsync(ws.b.views, ws.host_views.data(), sizeof(DevView) * ws.host_views.size(),
-                              cudaMemcpyHostToDevice, s),
-              "upload view table");
-        check(cudaMemcpyAsync(ws.b.target, &T, sizeof(T), cudaMemcpyHostToDevice, s), "upload target");
         DebugPtrs dbg;
         if (dbg_out) {
             dbg.warped_uvz = dbg_out->warped_uvz;
@@ -300,7 +307,9 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
             dbg.blend_quality = dbg_out->blend_quality;
             dbg.inpaint_source = dbg_out->inpaint_source;
         }
-        int launches = launch_synthesis(ws.b, ws.shape, dbg, out->y, out->u, out->v, s);
+        int launches = launch_synthesis(ws.b, ws.table, ws.shape, dbg, out->y, out->u, out->v, s,
+                                        sc->profiling ? sc->events : nullptr);
+        sc->profiled = sc->profiling;
         if (launches < 0) check(cudaGetLastError(), "kernel launch");
         if (dbg.warped_uvz) {
             size_t off = 0;
@@ -375,7 +384,7 @@ rvsb_status rvsb_relative_pose(const rvsb_camera* input, const rvsb_camera* virt
 }
 
 rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs, rvsb_scene** out) {
-    if (!ctx || !inputs || !out || n_inputs <= 0 || n_inputs > 64) return RVSB_E_ARG;
+    if (!ctx || !inputs || !out || n_inputs <= 0 || n_inputs > MAX_VIEWS) return RVSB_E_ARG;
     *out = nullptr;
     return guarded(ctx, [&]() -> rvsb_status {
         check(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -451,6 +460,34 @@ rvsb_status rvsb_synthesize_debug(rvsb_scene* scene, const rvsb_camera* virt, co
 }
 
 int rvsb_scene_last_launch_count(const rvsb_scene* scene) { return scene ? scene->last_launches : 0; }
+
+rvsb_status rvsb_scene_set_profiling(rvsb_scene* sc, int enable) {
+    if (!sc) return RVSB_E_ARG;
+    return guarded(sc->ctx, [&]() -> rvsb_status {
+        check(cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+        if (enable && !sc->events[0])
+            for (auto& e : sc->events) check(cudaEventCreate(&e), "cudaEventCreate");
+        sc->profiling = enable != 0;
+        return RVSB_OK;
+    });
+}
+
+int rvsb_scene_stage_times(rvsb_scene* sc, float* ms, int max_stages) {
+    if (!sc || !ms || !sc->profiled) return -1;
+    const int n = std::min(max_stages, (int)NUM_STAGES);
+    for (int k = 0; k < n; ++k) {
+        if (cudaEventElapsedTime(&ms[k], sc->events[2 * k], sc->events[2 * k + 1]) != cudaSuccess) {
+            cudaGetLastError();
+            return -1;
+        }
+    }
+    return n;
+}
+
+const char* rvsb_stage_name(int stage) {
+    static const char* names[NUM_STAGES] = {"warp", "bin", "tile", "inpaint", "total"};
+    return (stage >= 0 && stage < NUM_STAGES) ? names[stage] : "";
+}
 
 rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs,
                                  const rvsb_view_planes* host_planes, const rvsb_camera* virt,

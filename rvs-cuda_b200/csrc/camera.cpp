@@ -101,7 +101,9 @@ const char* camera_problem(const rvsb_camera& c, bool as_output) {
         if (c.bit_depth_depth < 9 || c.bit_depth_depth > 16)
             return "depth bit depth must be 9..16 (16-bit samples)";
         if (!(c.depth_range[0] < c.depth_range[1])) return "inverted depth range";
-        if ((int64_t)(c.width - 1) * (c.height - 1) * 4 >= (int64_t)1 << 32) return "input too large";
+        int bits = 0;
+        while ((1 << bits) < c.width - 1) ++bits;
+        if (((int64_t)(c.height - 1) << (bits + 2)) > ((int64_t)1 << 32)) return "input too large";
     }
     if (c.projection == RVSB_PROJ_PERSPECTIVE && (c.focal[0] == 0.f || c.focal[1] == 0.f)) return "zero focal length";
     if (c.projection == RVSB_PROJ_EQUIRECTANGULAR &&

@@ -8,8 +8,8 @@ namespace rvsb {
 // Tiling constants.  A binning block is BLOCK_W x BLOCK_H quads of an input
 // view (each quad = two triangles, transform.cpp:159-176); an output tile is
 // TILE x TILE pixels whose 64-bit z-buffer lives in shared memory.
-constexpr int BLOCK_W = 16;
-constexpr int BLOCK_H = 8;
+constexpr int BLOCK_W = 8;
+constexpr int BLOCK_H = 4;
 constexpr int TILE = 32;
 constexpr int TILE_THREADS = 256;
 
@@ -34,7 +34,8 @@ struct DevView {
     float4* vert;                         // h*w warped vertices (u, v, z, 0)
     int4* bbox;                           // per binning block: x0, y0, x1, y1 (x0 > x1: empty)
     int nbx, nby;                         // binning blocks
-    int pad[2];
+    int tri_shift;                        // triangle index = i << tri_shift | j << 2 | t
+    int pad;
 };
 
 // Virtual camera of one synthesis.
@@ -48,10 +49,22 @@ struct DevTarget {
     unsigned max_val;                     // 2^bits - 1
     float blend_exp;                      // BlendingFactor
     float inv_blend_exp;                  // 1.0f / BlendingFactor
+    int blend_exp_int;                    // BlendingFactor when it is an integer in [2, 16], else 0
+    double lambda_mid;                    // midpoint of -1e-6f and the next float below it
     int ntx, nty;                         // output tiles
     int n_views;
     int bin_capacity;
 };
+
+// Largest number of input views of one synthesis; the whole table travels
+// as a kernel parameter (constant bank), not through global memory.
+constexpr int MAX_VIEWS = 16;
+
+struct ViewTable {
+    DevTarget t;
+    DevView v[MAX_VIEWS];
+};
+static_assert(sizeof(ViewTable) <= 4000, "kernel parameter space");
 
 // Status words written by the kernels (device memory, zeroed per call).
 struct DevStatus {

@@ -1,0 +1,377 @@
+// Inpainting stage: compute_nearest (rvs/src/inpainting.cpp:104-136) as two
+// sweeps of min-plus scans over the hole bounding box grown by one pixel,
+// then the fill of inpaint_color (inpainting.cpp:191-198) and the write of
+// the 2x2 output blocks that held holes.
+//
+// Why two sweeps of scans are exact: the reference alternates column-major
+// Gauss-Seidel sweeps (forward, then reverse) until one changes nothing.
+// After the forward sweep 0 and the reverse sweep 1 every distance equals
+// the L1 distance transform, so sweep 2 never changes anything and the
+// result is the state after sweep 1.  Each sweep is a min-plus recurrence
+// over left/up (or right/down) neighbours with a fixed neighbour priority:
+//  sweep 0: (D0, S0)(p) = lexmin over q with q.x <= p.x, q.y <= p.y of
+//           (C(q).d + |p - q|, C(q).source), C(q) = (0, q) for a non-hole,
+//           (1, down(q)) or else (1, right(q)) for a hole whose down/right
+//           neighbour is a non-hole;
+//  sweep 1: seeds T(q) = best of stay (D0, S0), left (D0 + 1, S0 of left),
+//           up (D0 + 1, S0 of up), in that priority (T'(q) without stay);
+//           a hole p takes the best seed of its lower-right quadrant, from
+//           its own column (smallest y) when the column holds a minimum,
+//           otherwise the minimum with the largest y, then smallest x, and
+//           changes only on strict improvement.
+#include "device_common.cuh"
+#include "kernels.hpp"
+
+namespace rvsb {
+namespace {
+
+using namespace dev;
+
+constexpr int kScanBias = 1 << 20;
+constexpr uint32_t kInfD = 0xFFFFFFFFu;
+
+struct Region {
+    int x0, y0, x1, y1;
+    bool empty;
+};
+
+__device__ __forceinline__ Region hole_region(const DevStatus* st, int wo, int ho) {
+    Region r;
+    r.empty = st->n_holes == 0;
+    r.x0 = max(0, st->hole_x0 - 1);
+    r.y0 = max(0, st->hole_y0 - 1);
+    r.x1 = min(wo - 1, st->hole_x1 + 1);
+    r.y1 = min(ho - 1, st->hole_y1 + 1);
+    return r;
+}
+
+__device__ __forceinline__ bool is_hole(const uint64_t* codes, int wo, int x, int y) {
+    return (codes[(size_t)y * wo + x] & kHoleBit) != 0;
+}
+
+__device__ __forceinline__ uint64_t pack_dxy(uint32_t d, int x, int y) {
+    return ((uint64_t)d << 32) | ((uint64_t)(uint32_t)x << 16) | (uint64_t)(uint32_t)y;
+}
+
+__device__ __forceinline__ unsigned long long warp_incl_min(unsigned long long v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v = y < v ? y : v;
+    }
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_incl_min_rev(unsigned long long v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_down_sync(0xffffffffu, v, o);
+        if (lane + o < 32) v = y < v ? y : v;
+    }
+    return v;
+}
+
+// Sweep 0, rows (forward): R(p) = lexmin over q.x <= p.x of
+// (C(q).d + p.x - q.x, C(q).src).  One warp per row of the region.
+__global__ void inpaint_row0_kernel(int wo, int ho, const DevStatus* __restrict__ st,
+                                    const uint64_t* __restrict__ codes, uint64_t* __restrict__ R) {
+    const Region rg = hole_region(st, wo, ho);
+    if (rg.empty) return;
+    const int lane = threadIdx.x & 31;
+    const int y = rg.y0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (y > rg.y1) return;
+    unsigned long long carry = kEmptyKey;
+    for (int base = rg.x0; base <= rg.x1; base += 32) {
+        const int x = base + lane;
+        unsigned long long key = kEmptyKey;
+        if (x <= rg.x1) {
+            uint32_t d = kInfD;
+            int sx = x, sy = y;
+            if (!is_hole(codes, wo, x, y)) {
+                d = 0;
+            } else if (y + 1 < ho && !is_hole(codes, wo, x, y + 1)) {
+                d = 1; sy = y + 1;
+            } else if (x + 1 < wo && !is_hole(codes, wo, x + 1, y)) {
+                d = 1; sx = x + 1;
+            }
+            if (d != kInfD) key = pack_dxy((uint32_t)((int)d - x + kScanBias), sx, sy);
+        }
+        key = warp_incl_min(key, lane);
+        key = key < carry ? key : carry;
+        if (x <= rg.x1) {
+            uint64_t out = ~0ull;
+            if (key != kEmptyKey)
+                out = pack_dxy((uint32_t)((int)(key >> 32) - kScanBias + x), (int)((key >> 16) & 0xffff),
+                               (int)(key & 0xffff));
+            R[(size_t)y * wo + x] = out;
+        }
+        carry = __shfl_sync(0xffffffffu, key, 31);
+    }
+}
+
+// Column scans: CTA = 32 columns x 32 row segments (one warp per segment).
+// Phase 1 reduces each segment, phase 2 rescans it with the carry of the
+// segments before it (above for forward scans, below for backward scans).
+
+// Sweep 0, columns (forward): D0, S0 (p) = lexmin over q.y <= p.y of
+// (R(q).d + p.y - q.y, src).  Output packed (D0, S0) per pixel.
+__device__ __forceinline__ unsigned long long col0_key(const uint64_t* R, int wo, int x, int y) {
+    const uint64_t r = R[(size_t)y * wo + x];
+    if (r == ~0ull) return kEmptyKey;
+    const int d = (int)(r >> 32);
+    return pack_dxy((uint32_t)(d - y + kScanBias), (int)((r >> 16) & 0xffff), (int)(r & 0xffff));
+}
+
+__global__ void __launch_bounds__(1024) inpaint_col0_kernel(int wo, int ho,
+                                                            const DevStatus* __restrict__ st,
+                                                            const uint64_t* __restrict__ codes,
+                                                            const uint64_t* __restrict__ R,
+                                                            uint64_t* __restrict__ DS) {
+    __shared__ unsigned long long seg[32][33];
+    const Region rg = hole_region(st, wo, ho);
+    if (rg.empty) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int x = rg.x0 + (int)blockIdx.x * 32 + lane;
+    if (rg.x0 + (int)blockIdx.x * 32 > rg.x1) return;
+    const int nrows = rg.y1 - rg.y0 + 1;
+    const int L = (nrows + 31) / 32;
+    const int yb = rg.y0 + w * L, ye = min(rg.y1, yb + L - 1);
+    const bool col_ok = x <= rg.x1;
+    unsigned long long m = kEmptyKey;
+    if (col_ok)
+        for (int y = yb; y <= ye; ++y) {
+            const unsigned long long k = col0_key(R, wo, x, y);
+            m = k < m ? k : m;
+        }
+    seg[w][lane] = m;
+    __syncthreads();
+    unsigned long long run = kEmptyKey;
+    for (int s = 0; s < w; ++s) run = seg[s][lane] < run ? seg[s][lane] : run;
+    if (!col_ok) return;
+    const uint32_t big = (uint32_t)(wo + ho);
+    for (int y = yb; y <= ye; ++y) {
+        const unsigned long long k = col0_key(R, wo, x, y);
+        run = k < run ? k : run;
+        uint64_t out;
+        if (!is_hole(codes, wo, x, y))
+            out = pack_dxy(0, x, y);
+        else if (run == kEmptyKey)
+            out = pack_dxy(big, x, y);
+        else
+            out = pack_dxy((uint32_t)((int)(run >> 32) - kScanBias + y), (int)((run >> 16) & 0xffff),
+                           (int)(run & 0xffff));
+        DS[(size_t)y * wo + x] = out;
+    }
+}
+
+// Packed (D0, S0) of pixel (x, y), or (0, itself) outside the region (a
+// non-hole: every hole lies inside the region).
+__device__ __forceinline__ uint64_t ds_at(const uint64_t* DS, const Region& rg, int wo, int x, int y) {
+    if (x < rg.x0 || x > rg.x1 || y < rg.y0 || y > rg.y1) return pack_dxy(0, x, y);
+    return DS[(size_t)y * wo + x];
+}
+
+// Sweep 1 seeds: T(q) = best of stay (D0(q), S0(q)), left (D0+1, S0 of left),
+// up (D0+1, S0 of up) with priority stay > left > up; T'(q) the same without
+// stay.  Non-holes: (0, q).
+__global__ void inpaint_seed1_kernel(int wo, int ho, const DevStatus* __restrict__ st,
+                                     const uint64_t* __restrict__ codes, const uint64_t* __restrict__ DS,
+                                     uint64_t* __restrict__ Tq, uint64_t* __restrict__ Tp) {
+    const Region rg = hole_region(st, wo, ho);
+    if (rg.empty) return;
+    const int x = rg.x0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = rg.y0 + (int)blockIdx.y;
+    if (x > rg.x1 || y > rg.y1) return;
+    const size_t o = (size_t)y * wo + x;
+    if (!is_hole(codes, wo, x, y)) {
+        Tq[o] = pack_dxy(0, x, y);
+        Tp[o] = pack_dxy(0, x, y);
+        return;
+    }
+    const uint64_t self = DS[o];
+    uint64_t best = self;
+    uint64_t bp = ~0ull;
+    if (x > 0) {
+        const uint64_t l = ds_at(DS, rg, wo, x - 1, y);
+        const uint64_t c = l + (1ull << 32);
+        if ((c >> 32) < (best >> 32)) best = c;
+        bp = c;
+    }
+    if (y > 0) {
+        const uint64_t u = ds_at(DS, rg, wo, x, y - 1);
+        const uint64_t c = u + (1ull << 32);
+        if ((c >> 32) < (best >> 32)) best = c;
+        if (bp == ~0ull || (c >> 32) < (bp >> 32)) bp = c;
+    }
+    Tq[o] = best;
+    Tp[o] = bp;
+}
+
+// Sweep 1, rows (backward, exclusive): RR(x, y) = min over q.x > x of
+// (T(q).d + q.x, q.x).  One warp per row.
+__global__ void inpaint_row1_kernel(int wo, int ho, const DevStatus* __restrict__ st,
+                                    const uint64_t* __restrict__ Tq, uint64_t* __restrict__ RR) {
+    const Region rg = hole_region(st, wo, ho);
+    if (rg.empty) return;
+    const int lane = threadIdx.x & 31;
+    const int y = rg.y0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (y > rg.y1) return;
+    unsigned long long carry = kEmptyKey;
+    const int n = rg.x1 - rg.x0 + 1;
+    for (int base = 0; base < n; base += 32) {
+        // process x from the right end: x = x1 - (base + lane)
+        const int x = rg.x1 - (base + (31 - lane));
+        unsigned long long key = kEmptyKey;
+        if (x >= rg.x0) {
+            const uint64_t t = Tq[(size_t)y * wo + x];
+            key = ((unsigned long long)((t >> 32) + (uint64_t)x) << 16) | (unsigned long long)x;
+        }
+        // lane 31 holds the rightmost x of this chunk; suffix min towards lane 0
+        unsigned long long incl = warp_incl_min_rev(key, lane);
+        incl = incl < carry ? incl : carry;
+        // exclusive: the value of lane + 1, or the carry for lane 31
+        unsigned long long excl = __shfl_down_sync(0xffffffffu, incl, 1);
+        if (lane == 31) excl = carry;
+        if (x >= rg.x0) RR[(size_t)y * wo + x] = excl;
+        carry = __shfl_sync(0xffffffffu, incl, 0);
+    }
+}
+
+// Sweep 1, columns (backward): for each hole p choose its sweep-1 source
+// and copy that pixel's codes (the fill of inpaint_color,
+// inpainting.cpp:191-198).
+__global__ void __launch_bounds__(1024) inpaint_col1_kernel(
+    int wo, int ho, const DevStatus* __restrict__ st, uint64_t* __restrict__ codes,
+    const uint64_t* __restrict__ DS, const uint64_t* __restrict__ Tq, const uint64_t* __restrict__ Tp,
+    const uint64_t* __restrict__ RR, int32_t* __restrict__ dbg_source) {
+    __shared__ unsigned long long seg_col[32][33];
+    __shared__ unsigned long long seg_off[32][33];
+    const Region rg = hole_region(st, wo, ho);
+    if (rg.empty) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int x = rg.x0 + (int)blockIdx.x * 32 + lane;
+    if (rg.x0 + (int)blockIdx.x * 32 > rg.x1) return;
+    const bool col_ok = x <= rg.x1;
+    const int nrows = rg.y1 - rg.y0 + 1;
+    const int L = (nrows + 31) / 32;
+    const int yb = rg.y0 + w * L, ye = min(rg.y1, yb + L - 1);
+    // Keys: column part (T.d + y) << 16 | y (minimum y on ties);
+    //       off-column (RR.d - x + y) << 32 | (0xffff - y) << 16 | qx
+    //       (largest y, then smallest x on ties).
+    auto col_key = [&](int y) -> unsigned long long {
+        const uint64_t t = Tq[(size_t)y * wo + x];
+        return ((unsigned long long)((t >> 32) + (uint64_t)y) << 16) | (unsigned long long)y;
+    };
+    auto off_key = [&](int y) -> unsigned long long {
+        const uint64_t r = RR[(size_t)y * wo + x];
+        if (r == kEmptyKey) return kEmptyKey;
+        const uint64_t v = (r >> 16) - (uint64_t)x + (uint64_t)y;
+        return (v << 32) | ((uint64_t)(0xffff - y) << 16) | (r & 0xffff);
+    };
+    unsigned long long mc = kEmptyKey, mo = kEmptyKey;
+    if (col_ok)
+        for (int y = yb; y <= ye; ++y) {
+            const unsigned long long a = col_key(y), b = off_key(y);
+            mc = a < mc ? a : mc;
+            mo = b < mo ? b : mo;
+        }
+    seg_col[w][lane] = mc;
+    seg_off[w][lane] = mo;
+    __syncthreads();
+    unsigned long long run_c = kEmptyKey, run_o = kEmptyKey;
+    for (int s = w + 1; s < 32; ++s) {
+        run_c = seg_col[s][lane] < run_c ? seg_col[s][lane] : run_c;
+        run_o = seg_off[s][lane] < run_o ? seg_off[s][lane] : run_o;
+    }
+    if (!col_ok) return;
+    for (int y = ye; y >= yb; --y) {
+        // run_c holds the exclusive (rows below) column minimum here.
+        const unsigned long long ok = off_key(y);
+        run_o = ok < run_o ? ok : run_o;
+        const size_t o = (size_t)y * wo + x;
+        const uint64_t code = codes[o];
+        if (code & kHoleBit) {
+            const uint64_t tp = Tp[o];
+            // column candidate (cost, y)
+            uint64_t c_cost = tp == ~0ull ? (uint64_t)1 << 40 : (tp >> 32);
+            int c_y = y;
+            if (run_c != kEmptyKey) {
+                const uint64_t cost = (run_c >> 16) - (uint64_t)y;
+                if (cost < c_cost) {
+                    c_cost = cost;
+                    c_y = (int)(run_c & 0xffff);
+                }
+            }
+            uint64_t o_cost = (uint64_t)1 << 40;
+            int o_x = 0, o_y = 0;
+            if (run_o != kEmptyKey) {
+                o_cost = (run_o >> 32) - (uint64_t)y;
+                o_y = 0xffff - (int)((run_o >> 16) & 0xffff);
+                o_x = (int)(run_o & 0xffff);
+            }
+            const uint64_t ds = DS[o];
+            const uint64_t d0 = ds >> 32;
+            uint64_t src = ds;
+            if (c_cost <= o_cost) {
+                if (c_cost < d0) src = (c_y == y) ? tp : Tq[(size_t)c_y * wo + x];
+            } else {
+                if (o_cost < d0) src = Tq[(size_t)o_y * wo + o_x];
+            }
+            const int sx = (int)((src >> 16) & 0xffff), sy = (int)(src & 0xffff);
+            codes[o] = (codes[(size_t)sy * wo + sx] & kCodeMask) | kHoleBit;
+            if (dbg_source) {
+                dbg_source[o * 2 + 0] = sx;
+                dbg_source[o * 2 + 1] = sy;
+            }
+        }
+        const unsigned long long ck = col_key(y);
+        run_c = ck < run_c ? ck : run_c;
+    }
+}
+
+// Writes the 2x2 output blocks of the region that hold at least one hole.
+__global__ void inpaint_write_kernel(int wo, int ho, const DevStatus* __restrict__ st,
+                                     const uint64_t* __restrict__ codes, uint16_t* __restrict__ out_y,
+                                     uint16_t* __restrict__ out_u, uint16_t* __restrict__ out_v) {
+    const Region rg = hole_region(st, wo, ho);
+    if (rg.empty) return;
+    const int bx0 = rg.x0 / 2, by0 = rg.y0 / 2;
+    const int x = 2 * (bx0 + (int)(blockIdx.x * blockDim.x + threadIdx.x));
+    const int y = 2 * (by0 + (int)blockIdx.y);
+    if (x > rg.x1 || y > rg.y1 || x >= wo || y >= ho) return;
+    const size_t o = (size_t)y * wo + x;
+    const uint64_t c00 = codes[o], c01 = codes[o + 1], c10 = codes[o + wo], c11 = codes[o + wo + 1];
+    if (!((c00 | c01 | c10 | c11) & kHoleBit)) return;
+    out_y[o] = (uint16_t)(c00 & 0xffff);
+    out_y[o + 1] = (uint16_t)(c01 & 0xffff);
+    out_y[o + wo] = (uint16_t)(c10 & 0xffff);
+    out_y[o + wo + 1] = (uint16_t)(c11 & 0xffff);
+    const size_t co = (size_t)(y / 2) * (wo / 2) + x / 2;
+    const uint32_t su = (uint32_t)((c00 >> 16) & 0xffff) + ((c01 >> 16) & 0xffff) + ((c10 >> 16) & 0xffff) +
+                        ((c11 >> 16) & 0xffff);
+    const uint32_t sv = (uint32_t)((c00 >> 32) & 0xffff) + ((c01 >> 32) & 0xffff) + ((c10 >> 32) & 0xffff) +
+                        ((c11 >> 32) & 0xffff);
+    out_u[co] = (uint16_t)((su + 2) >> 2);
+    out_v[co] = (uint16_t)((sv + 2) >> 2);
+}
+
+
+}  // namespace
+
+void launch_inpaint(const SynthBuffers& b, const LaunchShape& sh, const DebugPtrs& dbg, uint16_t* out_y,
+                    uint16_t* out_u, uint16_t* out_v, cudaStream_t s) {
+    const int rows_per_cta = 8;  // 8 warps of 32
+    inpaint_row0_kernel<<<(sh.ho + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(sh.wo, sh.ho, b.status, b.codes,
+                                                                                  b.scan_a);
+    inpaint_col0_kernel<<<(sh.wo + 31) / 32, 1024, 0, s>>>(sh.wo, sh.ho, b.status, b.codes, b.scan_a, b.scan_b);
+    inpaint_seed1_kernel<<<dim3((sh.wo + 255) / 256, sh.ho), 256, 0, s>>>(sh.wo, sh.ho, b.status, b.codes, b.scan_b,
+                                                                        b.scan_c, b.scan_d);
+    inpaint_row1_kernel<<<(sh.ho + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(sh.wo, sh.ho, b.status, b.scan_c,
+                                                                                  b.scan_a);
+    inpaint_col1_kernel<<<(sh.wo + 31) / 32, 1024, 0, s>>>(sh.wo, sh.ho, b.status, b.codes, b.scan_b, b.scan_c,
+                                                          b.scan_d, b.scan_a, dbg.inpaint_source);
+    inpaint_write_kernel<<<dim3((sh.wo / 2 + 127) / 128, (sh.ho + 1) / 2), 128, 0, s>>>(sh.wo, sh.ho, b.status,
+                                                                                      b.codes, out_y, out_u, out_v);
+}
+
+}  // namespace rvsb

@@ -10,8 +10,6 @@ namespace rvsb {
 
 // Device buffers of one synthesis workspace.
 struct SynthBuffers {
-    DevView* views = nullptr;      // n_views entries (device)
-    DevTarget* target = nullptr;   // 1 entry (device)
     DevStatus* status = nullptr;   // 1 entry (device)
     int* counts = nullptr;         // ntiles * n_views
     int* offsets = nullptr;        // ntiles * n_views
@@ -47,14 +45,17 @@ struct LaunchShape {
     int max_blocks;          // largest nbx * nby
     int wo, ho;
     int ntx, nty;
-    int input_w[64];         // per view (for the debug copy of warped vertices)
-    int input_h[64];
-    int64_t vert_offset[64]; // element offset of each view's vertices in the vertex arena
+    int input_w[MAX_VIEWS];  // per view (for the debug copy of warped vertices)
+    int input_h[MAX_VIEWS];
+    int64_t vert_offset[MAX_VIEWS];  // element offset of each view's vertices in the vertex arena
 };
 
 // Issues the whole synthesis on `stream`; returns the number of kernel
 // launches, or -1 on a launch error (cudaGetLastError holds the cause).
-int launch_synthesis(const SynthBuffers& b, const LaunchShape& shape, const DebugPtrs& dbg,
-                     uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t stream);
+// `events` (optional) holds 2 * NUM_STAGES events recorded around the stages.
+constexpr int NUM_STAGES = 5;
+int launch_synthesis(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& shape, const DebugPtrs& dbg,
+                     uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t stream,
+                     cudaEvent_t* events = nullptr);
 
 }  // namespace rvsb

@@ -25,8 +25,11 @@ EXPORTED = [
     "rvsb_config_texture_path", "rvsb_config_depth_path", "rvsb_config_output_path", "rvsb_config_frames",
     "rvsb_config_synth_params", "rvsb_config_virtual_camera_at", "rvsb_relative_pose", "rvsb_scene_create",
     "rvsb_scene_destroy", "rvsb_scene_upload", "rvsb_synthesize", "rvsb_synthesize_host",
-    "rvsb_synthesize_debug", "rvsb_scene_last_launch_count",
+    "rvsb_synthesize_debug", "rvsb_scene_last_launch_count", "rvsb_scene_set_profiling",
+    "rvsb_scene_stage_times", "rvsb_stage_name",
 ]
+
+STAGES = ["warp", "bin", "tile", "inpaint", "total"]
 
 _lib = None
 
@@ -82,6 +85,10 @@ def load():
                                        P(SynthParams), P(Yuv420), c_p]
     L.rvsb_synthesize_debug.argtypes = [c_p, P(Camera), P(SynthParams), P(Yuv420), P(DebugOut), c_p]
     L.rvsb_scene_last_launch_count.argtypes = [c_p]
+    L.rvsb_scene_set_profiling.argtypes = [c_p, ctypes.c_int]
+    L.rvsb_scene_stage_times.argtypes = [c_p, P(ctypes.c_float), ctypes.c_int]
+    L.rvsb_stage_name.argtypes = [ctypes.c_int]
+    L.rvsb_stage_name.restype = ctypes.c_char_p
     _lib = L
     return L
 
@@ -175,6 +182,17 @@ class Scene:
 
     def last_launch_count(self):
         return self.ctx.lib.rvsb_scene_last_launch_count(self.h)
+
+    def set_profiling(self, on=True):
+        return self.ctx.check(self.ctx.lib.rvsb_scene_set_profiling(self.h, 1 if on else 0))
+
+    def stage_times(self):
+        """{stage: ms} of the last profiled synthesis (stream must be complete)."""
+        buf = (ctypes.c_float * len(STAGES))()
+        n = self.ctx.lib.rvsb_scene_stage_times(self.h, buf, len(STAGES))
+        if n < 0:
+            raise RvsbError(-1, "no profiled synthesis")
+        return {STAGES[i]: buf[i] for i in range(n)}
 
     def close(self):
         if self.h:

@@ -25,9 +25,6 @@ import numpy as np
 
 from . import abi
 
-_MASK64 = np.uint64(0xFFFFFFFFFFFFFFFF)
-
-
 def rotation_matrix(rot_deg):
     """Rz(yaw) * Ry(pitch) * Rx(roll), float64 (camera -> world)."""
     a, b, c = (math.radians(float(x)) for x in rot_deg)
@@ -35,49 +32,6 @@ def rotation_matrix(rot_deg):
     ry = np.array([[math.cos(b), 0, math.sin(b)], [0, 1, 0], [-math.sin(b), 0, math.cos(b)]])
     rx = np.array([[1, 0, 0], [0, math.cos(c), -math.sin(c)], [0, math.sin(c), math.cos(c)]])
     return rz @ ry @ rx
-
-
-def _mix64(h):
-    h = h ^ (h >> np.uint64(33))
-    h = h * np.uint64(0xFF51AFD7ED558CCD)
-    h = h ^ (h >> np.uint64(33))
-    h = h * np.uint64(0xC4CEB9FE1A85EC53)
-    h = h ^ (h >> np.uint64(33))
-    return h
-
-
-def _lattice(ix, iy, iz, seed):
-    h = (ix.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)) ^ \
-        (iy.astype(np.uint64) * np.uint64(0xC2B2AE3D27D4EB4F)) ^ \
-        (iz.astype(np.uint64) * np.uint64(0x165667B19E3779F9)) ^ np.uint64(seed)
-    h = _mix64(h)
-    return (h >> np.uint64(40)).astype(np.float32) * np.float32(1.0 / (1 << 24))
-
-
-def value_noise(p, seed, octaves=4, base_freq=2.0):
-    """Fractal 3-D value noise in [0, 1] at points p (N, 3)."""
-    total = np.zeros(p.shape[0], np.float32)
-    amp, norm, freq = 1.0, 0.0, base_freq
-    for o in range(octaves):
-        q = p * freq
-        f = np.floor(q)
-        t = (q - f).astype(np.float32)
-        t = t * t * (3 - 2 * t)
-        i0 = f.astype(np.int64)
-        acc = np.zeros(p.shape[0], np.float32)
-        for dz in (0, 1):
-            wz = t[:, 2] if dz else 1 - t[:, 2]
-            for dy in (0, 1):
-                wy = t[:, 1] if dy else 1 - t[:, 1]
-                for dx in (0, 1):
-                    wx = t[:, 0] if dx else 1 - t[:, 0]
-                    v = _lattice(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz, seed + 7919 * o)
-                    acc += wx * wy * wz * v
-        total += amp * acc
-        norm += amp
-        amp *= 0.5
-        freq *= 2.0
-    return total / norm
 
 
 class Rng:
@@ -123,118 +77,56 @@ class Scene:
         v = np.cross(n, u)
         self.rects.append((np.asarray(center, float), u * half_u, v * half_v, n))
 
-    def intersect(self, origin, dirs):
-        """Closest positive hit distance along dirs (N, 3) from origin; inf on miss."""
-        n = dirs.shape[0]
-        best = np.full(n, np.inf)
-        for c, au, av, nn in self.rects:
-            denom = dirs @ nn
-            with np.errstate(divide="ignore", invalid="ignore"):
-                s = ((c - origin) @ nn) / denom
-            hit = origin + s[:, None] * dirs - c
-            lu = (hit @ au) / (au @ au)
-            lv = (hit @ av) / (av @ av)
-            ok = (s > 1e-6) & (np.abs(lu) <= 1) & (np.abs(lv) <= 1) & (s < best)
-            best = np.where(ok, s, best)
-        for c, r in self.spheres:
-            oc = origin - c
-            b = dirs @ oc
-            a = np.einsum("ij,ij->i", dirs, dirs)
-            cc = oc @ oc - r * r
-            disc = b * b - a * cc
-            with np.errstate(invalid="ignore", divide="ignore"):
-                sq = np.sqrt(np.maximum(disc, 0))
-                s0 = (-b - sq) / a
-                s1 = (-b + sq) / a
-            s = np.where(s0 > 1e-6, s0, s1)
-            ok = (disc >= 0) & (s > 1e-6) & (s < best)
-            best = np.where(ok, s, best)
-        for lo, hi, inward in self.boxes:
-            with np.errstate(divide="ignore", invalid="ignore"):
-                t1 = (lo - origin) / dirs
-                t2 = (hi - origin) / dirs
-            tmin = np.nanmax(np.minimum(t1, t2), axis=1)
-            tmax = np.nanmin(np.maximum(t1, t2), axis=1)
-            s = tmax if inward else tmin
-            ok = (tmax >= tmin) & (s > 1e-6) & (s < best)
-            best = np.where(ok, s, best)
-        return best
 
-    def shade(self, pts):
-        """YUV in [0, 1] at world points (N, 3)."""
-        y = 0.12 + 0.76 * value_noise(pts, self.seed ^ 0x1111)
-        u = 0.5 + 0.36 * (value_noise(pts * 0.7, self.seed ^ 0x2222, octaves=3) - 0.5)
-        v = 0.5 + 0.36 * (value_noise(pts * 0.7 + 3.1, self.seed ^ 0x3333, octaves=3) - 0.5)
-        for c, r, col in self.patches:
-            inside = np.sum((pts - c) ** 2, axis=1) <= r * r
-            y = np.where(inside, col[0], y)
-            u = np.where(inside, col[1], u)
-            v = np.where(inside, col[2], v)
-        return np.stack([y, u, v], axis=1).astype(np.float64)
+_sg = None
 
 
-def camera_rays(cam):
-    """Unit-or-forward-normalised ray directions (H*W, 3) in world space and
-    the factor that converts hit distance to the depth the camera stores."""
+def _scenegen():
+    """ctypes handle of libscenegen.so (the C++ ray caster, built by build.py)."""
+    global _sg
+    if _sg is None:
+        import ctypes
+        path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "lib",
+                            "libscenegen.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing (run rvs-cuda_b200/build.py)")
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        L.sg_render.argtypes = [P, P, P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int,
+                                ctypes.c_uint64, P, P, P, P]
+        _sg = L
+    return _sg
+
+
+def render(scene, cam):
+    """Renders (Y, U, V, depth) uint16 planes of camera `cam`: per pixel the
+    closest hit along the camera ray (perspective: x component 1, so hit
+    distance = stored depth; ERP: unit rays, hit distance = radius), misses
+    at the far plane, value-noise texture, 2x2-averaged chroma and the
+    normalised-disparity depth encoding."""
     w, h = cam.width, cam.height
-    jj, ii = np.meshgrid(np.arange(w, dtype=np.float64) + 0.5, np.arange(h, dtype=np.float64) + 0.5)
-    if cam.projection == abi.PERSPECTIVE:
-        x = np.ones_like(jj)
-        yl = -(jj - cam.principle_point[0]) / cam.focal[0]
-        zl = -(ii - cam.principle_point[1]) / cam.focal[1]
-        local = np.stack([x, yl, zl], axis=-1).reshape(-1, 3)
-    else:
-        ii = ii.copy()
-        ii[0, :] = 1e-3
-        ii[-1, :] = h - 1e-3
-        rpd = math.pi / 180.0
-        phi = rpd * cam.hor_range[1] - rpd * (cam.hor_range[1] - cam.hor_range[0]) / w * jj
-        theta = rpd * cam.ver_range[1] - rpd * (cam.ver_range[1] - cam.ver_range[0]) / h * ii
-        local = np.stack([np.cos(theta) * np.cos(phi), np.cos(theta) * np.sin(phi),
-                          np.sin(theta)], axis=-1).reshape(-1, 3)
+    ci = np.array([cam.projection, w, h, cam.bit_depth_color, cam.bit_depth_depth], np.int32)
     R = rotation_matrix(cam.rotation)
-    return local @ R.T
-
-
-def render(scene, cam, chunk=1 << 20):
-    """Renders (Y, U, V, depth) uint16 planes of camera `cam`."""
-    w, h = cam.width, cam.height
-    origin = np.array(list(cam.position), float)
-    dirs = camera_rays(cam)
-    near, far = float(cam.depth_range[0]), float(cam.depth_range[1])
-    z = np.empty(w * h)
-    yuv = np.empty((w * h, 3))
-    for s in range(0, w * h, chunk):
-        d = dirs[s:s + chunk]
-        t = scene.intersect(origin, d)
-        miss = ~np.isfinite(t)
-        t = np.where(miss, np.inf, t)
-        # Distance along the ray equals the stored depth: the forward
-        # coordinate for perspective rays (x component 1), the radius for ERP.
-        zz = np.where(miss, far, np.minimum(t, far))
-        z[s:s + chunk] = zz
-        pts = origin + d * np.where(miss, far, t)[:, None]
-        yuv[s:s + chunk] = scene.shade(pts)
-    maxc = (1 << cam.bit_depth_color) - 1
-    yuv = np.clip(yuv, 0, 1).reshape(h, w, 3)
-    Y = np.round(yuv[:, :, 0] * maxc).astype(np.uint16)
-    ch = yuv[:, :, 1:].reshape(h // 2, 2, w // 2, 2, 2).mean(axis=(1, 3))
-    U = np.round(ch[:, :, 0] * maxc).astype(np.uint16)
-    V = np.round(ch[:, :, 1] * maxc).astype(np.uint16)
-    z = z.reshape(h, w)
-    maxd = (1 << cam.bit_depth_depth) - 1
-    if far >= 1000.0:
-        dn = near / z
-    else:
-        dn = (far * near / z - near) / (far - near)
-    D = np.round(np.clip(dn, 0, 1) * maxd).astype(np.uint16)
+    cd = np.array(list(cam.position) + list(R.ravel()) + list(cam.focal) + list(cam.principle_point) +
+                  list(cam.hor_range) + list(cam.ver_range) + [cam.depth_range[0], cam.depth_range[1]],
+                  np.float64)
+    rects = np.array([np.concatenate([c, au, av, n]) for c, au, av, n in scene.rects],
+                     np.float64).reshape(-1, 12)
+    sph = np.array([np.concatenate([c, [r]]) for c, r in scene.spheres], np.float64).reshape(-1, 4)
+    boxes = np.array([np.concatenate([lo, hi, [1.0 if inward else 0.0]]) for lo, hi, inward in scene.boxes],
+                     np.float64).reshape(-1, 7)
+    pat = np.array([np.concatenate([c, [r], col]) for c, r, col in scene.patches], np.float64).reshape(-1, 7)
+    Y = np.empty((h, w), np.uint16)
+    U = np.empty((h // 2, w // 2), np.uint16)
+    V = np.empty((h // 2, w // 2), np.uint16)
+    D = np.empty((h, w), np.uint16)
+    rc = _scenegen().sg_render(ci.ctypes.data, cd.ctypes.data, rects.ctypes.data, len(rects), sph.ctypes.data,
+                               len(sph), boxes.ctypes.data, len(boxes), pat.ctypes.data, len(pat),
+                               scene.seed & 0xFFFFFFFFFFFFFFFF, Y.ctypes.data, U.ctypes.data, V.ctypes.data,
+                               D.ctypes.data)
+    if rc != 0:
+        raise ValueError("scene render failed (odd or empty resolution)")
     return Y, U, V, D
-
-
-def _add_patches(scene, rng, n, lo, hi):
-    for _ in range(n):
-        scene.patches.append((rng.vec(lo, hi), rng.uniform(0.15, 0.45),
-                              (rng.uniform(0.1, 0.9), rng.uniform(0.3, 0.7), rng.uniform(0.3, 0.7))))
 
 
 def _front_scene(seed, n_planes, n_spheres, dmin, dmax, spread):
