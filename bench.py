@@ -2,7 +2,9 @@
 
 Default workload (N=1): 4 perspective inputs 1920x1080 (10-bit YUV420, 16-bit
 depth) -> 1 perspective 1920x1080 view, seeded synthetic scene.  A step is
-one synthesis of the virtual view from the resident raw input planes.
+one synthesis of the virtual view from raw input planes resident in HBM:
+loading the four views into the scene (copy + colour decode, the
+reference's per-frame InputView::load) and synthesising.
 
   value  views/s with the input planes resident in HBM (device-timed with
          CUDA events around each synthesis; L2 flushed between steps).
@@ -238,10 +240,13 @@ def main():
     scene.set_profiling(True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
+    def plain_step():
+        scene.synthesize_frame(dev_planes, target, p, out, stream=stream)
+
     sampler = ClockSampler(local)
     sampler.start()
     for _ in range(args.warmup):
-        scene.synthesize(target, p, out, stream=stream)
+        plain_step()
     torch.cuda.synchronize()
     launches_per_step = scene.last_launch_count()
 
@@ -252,7 +257,7 @@ def main():
     for k in range(args.steps):
         flush.zero_()  # L2 flush (256 MiB > 126 MB L2), outside the timed events
         ev[k][0].record(stream)
-        scene.synthesize(target, p, out, stream=stream)
+        plain_step()
         ev[k][1].record(stream)
         ev[k][1].synchronize()
         for name, ms in scene.stage_times().items():
@@ -292,16 +297,20 @@ def main():
     n_in = sum(c.width * c.height for c in wl.inputs)
     n_out = wo * ho
     stage_avg = {k: v / args.steps for k, v in stage_acc.items()}
+    stage_avg["upload_decode"] = statistics.mean(step_ms) - stage_avg["total"]
+    # Algorithmic bytes per launch: warp 14 B per input pixel (depth read +
+    # warped u, v, z write); blend (10N + 4) B per output pixel (per view
+    # colour 3 x u16 + weight fp32, output YUV420 + mask); the raster reads
+    # the warped mesh, 12 B per input pixel.
     algorithmic = {
-        # SURVEY-defined figures: warp 14 B per input pixel; blend (10N + 4) B
-        # per output pixel; the tile kernel also reads the warped mesh
-        # (12 B per input pixel) for its raster.
         "warp": 14 * n_in,
-        "tile": 12 * n_in + (10 * n_views + 4) * n_out,
+        "raster": 12 * n_in,
+        "resolve": (10 * n_views + 4) * n_out,
     }
-    dominant = max(("warp", "tile", "inpaint", "bin"), key=lambda k: stage_avg[k])
+    kernel_names = {"warp": "warp_kernel", "raster": "raster_kernel", "resolve": "resolve_kernel"}
+    dominant = max(("warp", "bin", "raster", "resolve", "inpaint"), key=lambda k: stage_avg[k])
     peak, peak_kind = measured_peaks()
-    rk = dominant if dominant in algorithmic else "tile"
+    rk = dominant if dominant in algorithmic else "raster"
     achieved = algorithmic[rk] / (stage_avg[rk] / 1000.0) / 1e9
     traffic = None
     prof_path = os.path.join(ROOT, "profiles", "tile_kernel_traffic.json")
@@ -310,7 +319,7 @@ def main():
             traffic = json.load(open(prof_path)).get(rk)
         except Exception:
             traffic = None
-    roofline = {"kernel": {"tile": "tile_kernel", "warp": "warp_kernel"}[rk], "bound": "hbm",
+    roofline = {"kernel": kernel_names[rk], "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": algorithmic[rk], "ms_per_launch": stage_avg[rk],
@@ -318,6 +327,12 @@ def main():
     stage_roof = {k: {"ms": stage_avg[k], "GBs": algorithmic[k] / (stage_avg[k] / 1000.0) / 1e9,
                       "frac": algorithmic[k] / (stage_avg[k] / 1000.0) / 1e9 / peak}
                   for k in algorithmic}
+    blend_ms = stage_avg["resolve"] + stage_avg["inpaint"]
+    stage_roof["blend_inpaint_write"] = {
+        "ms": blend_ms, "GBs": algorithmic["resolve"] / (blend_ms / 1000.0) / 1e9,
+        "frac": algorithmic["resolve"] / (blend_ms / 1000.0) / 1e9 / peak}
+    triangles = 2 * sum((c.width - 1) * (c.height - 1) for c in wl.inputs)
+    stage_roof["raster"]["triangles_per_s"] = triangles / (stage_avg["raster"] / 1000.0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -214,6 +214,16 @@ rvsb_status rvsb_synthesize(rvsb_scene* scene, const rvsb_camera* virt,
                             const rvsb_synth_params* params, const rvsb_yuv420* out,
                             void* stream);
 
+/* One frame of the reference's per-frame path with the raw input planes
+ * already in device memory (the InputView::load + computeView pair of
+ * rvs/src/Pipeline.cpp:215-285): decodes every view's colour from
+ * `device_planes` (n = the scene's view count) into the scene, reads their
+ * depth planes in place and synthesises `virt` into `out`.  No plane is
+ * copied; the planes must stay valid until the work on `stream` is done. */
+rvsb_status rvsb_synthesize_frame(rvsb_scene* scene, const rvsb_view_planes* device_planes,
+                                  const rvsb_camera* virt, const rvsb_synth_params* params,
+                                  const rvsb_yuv420* out, void* stream);
+
 /* The same call with host buffers on both sides (the reference's plain
  * per-frame path): uploads the n raw input views from host memory,
  * synthesises, and copies the YUV420 result back into host memory.  Blocks
@@ -256,9 +266,9 @@ int rvsb_scene_last_launch_count(const rvsb_scene* scene);
 
 /* Per-stage timing with CUDA events recorded on the launch stream (the
  * per-stage timers that replace the reference's whole-run clock(),
- * rvs/src/view_synthesis.cpp:149-166).  Stages: 0 warp, 1 bin, 2 tile
- * (raster + resolve + blend + quantise), 3 inpaint, 4 whole synthesis. */
-#define RVSB_NUM_STAGES 5
+ * rvs/src/view_synthesis.cpp:149-166).  Stages: 0 warp, 1 bin, 2 raster,
+ * 3 inpaint, 4 whole synthesis, 5 resolve (+ blend + quantise). */
+#define RVSB_NUM_STAGES 6
 rvsb_status rvsb_scene_set_profiling(rvsb_scene* scene, int enable);
 /* Milliseconds per stage of the most recent profiled synthesis; call after
  * its stream has completed.  Returns the number of values written, or -1. */

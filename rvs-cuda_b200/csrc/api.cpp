@@ -81,7 +81,7 @@ struct DevMem {
 
 struct Workspace {
     int wo = 0, ho = 0;
-    DevMem status, counts, offsets, cursor, list, codes, scan[4], vert, bbox;
+    DevMem status, counts, offsets, cursor, list, keys, codes, holes, scan[4], vert, bbox;
     SynthBuffers b;
     LaunchShape shape{};
     ViewTable table{};
@@ -95,6 +95,7 @@ struct rvsb_scene {
     std::vector<rvsb_camera> cams;
     std::vector<std::unique_ptr<DevMem>> planes;  // 4 per view: y, u, v, depth
     std::vector<std::unique_ptr<DevMem>> erp;     // 2 per view: rows, cols (ERP inputs)
+    std::vector<std::unique_ptr<DevMem>> color;   // 1 per view: decoded colour words
     std::vector<bool> uploaded;
     std::unique_ptr<Workspace> ws;
     int last_launches = 0;
@@ -176,7 +177,9 @@ void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
     ws->cursor.alloc(ctx, nbins * sizeof(int));
     ws->list.alloc(ctx, (size_t)capacity * sizeof(int));
     const size_t npix = (size_t)wo * ho;
+    ws->keys.alloc(ctx, npix * n * sizeof(uint64_t));
     ws->codes.alloc(ctx, npix * sizeof(uint64_t));
+    ws->holes.alloc(ctx, npix);
     for (auto& s : ws->scan) s.alloc(ctx, npix * sizeof(uint64_t));
     SynthBuffers& b = ws->b;
     b.status = ws->status.as<DevStatus>();
@@ -185,7 +188,9 @@ void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
     b.cursor = ws->cursor.as<int>();
     b.list = ws->list.as<int>();
     b.capacity = capacity;
+    b.keys = ws->keys.as<uint64_t>();
     b.codes = ws->codes.as<uint64_t>();
+    b.holes = ws->holes.as<uint8_t>();
     b.scan_a = ws->scan[0].as<uint64_t>();
     b.scan_b = ws->scan[1].as<uint64_t>();
     b.scan_c = ws->scan[2].as<uint64_t>();
@@ -240,6 +245,7 @@ void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_param
             V.erp_row = sc->erp[v * 2 + 0]->as<float>();
             V.erp_col = sc->erp[v * 2 + 1]->as<float>();
         }
+        V.color = sc->color[v]->as<uint64_t>();
         V.vert = ws.vert.as<float4>() + ws.vert_off[v];
         V.bbox = ws.bbox.as<int4>() + ws.bbox_off[v];
         V.tri_shift = 2;
@@ -265,10 +271,7 @@ void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_param
     T.blend_exp_int = 0;
     if (p.blending_factor == std::floor(p.blending_factor) && p.blending_factor >= 2.f && p.blending_factor <= 16.f)
         T.blend_exp_int = (int)p.blending_factor;
-    {
-        const float t = -1e-6f;
-        T.lambda_mid = ((double)t + (double)std::nextafter(t, -INFINITY)) / 2.0;
-    }
+
     T.ntx = ws.shape.ntx;
     T.nty = ws.shape.nty;
     T.n_views = n;
@@ -282,21 +285,40 @@ void validate_params(const rvsb_synth_params* p) {
     if (p->precision != 1.f) throw Unsupported("Precision other than 1 is not supported");
 }
 
+// `frame` (optional): raw device planes of every input view for this call;
+// their colour is decoded into the scene and their depth read in place.
 rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_synth_params* params,
-                            const rvsb_yuv420* out, const rvsb_debug_out* dbg_out, void* stream) {
+                            const rvsb_yuv420* out, const rvsb_debug_out* dbg_out, void* stream,
+                            const rvsb_view_planes* frame = nullptr) {
     if (!sc) return RVSB_E_ARG;
     rvsb_context* ctx = sc->ctx;
     return guarded(ctx, [&]() -> rvsb_status {
         if (!virt || !out || !out->y || !out->u || !out->v) throw ArgError("null camera or output planes");
         validate_params(params);
         if (const char* why = camera_problem(*virt, true)) throw ArgError(std::string("virtual camera: ") + why);
-        for (size_t v = 0; v < sc->cams.size(); ++v)
-            if (!sc->uploaded[v]) throw ArgError("input view " + std::to_string(v) + " was not uploaded");
+        if (frame) {
+            for (size_t v = 0; v < sc->cams.size(); ++v)
+                if (!frame[v].y || !frame[v].u || !frame[v].v || !frame[v].depth) throw ArgError("null plane");
+        } else {
+            for (size_t v = 0; v < sc->cams.size(); ++v)
+                if (!sc->uploaded[v]) throw ArgError("input view " + std::to_string(v) + " was not uploaded");
+        }
         check(cudaSetDevice(ctx->device), "cudaSetDevice");
         ensure_workspace(sc, virt->width, virt->height);
         Workspace& ws = *sc->ws;
         fill_tables(sc, *virt, *params);
         cudaStream_t s = static_cast<cudaStream_t>(stream);
+        int decodes = 0;
+        if (frame) {
+            for (size_t v = 0; v < sc->cams.size(); ++v) {
+                const rvsb_camera& c = sc->cams[v];
+                launch_decode_color(frame[v].y, frame[v].u, frame[v].v, c.width, c.height,
+                                    sc->color[v]->as<uint64_t>(), s);
+                ws.table.v[v].pd = frame[v].depth;
+                ++decodes;
+            }
+            check(cudaPeekAtLastError(), "decode colour");
+        }
         DebugPtrs dbg;
         if (dbg_out) {
             dbg.warped_uvz = dbg_out->warped_uvz;
@@ -321,7 +343,7 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
                 off += nv;
             }
         }
-        sc->last_launches = launches;
+        sc->last_launches = launches + decodes;
         return RVSB_OK;
     });
 }
@@ -415,6 +437,9 @@ rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int 
             }
             sc->erp.push_back(std::move(r));
             sc->erp.push_back(std::move(c));
+            auto col = std::make_unique<DevMem>();
+            col->alloc(ctx, (size_t)inputs[v].width * inputs[v].height * sizeof(uint64_t));
+            sc->color.push_back(std::move(col));
         }
         sc->uploaded.assign(n_inputs, false);
         *out = sc.release();
@@ -444,6 +469,10 @@ rvsb_status rvsb_scene_upload(rvsb_scene* sc, int view, const rvsb_view_planes* 
             check(cudaMemcpyAsync(sc->planes[view * 4 + k]->ptr, src[k], plane_bytes(c, k),
                                   planes_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s),
                   "upload plane");
+        launch_decode_color(sc->planes[view * 4 + 0]->as<uint16_t>(), sc->planes[view * 4 + 1]->as<uint16_t>(),
+                            sc->planes[view * 4 + 2]->as<uint16_t>(), c.width, c.height,
+                            sc->color[view]->as<uint64_t>(), s);
+        check(cudaPeekAtLastError(), "decode colour");
         sc->uploaded[view] = true;
         return RVSB_OK;
     });
@@ -457,6 +486,13 @@ rvsb_status rvsb_synthesize(rvsb_scene* scene, const rvsb_camera* virt, const rv
 rvsb_status rvsb_synthesize_debug(rvsb_scene* scene, const rvsb_camera* virt, const rvsb_synth_params* params,
                                   const rvsb_yuv420* out, const rvsb_debug_out* dbg, void* stream) {
     return synthesize_impl(scene, virt, params, out, dbg, stream);
+}
+
+rvsb_status rvsb_synthesize_frame(rvsb_scene* scene, const rvsb_view_planes* device_planes,
+                                  const rvsb_camera* virt, const rvsb_synth_params* params,
+                                  const rvsb_yuv420* out, void* stream) {
+    if (!device_planes) return RVSB_E_ARG;
+    return synthesize_impl(scene, virt, params, out, nullptr, stream, device_planes);
 }
 
 int rvsb_scene_last_launch_count(const rvsb_scene* scene) { return scene ? scene->last_launches : 0; }
@@ -485,7 +521,7 @@ int rvsb_scene_stage_times(rvsb_scene* sc, float* ms, int max_stages) {
 }
 
 const char* rvsb_stage_name(int stage) {
-    static const char* names[NUM_STAGES] = {"warp", "bin", "tile", "inpaint", "total"};
+    static const char* names[NUM_STAGES] = {"warp", "bin", "raster", "inpaint", "total", "resolve"};
     return (stage >= 0 && stage < NUM_STAGES) ? names[stage] : "";
 }
 

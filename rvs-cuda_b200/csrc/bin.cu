@@ -74,7 +74,7 @@ __global__ void bin_fill_kernel(const __grid_constant__ ViewTable tab, int* __re
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
             const int pos = atomicAdd(&cursor[(ty * ntx + tx) * n + v], 1);
-            list[pos] = b;
+            list[pos] = ((b / V.nbx) << 11) | (b % V.nbx);  // block row << 11 | block column
         }
 }
 

@@ -120,21 +120,15 @@ __device__ __forceinline__ float tri_quality(float ax, float ay, float bx, float
 
 struct TriSetup {
     float b1c1, c0b0, c1a1, a0c0, den;
-    int x0, x1, y0, y1;  // CPU bounding box
-    float tn;            // coverage threshold of the numerators (coverage_threshold)
-    float rinv;          // 1 / den, correctly rounded
+    int x0, x1, y0, y1;  // candidate pixel range
+    float rinv;          // approximate 1 / den (at most 1 ulp off)
 };
 
-// fl(n / den) >= -1e-6f  <=>  n / den > M (real), where M is the midpoint
-// between -1e-6f and the next float below it: a quotient exactly at M rounds
-// to that neighbour, whose mantissa is even, and fails.  With den > 0 this is
-// n > M * den; M * den is exact in double (25 + 24 significant bits), so for
-// a float n the test is n >= T, T = the smallest float above M * den.
-__device__ __forceinline__ float coverage_threshold(float den, double lambda_mid) {
-    const double md = __dmul_rn(lambda_mid, (double)den);
-    float t = __double2float_rn(md);
-    if ((double)t <= md) t = nextafterf(t, INFINITY);
-    return t;
+// Reciprocal with at most 1 ulp error (PTX rcp.approx.f32, subnormals kept).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
 // Edge coefficients and den of colorize_triangle (transform.cpp:82-84).

@@ -31,6 +31,7 @@ struct DevView {
     const uint16_t* pd;
     const float* erp_row;                 // ERP: per row (cos theta, sin theta), 2*h floats
     const float* erp_col;                 // ERP: per column (cos phi, sin phi), 2*w floats
+    const uint64_t* color;                // h*w decoded colour: Y | 4U << 18 | 4V << 36
     float4* vert;                         // h*w warped vertices (u, v, z, 0)
     int4* bbox;                           // per binning block: x0, y0, x1, y1 (x0 > x1: empty)
     int nbx, nby;                         // binning blocks
@@ -50,7 +51,6 @@ struct DevTarget {
     float blend_exp;                      // BlendingFactor
     float inv_blend_exp;                  // 1.0f / BlendingFactor
     int blend_exp_int;                    // BlendingFactor when it is an integer in [2, 16], else 0
-    double lambda_mid;                    // midpoint of -1e-6f and the next float below it
     int ntx, nty;                         // output tiles
     int n_views;
     int bin_capacity;

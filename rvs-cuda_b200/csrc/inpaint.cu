@@ -19,6 +19,10 @@
 //           its own column (smallest y) when the column holds a minimum,
 //           otherwise the minimum with the largest y, then smallest x, and
 //           changes only on strict improvement.
+// Every hole lies inside the region and every source lies within one pixel
+// of a hole, so restricting the scans to the grown bounding box changes
+// nothing.  Loads are issued in batches (RB rows, CB chunks) so each thread
+// keeps several in flight.
 #include "device_common.cuh"
 #include "kernels.hpp"
 
@@ -29,6 +33,8 @@ using namespace dev;
 
 constexpr int kScanBias = 1 << 20;
 constexpr uint32_t kInfD = 0xFFFFFFFFu;
+constexpr int CB = 4;  // row scans: 32-pixel chunks loaded per batch
+constexpr int RB = 8;  // column scans: rows loaded per batch
 
 struct Region {
     int x0, y0, x1, y1;
@@ -45,19 +51,19 @@ __device__ __forceinline__ Region hole_region(const DevStatus* st, int wo, int h
     return r;
 }
 
-__device__ __forceinline__ bool is_hole(const uint64_t* codes, int wo, int x, int y) {
-    return (codes[(size_t)y * wo + x] & kHoleBit) != 0;
-}
-
 __device__ __forceinline__ uint64_t pack_dxy(uint32_t d, int x, int y) {
     return ((uint64_t)d << 32) | ((uint64_t)(uint32_t)x << 16) | (uint64_t)(uint32_t)y;
+}
+
+__device__ __forceinline__ unsigned long long umin64(unsigned long long a, unsigned long long b) {
+    return b < a ? b : a;
 }
 
 __device__ __forceinline__ unsigned long long warp_incl_min(unsigned long long v, int lane) {
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned long long y = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v = y < v ? y : v;
+        if (lane >= o) v = umin64(v, y);
     }
     return v;
 }
@@ -66,7 +72,7 @@ __device__ __forceinline__ unsigned long long warp_incl_min_rev(unsigned long lo
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned long long y = __shfl_down_sync(0xffffffffu, v, o);
-        if (lane + o < 32) v = y < v ? y : v;
+        if (lane + o < 32) v = umin64(v, y);
     }
     return v;
 }
@@ -74,38 +80,47 @@ __device__ __forceinline__ unsigned long long warp_incl_min_rev(unsigned long lo
 // Sweep 0, rows (forward): R(p) = lexmin over q.x <= p.x of
 // (C(q).d + p.x - q.x, C(q).src).  One warp per row of the region.
 __global__ void inpaint_row0_kernel(int wo, int ho, const DevStatus* __restrict__ st,
-                                    const uint64_t* __restrict__ codes, uint64_t* __restrict__ R) {
+                                    const uint8_t* __restrict__ holes, uint64_t* __restrict__ R) {
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
     const int lane = threadIdx.x & 31;
     const int y = rg.y0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (y > rg.y1) return;
+    const uint8_t* hr = holes + (size_t)y * wo;
+    const uint8_t* hd = y + 1 < ho ? hr + wo : nullptr;
     unsigned long long carry = kEmptyKey;
-    for (int base = rg.x0; base <= rg.x1; base += 32) {
-        const int x = base + lane;
-        unsigned long long key = kEmptyKey;
-        if (x <= rg.x1) {
-            uint32_t d = kInfD;
-            int sx = x, sy = y;
-            if (!is_hole(codes, wo, x, y)) {
-                d = 0;
-            } else if (y + 1 < ho && !is_hole(codes, wo, x, y + 1)) {
-                d = 1; sy = y + 1;
-            } else if (x + 1 < wo && !is_hole(codes, wo, x + 1, y)) {
-                d = 1; sx = x + 1;
+    for (int base = rg.x0; base <= rg.x1; base += 32 * CB) {
+        unsigned long long key[CB];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+            const int x = base + 32 * c + lane;
+            key[c] = kEmptyKey;
+            if (x <= rg.x1) {
+                uint32_t d = kInfD;
+                int sx = x, sy = y;
+                if (!hr[x]) {
+                    d = 0;
+                } else if (hd && !hd[x]) {
+                    d = 1; sy = y + 1;
+                } else if (x + 1 < wo && !hr[x + 1]) {
+                    d = 1; sx = x + 1;
+                }
+                if (d != kInfD) key[c] = pack_dxy((uint32_t)((int)d - x + kScanBias), sx, sy);
             }
-            if (d != kInfD) key = pack_dxy((uint32_t)((int)d - x + kScanBias), sx, sy);
         }
-        key = warp_incl_min(key, lane);
-        key = key < carry ? key : carry;
-        if (x <= rg.x1) {
-            uint64_t out = ~0ull;
-            if (key != kEmptyKey)
-                out = pack_dxy((uint32_t)((int)(key >> 32) - kScanBias + x), (int)((key >> 16) & 0xffff),
-                               (int)(key & 0xffff));
-            R[(size_t)y * wo + x] = out;
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+            const int x = base + 32 * c + lane;
+            unsigned long long k = umin64(warp_incl_min(key[c], lane), carry);
+            if (x <= rg.x1) {
+                uint64_t out = ~0ull;
+                if (k != kEmptyKey)
+                    out = pack_dxy((uint32_t)((int)(k >> 32) - kScanBias + x), (int)((k >> 16) & 0xffff),
+                                   (int)(k & 0xffff));
+                R[(size_t)y * wo + x] = out;
+            }
+            carry = __shfl_sync(0xffffffffu, k, 31);
         }
-        carry = __shfl_sync(0xffffffffu, key, 31);
     }
 }
 
@@ -113,18 +128,16 @@ __global__ void inpaint_row0_kernel(int wo, int ho, const DevStatus* __restrict_
 // Phase 1 reduces each segment, phase 2 rescans it with the carry of the
 // segments before it (above for forward scans, below for backward scans).
 
-// Sweep 0, columns (forward): D0, S0 (p) = lexmin over q.y <= p.y of
-// (R(q).d + p.y - q.y, src).  Output packed (D0, S0) per pixel.
-__device__ __forceinline__ unsigned long long col0_key(const uint64_t* R, int wo, int x, int y) {
-    const uint64_t r = R[(size_t)y * wo + x];
+__device__ __forceinline__ unsigned long long col0_key(uint64_t r, int y) {
     if (r == ~0ull) return kEmptyKey;
     const int d = (int)(r >> 32);
     return pack_dxy((uint32_t)(d - y + kScanBias), (int)((r >> 16) & 0xffff), (int)(r & 0xffff));
 }
 
-__global__ void __launch_bounds__(1024) inpaint_col0_kernel(int wo, int ho,
-                                                            const DevStatus* __restrict__ st,
-                                                            const uint64_t* __restrict__ codes,
+// Sweep 0, columns (forward): D0, S0 (p) = lexmin over q.y <= p.y of
+// (R(q).d + p.y - q.y, src).  Output packed (D0, S0) per pixel.
+__global__ void __launch_bounds__(1024) inpaint_col0_kernel(int wo, int ho, const DevStatus* __restrict__ st,
+                                                            const uint8_t* __restrict__ holes,
                                                             const uint64_t* __restrict__ R,
                                                             uint64_t* __restrict__ DS) {
     __shared__ unsigned long long seg[32][33];
@@ -139,28 +152,43 @@ __global__ void __launch_bounds__(1024) inpaint_col0_kernel(int wo, int ho,
     const bool col_ok = x <= rg.x1;
     unsigned long long m = kEmptyKey;
     if (col_ok)
-        for (int y = yb; y <= ye; ++y) {
-            const unsigned long long k = col0_key(R, wo, x, y);
-            m = k < m ? k : m;
+        for (int y0 = yb; y0 <= ye; y0 += RB) {
+            uint64_t r[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) r[k] = y0 + k <= ye ? R[(size_t)(y0 + k) * wo + x] : ~0ull;
+#pragma unroll
+            for (int k = 0; k < RB; ++k) m = umin64(m, col0_key(r[k], y0 + k));
         }
     seg[w][lane] = m;
     __syncthreads();
     unsigned long long run = kEmptyKey;
-    for (int s = 0; s < w; ++s) run = seg[s][lane] < run ? seg[s][lane] : run;
+    for (int s = 0; s < w; ++s) run = umin64(run, seg[s][lane]);
     if (!col_ok) return;
     const uint32_t big = (uint32_t)(wo + ho);
-    for (int y = yb; y <= ye; ++y) {
-        const unsigned long long k = col0_key(R, wo, x, y);
-        run = k < run ? k : run;
-        uint64_t out;
-        if (!is_hole(codes, wo, x, y))
-            out = pack_dxy(0, x, y);
-        else if (run == kEmptyKey)
-            out = pack_dxy(big, x, y);
-        else
-            out = pack_dxy((uint32_t)((int)(run >> 32) - kScanBias + y), (int)((run >> 16) & 0xffff),
-                           (int)(run & 0xffff));
-        DS[(size_t)y * wo + x] = out;
+    for (int y0 = yb; y0 <= ye; y0 += RB) {
+        uint64_t r[RB];
+        uint8_t h[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+            const bool ok = y0 + k <= ye;
+            r[k] = ok ? R[(size_t)(y0 + k) * wo + x] : ~0ull;
+            h[k] = ok ? holes[(size_t)(y0 + k) * wo + x] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+            const int y = y0 + k;
+            if (y > ye) break;
+            run = umin64(run, col0_key(r[k], y));
+            uint64_t out;
+            if (!h[k])
+                out = pack_dxy(0, x, y);
+            else if (run == kEmptyKey)
+                out = pack_dxy(big, x, y);
+            else
+                out = pack_dxy((uint32_t)((int)(run >> 32) - kScanBias + y), (int)((run >> 16) & 0xffff),
+                               (int)(run & 0xffff));
+            DS[(size_t)y * wo + x] = out;
+        }
     }
 }
 
@@ -175,7 +203,7 @@ __device__ __forceinline__ uint64_t ds_at(const uint64_t* DS, const Region& rg, 
 // up (D0+1, S0 of up) with priority stay > left > up; T'(q) the same without
 // stay.  Non-holes: (0, q).
 __global__ void inpaint_seed1_kernel(int wo, int ho, const DevStatus* __restrict__ st,
-                                     const uint64_t* __restrict__ codes, const uint64_t* __restrict__ DS,
+                                     const uint8_t* __restrict__ holes, const uint64_t* __restrict__ DS,
                                      uint64_t* __restrict__ Tq, uint64_t* __restrict__ Tp) {
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
@@ -183,7 +211,7 @@ __global__ void inpaint_seed1_kernel(int wo, int ho, const DevStatus* __restrict
     const int y = rg.y0 + (int)blockIdx.y;
     if (x > rg.x1 || y > rg.y1) return;
     const size_t o = (size_t)y * wo + x;
-    if (!is_hole(codes, wo, x, y)) {
+    if (!holes[o]) {
         Tq[o] = pack_dxy(0, x, y);
         Tp[o] = pack_dxy(0, x, y);
         return;
@@ -192,14 +220,12 @@ __global__ void inpaint_seed1_kernel(int wo, int ho, const DevStatus* __restrict
     uint64_t best = self;
     uint64_t bp = ~0ull;
     if (x > 0) {
-        const uint64_t l = ds_at(DS, rg, wo, x - 1, y);
-        const uint64_t c = l + (1ull << 32);
+        const uint64_t c = ds_at(DS, rg, wo, x - 1, y) + (1ull << 32);
         if ((c >> 32) < (best >> 32)) best = c;
         bp = c;
     }
     if (y > 0) {
-        const uint64_t u = ds_at(DS, rg, wo, x, y - 1);
-        const uint64_t c = u + (1ull << 32);
+        const uint64_t c = ds_at(DS, rg, wo, x, y - 1) + (1ull << 32);
         if ((c >> 32) < (best >> 32)) best = c;
         if (bp == ~0ull || (c >> 32) < (bp >> 32)) bp = c;
     }
@@ -218,22 +244,27 @@ __global__ void inpaint_row1_kernel(int wo, int ho, const DevStatus* __restrict_
     if (y > rg.y1) return;
     unsigned long long carry = kEmptyKey;
     const int n = rg.x1 - rg.x0 + 1;
-    for (int base = 0; base < n; base += 32) {
-        // process x from the right end: x = x1 - (base + lane)
-        const int x = rg.x1 - (base + (31 - lane));
-        unsigned long long key = kEmptyKey;
-        if (x >= rg.x0) {
-            const uint64_t t = Tq[(size_t)y * wo + x];
-            key = ((unsigned long long)((t >> 32) + (uint64_t)x) << 16) | (unsigned long long)x;
+    for (int base = 0; base < n; base += 32 * CB) {
+        unsigned long long key[CB];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+            // x runs from the right end: lane 31 holds the rightmost pixel of chunk c.
+            const int x = rg.x1 - (base + 32 * c + (31 - lane));
+            key[c] = kEmptyKey;
+            if (x >= rg.x0) {
+                const uint64_t t = Tq[(size_t)y * wo + x];
+                key[c] = ((unsigned long long)((t >> 32) + (uint64_t)x) << 16) | (unsigned long long)x;
+            }
         }
-        // lane 31 holds the rightmost x of this chunk; suffix min towards lane 0
-        unsigned long long incl = warp_incl_min_rev(key, lane);
-        incl = incl < carry ? incl : carry;
-        // exclusive: the value of lane + 1, or the carry for lane 31
-        unsigned long long excl = __shfl_down_sync(0xffffffffu, incl, 1);
-        if (lane == 31) excl = carry;
-        if (x >= rg.x0) RR[(size_t)y * wo + x] = excl;
-        carry = __shfl_sync(0xffffffffu, incl, 0);
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+            const int x = rg.x1 - (base + 32 * c + (31 - lane));
+            const unsigned long long incl = umin64(warp_incl_min_rev(key[c], lane), carry);
+            unsigned long long excl = __shfl_down_sync(0xffffffffu, incl, 1);
+            if (lane == 31) excl = carry;
+            if (x >= rg.x0) RR[(size_t)y * wo + x] = excl;
+            carry = __shfl_sync(0xffffffffu, incl, 0);
+        }
     }
 }
 
@@ -241,7 +272,7 @@ __global__ void inpaint_row1_kernel(int wo, int ho, const DevStatus* __restrict_
 // and copy that pixel's codes (the fill of inpaint_color,
 // inpainting.cpp:191-198).
 __global__ void __launch_bounds__(1024) inpaint_col1_kernel(
-    int wo, int ho, const DevStatus* __restrict__ st, uint64_t* __restrict__ codes,
+    int wo, int ho, const DevStatus* __restrict__ st, uint64_t* __restrict__ codes, const uint8_t* __restrict__ holes,
     const uint64_t* __restrict__ DS, const uint64_t* __restrict__ Tq, const uint64_t* __restrict__ Tp,
     const uint64_t* __restrict__ RR, int32_t* __restrict__ dbg_source) {
     __shared__ unsigned long long seg_col[32][33];
@@ -258,74 +289,94 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(
     // Keys: column part (T.d + y) << 16 | y (minimum y on ties);
     //       off-column (RR.d - x + y) << 32 | (0xffff - y) << 16 | qx
     //       (largest y, then smallest x on ties).
-    auto col_key = [&](int y) -> unsigned long long {
-        const uint64_t t = Tq[(size_t)y * wo + x];
+    auto col_key = [&](uint64_t t, int y) -> unsigned long long {
         return ((unsigned long long)((t >> 32) + (uint64_t)y) << 16) | (unsigned long long)y;
     };
-    auto off_key = [&](int y) -> unsigned long long {
-        const uint64_t r = RR[(size_t)y * wo + x];
+    auto off_key = [&](uint64_t r, int y) -> unsigned long long {
         if (r == kEmptyKey) return kEmptyKey;
         const uint64_t v = (r >> 16) - (uint64_t)x + (uint64_t)y;
         return (v << 32) | ((uint64_t)(0xffff - y) << 16) | (r & 0xffff);
     };
     unsigned long long mc = kEmptyKey, mo = kEmptyKey;
     if (col_ok)
-        for (int y = yb; y <= ye; ++y) {
-            const unsigned long long a = col_key(y), b = off_key(y);
-            mc = a < mc ? a : mc;
-            mo = b < mo ? b : mo;
+        for (int y0 = yb; y0 <= ye; y0 += RB) {
+            uint64_t t[RB], r[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                const bool ok = y0 + k <= ye;
+                t[k] = ok ? Tq[(size_t)(y0 + k) * wo + x] : ~0ull;
+                r[k] = ok ? RR[(size_t)(y0 + k) * wo + x] : ~0ull;
+            }
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                if (y0 + k > ye) break;
+                mc = umin64(mc, col_key(t[k], y0 + k));
+                mo = umin64(mo, off_key(r[k], y0 + k));
+            }
         }
     seg_col[w][lane] = mc;
     seg_off[w][lane] = mo;
     __syncthreads();
     unsigned long long run_c = kEmptyKey, run_o = kEmptyKey;
     for (int s = w + 1; s < 32; ++s) {
-        run_c = seg_col[s][lane] < run_c ? seg_col[s][lane] : run_c;
-        run_o = seg_off[s][lane] < run_o ? seg_off[s][lane] : run_o;
+        run_c = umin64(run_c, seg_col[s][lane]);
+        run_o = umin64(run_o, seg_off[s][lane]);
     }
     if (!col_ok) return;
-    for (int y = ye; y >= yb; --y) {
-        // run_c holds the exclusive (rows below) column minimum here.
-        const unsigned long long ok = off_key(y);
-        run_o = ok < run_o ? ok : run_o;
-        const size_t o = (size_t)y * wo + x;
-        const uint64_t code = codes[o];
-        if (code & kHoleBit) {
-            const uint64_t tp = Tp[o];
-            // column candidate (cost, y)
-            uint64_t c_cost = tp == ~0ull ? (uint64_t)1 << 40 : (tp >> 32);
-            int c_y = y;
-            if (run_c != kEmptyKey) {
-                const uint64_t cost = (run_c >> 16) - (uint64_t)y;
-                if (cost < c_cost) {
-                    c_cost = cost;
-                    c_y = (int)(run_c & 0xffff);
+    // Bottom-up over the segment in batches of RB rows.
+    for (int y1 = ye; y1 >= yb; y1 -= RB) {
+        uint64_t t[RB], r[RB];
+        uint8_t h[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+            const int y = y1 - k;
+            const bool ok = y >= yb;
+            t[k] = ok ? Tq[(size_t)y * wo + x] : ~0ull;
+            r[k] = ok ? RR[(size_t)y * wo + x] : ~0ull;
+            h[k] = ok ? holes[(size_t)y * wo + x] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+            const int y = y1 - k;
+            if (y < yb) break;
+            // run_c holds the exclusive (rows below) column minimum here.
+            run_o = umin64(run_o, off_key(r[k], y));
+            if (h[k]) {
+                const size_t o = (size_t)y * wo + x;
+                const uint64_t tp = Tp[o];
+                uint64_t c_cost = tp == ~0ull ? (uint64_t)1 << 40 : (tp >> 32);
+                int c_y = y;
+                if (run_c != kEmptyKey) {
+                    const uint64_t cost = (run_c >> 16) - (uint64_t)y;
+                    if (cost < c_cost) {
+                        c_cost = cost;
+                        c_y = (int)(run_c & 0xffff);
+                    }
+                }
+                uint64_t o_cost = (uint64_t)1 << 40;
+                int o_x = 0, o_y = 0;
+                if (run_o != kEmptyKey) {
+                    o_cost = (run_o >> 32) - (uint64_t)y;
+                    o_y = 0xffff - (int)((run_o >> 16) & 0xffff);
+                    o_x = (int)(run_o & 0xffff);
+                }
+                const uint64_t ds = DS[o];
+                const uint64_t d0 = ds >> 32;
+                uint64_t src = ds;
+                if (c_cost <= o_cost) {
+                    if (c_cost < d0) src = (c_y == y) ? tp : Tq[(size_t)c_y * wo + x];
+                } else {
+                    if (o_cost < d0) src = Tq[(size_t)o_y * wo + o_x];
+                }
+                const int sx = (int)((src >> 16) & 0xffff), sy = (int)(src & 0xffff);
+                codes[o] = (codes[(size_t)sy * wo + sx] & kCodeMask) | kHoleBit;
+                if (dbg_source) {
+                    dbg_source[o * 2 + 0] = sx;
+                    dbg_source[o * 2 + 1] = sy;
                 }
             }
-            uint64_t o_cost = (uint64_t)1 << 40;
-            int o_x = 0, o_y = 0;
-            if (run_o != kEmptyKey) {
-                o_cost = (run_o >> 32) - (uint64_t)y;
-                o_y = 0xffff - (int)((run_o >> 16) & 0xffff);
-                o_x = (int)(run_o & 0xffff);
-            }
-            const uint64_t ds = DS[o];
-            const uint64_t d0 = ds >> 32;
-            uint64_t src = ds;
-            if (c_cost <= o_cost) {
-                if (c_cost < d0) src = (c_y == y) ? tp : Tq[(size_t)c_y * wo + x];
-            } else {
-                if (o_cost < d0) src = Tq[(size_t)o_y * wo + o_x];
-            }
-            const int sx = (int)((src >> 16) & 0xffff), sy = (int)(src & 0xffff);
-            codes[o] = (codes[(size_t)sy * wo + sx] & kCodeMask) | kHoleBit;
-            if (dbg_source) {
-                dbg_source[o * 2 + 0] = sx;
-                dbg_source[o * 2 + 1] = sy;
-            }
+            run_c = umin64(run_c, col_key(t[k], y));
         }
-        const unsigned long long ck = col_key(y);
-        run_c = ck < run_c ? ck : run_c;
     }
 }
 
@@ -355,23 +406,21 @@ __global__ void inpaint_write_kernel(int wo, int ho, const DevStatus* __restrict
     out_v[co] = (uint16_t)((sv + 2) >> 2);
 }
 
-
 }  // namespace
 
 void launch_inpaint(const SynthBuffers& b, const LaunchShape& sh, const DebugPtrs& dbg, uint16_t* out_y,
                     uint16_t* out_u, uint16_t* out_v, cudaStream_t s) {
     const int rows_per_cta = 8;  // 8 warps of 32
-    inpaint_row0_kernel<<<(sh.ho + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(sh.wo, sh.ho, b.status, b.codes,
-                                                                                  b.scan_a);
-    inpaint_col0_kernel<<<(sh.wo + 31) / 32, 1024, 0, s>>>(sh.wo, sh.ho, b.status, b.codes, b.scan_a, b.scan_b);
-    inpaint_seed1_kernel<<<dim3((sh.wo + 255) / 256, sh.ho), 256, 0, s>>>(sh.wo, sh.ho, b.status, b.codes, b.scan_b,
-                                                                        b.scan_c, b.scan_d);
-    inpaint_row1_kernel<<<(sh.ho + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(sh.wo, sh.ho, b.status, b.scan_c,
-                                                                                  b.scan_a);
-    inpaint_col1_kernel<<<(sh.wo + 31) / 32, 1024, 0, s>>>(sh.wo, sh.ho, b.status, b.codes, b.scan_b, b.scan_c,
-                                                          b.scan_d, b.scan_a, dbg.inpaint_source);
-    inpaint_write_kernel<<<dim3((sh.wo / 2 + 127) / 128, (sh.ho + 1) / 2), 128, 0, s>>>(sh.wo, sh.ho, b.status,
-                                                                                      b.codes, out_y, out_u, out_v);
+    const int wo = sh.wo, ho = sh.ho;
+    inpaint_row0_kernel<<<(ho + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(wo, ho, b.status, b.holes, b.scan_a);
+    inpaint_col0_kernel<<<(wo + 31) / 32, 1024, 0, s>>>(wo, ho, b.status, b.holes, b.scan_a, b.scan_b);
+    inpaint_seed1_kernel<<<dim3((wo + 255) / 256, ho), 256, 0, s>>>(wo, ho, b.status, b.holes, b.scan_b, b.scan_c,
+                                                                  b.scan_d);
+    inpaint_row1_kernel<<<(ho + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(wo, ho, b.status, b.scan_c, b.scan_a);
+    inpaint_col1_kernel<<<(wo + 31) / 32, 1024, 0, s>>>(wo, ho, b.status, b.codes, b.holes, b.scan_b, b.scan_c,
+                                                       b.scan_d, b.scan_a, dbg.inpaint_source);
+    inpaint_write_kernel<<<dim3((wo / 2 + 127) / 128, (ho + 1) / 2), 128, 0, s>>>(wo, ho, b.status, b.codes, out_y,
+                                                                               out_u, out_v);
 }
 
 }  // namespace rvsb

@@ -16,7 +16,9 @@ struct SynthBuffers {
     int* cursor = nullptr;         // ntiles * n_views
     int* list = nullptr;           // bin list, `capacity` entries
     int capacity = 0;
+    uint64_t* keys = nullptr;      // n_views * Wo*Ho raster keys (winning fragment per pixel)
     uint64_t* codes = nullptr;     // Wo*Ho packed output codes + hole bit
+    uint8_t* holes = nullptr;      // Wo*Ho hole mask (1 = no view covers the pixel)
     uint64_t* scan_a = nullptr;    // Wo*Ho inpainting scratch
     uint64_t* scan_b = nullptr;
     uint64_t* scan_c = nullptr;
@@ -52,8 +54,12 @@ struct LaunchShape {
 
 // Issues the whole synthesis on `stream`; returns the number of kernel
 // launches, or -1 on a launch error (cudaGetLastError holds the cause).
+// Decodes the colour planes of one input view into packed per-pixel words.
+void launch_decode_color(const uint16_t* y, const uint16_t* u, const uint16_t* v, int w, int h, uint64_t* out,
+                         cudaStream_t s);
+
 // `events` (optional) holds 2 * NUM_STAGES events recorded around the stages.
-constexpr int NUM_STAGES = 5;
+constexpr int NUM_STAGES = 6;
 int launch_synthesis(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& shape, const DebugPtrs& dbg,
                      uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t stream,
                      cudaEvent_t* events = nullptr);

@@ -25,11 +25,11 @@ EXPORTED = [
     "rvsb_config_texture_path", "rvsb_config_depth_path", "rvsb_config_output_path", "rvsb_config_frames",
     "rvsb_config_synth_params", "rvsb_config_virtual_camera_at", "rvsb_relative_pose", "rvsb_scene_create",
     "rvsb_scene_destroy", "rvsb_scene_upload", "rvsb_synthesize", "rvsb_synthesize_host",
-    "rvsb_synthesize_debug", "rvsb_scene_last_launch_count", "rvsb_scene_set_profiling",
+    "rvsb_synthesize_debug", "rvsb_synthesize_frame", "rvsb_scene_last_launch_count", "rvsb_scene_set_profiling",
     "rvsb_scene_stage_times", "rvsb_stage_name",
 ]
 
-STAGES = ["warp", "bin", "tile", "inpaint", "total"]
+STAGES = ["warp", "bin", "raster", "inpaint", "total", "resolve"]
 
 _lib = None
 
@@ -84,6 +84,7 @@ def load():
     L.rvsb_synthesize_host.argtypes = [c_p, P(Camera), ctypes.c_int, P(ViewPlanes), P(Camera),
                                        P(SynthParams), P(Yuv420), c_p]
     L.rvsb_synthesize_debug.argtypes = [c_p, P(Camera), P(SynthParams), P(Yuv420), P(DebugOut), c_p]
+    L.rvsb_synthesize_frame.argtypes = [c_p, P(ViewPlanes), P(Camera), P(SynthParams), P(Yuv420), c_p]
     L.rvsb_scene_last_launch_count.argtypes = [c_p]
     L.rvsb_scene_set_profiling.argtypes = [c_p, ctypes.c_int]
     L.rvsb_scene_stage_times.argtypes = [c_p, P(ctypes.c_float), ctypes.c_int]
@@ -170,6 +171,16 @@ class Scene:
         out = Yuv420(*(_ptr(a) for a in out_planes))
         return self.ctx.check(self.ctx.lib.rvsb_synthesize(self.h, ctypes.byref(virt), ctypes.byref(p),
                                                            ctypes.byref(out), _stream(stream)))
+
+    def synthesize_frame(self, device_planes, virt, p, out_planes, stream=None):
+        """Per-frame call with raw planes in device memory (no copies)."""
+        n = len(self.cams)
+        vp = (ViewPlanes * n)()
+        for i, planes in enumerate(device_planes):
+            vp[i].y, vp[i].u, vp[i].v, vp[i].depth = (_ptr(a) for a in planes)
+        out = Yuv420(*(_ptr(a) for a in out_planes))
+        return self.ctx.check(self.ctx.lib.rvsb_synthesize_frame(self.h, vp, ctypes.byref(virt), ctypes.byref(p),
+                                                                 ctypes.byref(out), _stream(stream)))
 
     def synthesize_debug(self, virt, p, out_planes, dbg, stream=None):
         out = Yuv420(*(_ptr(a) for a in out_planes))

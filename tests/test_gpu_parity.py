@@ -114,3 +114,23 @@ def test_plain_1080p_full_size(ctx):
     assert np.array_equal(~(dbg["blend_quality"] > 0), ~(cq > 0))
     r = assert_parity(yuv, cpu)
     print(r)
+
+
+def test_frame_call_matches_scene_call(ctx):
+    """rvsb_synthesize_frame (device planes, no copies) gives the same bytes
+    as rvsb_scene_upload + rvsb_synthesize."""
+    import torch
+    from helpers import to_u16, yuv_planes_torch
+    wl = scenes.random_pose_small(n_views=3, w=96, h=54, seed=31)
+    target = wl.targets[0]
+    a, sc = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0)
+    dev = [[torch.from_numpy(np.ascontiguousarray(x).view(np.int16)).reshape(-1).cuda() for x in pl]
+           for pl in wl.planes]
+    out = yuv_planes_torch(target.width, target.height)
+    sc2 = rvsb.Scene(ctx, wl.inputs)
+    sc2.synthesize_frame(dev, target, rvsb.params(5.0), out)
+    torch.cuda.synchronize()
+    wo, ho = target.width, target.height
+    b = (to_u16(out[0], (ho, wo)), to_u16(out[1], (ho // 2, wo // 2)), to_u16(out[2], (ho // 2, wo // 2)))
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
