@@ -108,35 +108,6 @@ def percentile(xs, q):
     return xs[f] + (xs[c] - xs[f]) * (k - f)
 
 
-def dist_setup():
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        backend = "nccl" if torch.cuda.is_available() else "gloo"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-    return world, rank, local
-
-
-def allreduce_max(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
 def workload_plain():
     from rvsb import scenes
     wl = scenes.plain_1080p()
@@ -219,7 +190,10 @@ def main():
     import torch
     import rvsb
 
-    world, rank, local = dist_setup()
+    from rvsb import replicas
+    world, rank, local = replicas.init()
+    barrier = replicas.barrier
+    allreduce_max = replicas.max_over_ranks
     torch.cuda.set_device(local)
     wl = workload_plain()
     target = wl.targets[0]
@@ -362,9 +336,7 @@ def main():
         print(json.dumps(line))
     scene.close()
     ctx.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish(world)
 
 
 if __name__ == "__main__":

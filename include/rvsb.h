@@ -102,11 +102,23 @@ typedef struct rvsb_yuv420 {
     uint16_t* v;
 } rvsb_yuv420;
 
+/* Rounding of the output chroma 2x2 mean.  write_color_YUV
+ * (rvs/src/image_writing.cpp:83-84) halves U and V with OpenCV's
+ * cv::resize(0.5, 0.5, INTER_LINEAR) on uint16 samples, whose ties depend on
+ * how OpenCV was built: with Intel IPP (the default of a source build on
+ * x86-64, and the opencv-python wheel) a 2x2 sum s gives round-half-even(s/4);
+ * without IPP it gives (s + 2) >> 2. */
+typedef enum rvsb_chroma_rounding {
+    RVSB_CHROMA_TIES_EVEN = 0, /* OpenCV built with IPP (default) */
+    RVSB_CHROMA_TIES_UP = 1    /* OpenCV built without IPP */
+} rvsb_chroma_rounding;
+
 /* Synthesis options (Config, rvs/src/Config.hpp:172-205). */
 typedef struct rvsb_synth_params {
     float blending_factor;    /* "BlendingFactor" (default 5); must be > 0 */
     float precision;          /* "Precision"; only 1 is supported */
-    int32_t reserved[2];
+    int32_t chroma_rounding;  /* rvsb_chroma_rounding; 0 unless set */
+    int32_t reserved;         /* must be 0 */
 } rvsb_synth_params;
 
 /* ----------------------------------------------------------------------- */

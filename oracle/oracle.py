@@ -38,6 +38,7 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         P = ctypes.POINTER(abi.Camera)
         L.orc_set_trig_mode.argtypes = [ctypes.c_int]
+        L.orc_set_chroma_round.argtypes = [ctypes.c_int]
         L.orc_decode_color.argtypes = [_U16, _U16, _U16, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F]
         L.orc_decode_depth.argtypes = [_U16, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                        ctypes.c_float, ctypes.c_int, _F]
@@ -53,6 +54,11 @@ def lib():
         L.orc_write_yuv420.argtypes = [_F, ctypes.c_int, ctypes.c_int, ctypes.c_int, _U16]
         L.orc_synthesize.argtypes = [ctypes.c_int, P, ctypes.POINTER(abi.ViewPlanes), P, ctypes.c_float,
                                      _U16, _F, _F]
+        L.orc_image_pos.argtypes = [P, _F]
+        L.orc_unproject.argtypes = [P, _F, _F, _F]
+        L.orc_project.argtypes = [P, _F, _F, _F, ctypes.POINTER(ctypes.c_int)]
+        L.orc_edge_norm.argtypes = [_F, _F]
+        L.orc_edge_norm.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -63,6 +69,11 @@ def _p(a, t):
 
 def set_trig_mode(mode):
     lib().orc_set_trig_mode(int(mode))
+
+
+def set_chroma_round(mode):
+    """0: ties to even (OpenCV built with IPP), 1: ties up (without)."""
+    lib().orc_set_chroma_round(int(mode))
 
 
 def decode_color(y, u, v, bits=10):
@@ -192,3 +203,32 @@ def synthesize(inputs, planes, virt, exponent, want_intermediate=False):
     if want_intermediate:
         return yuv, q, c
     return yuv
+
+
+def image_pos(cam):
+    uv = np.empty((cam.height, cam.width, 2), np.float32)
+    assert lib().orc_image_pos(ctypes.byref(cam), _p(uv, _F)) == 0
+    return uv
+
+
+def unproject(cam, uv, depth):
+    uv = np.ascontiguousarray(uv, np.float32)
+    depth = np.ascontiguousarray(depth, np.float32)
+    xyz = np.empty((cam.height, cam.width, 3), np.float32)
+    assert lib().orc_unproject(ctypes.byref(cam), _p(uv, _F), _p(depth, _F), _p(xyz, _F)) == 0
+    return xyz
+
+
+def project(cam, xyz):
+    xyz = np.ascontiguousarray(xyz, np.float32)
+    uv = np.empty((cam.height, cam.width, 2), np.float32)
+    d = np.empty((cam.height, cam.width), np.float32)
+    wrap = ctypes.c_int(0)
+    assert lib().orc_project(ctypes.byref(cam), _p(xyz, _F), _p(uv, _F), _p(d, _F), ctypes.byref(wrap)) == 0
+    return uv, d, wrap.value
+
+
+def edge_norm(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return lib().orc_edge_norm(_p(a, _F), _p(b, _F))

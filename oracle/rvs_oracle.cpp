@@ -10,11 +10,16 @@
  * the reference project root).  OpenCV operations on the path are written
  * out from their mathematical definitions:
  *   - cv::Matx33f * cv::Vec3f / Matx * Matx: s = 0; s += a(i,k)*b(k) in float
- *   - cv::norm(Vec2f a, Vec2f b): sqrt in double of sum of (double)(a-b)^2
+ *   - cv::norm(Vec2f a, Vec2f b): sqrt in double of sum of (double)(a-b)^2,
+ *     the difference taken in float (OpenCV 4.9's normL2Sqr<float, double>)
  *   - cv::norm(Vec3f): sqrt in double of sum of (double)x^2, cast to float
  *   - Vec3f / float: multiplication by (1.f / alpha)
- *   - cv::resize(0.5, 0.5, INTER_LINEAR) of uint16 planes: (a+b+c+d+2) >> 2
- *     (pinned against the Python cv2 wheel by tests/golden)
+ *   - cv::resize(0.5, 0.5, INTER_LINEAR) of uint16 planes: the 2x2 sum s
+ *     divided by 4 and rounded; ties go to even in an OpenCV built with
+ *     Intel IPP (the default of a source build on x86-64, and the opencv-python
+ *     wheel) and up, (s+2) >> 2, in one built without it.
+ *     orc_set_chroma_round selects the mode (0: half to even, the default;
+ *     1: half up).  Both are pinned against cv2 by tests/golden.
  * Float arithmetic follows the reference's operation order; the file is
  * compiled with -ffp-contract=off so no multiply-add is fused, except where
  * the reference itself runs a CUDA loader kernel built with nvcc's default
@@ -41,6 +46,14 @@
 namespace {
 
 int g_trig_mode = 0;  // 0: correctly rounded float trig, 1: host libm float trig
+int g_chroma_round = 0;  // 0: ties to even (OpenCV with IPP), 1: ties up (without)
+
+// Rounded quarter of a 2x2 sum of uint16 samples (cv::resize 0.5 x 0.5).
+inline uint16_t quarter_round(unsigned s) {
+    if (g_chroma_round) return (uint16_t)((s + 2) >> 2);
+    const unsigned q = s >> 2, r = s & 3;
+    return (uint16_t)(q + (r > 2 || (r == 2 && (q & 1))));
+}
 
 inline float f_cos(float x) { return g_trig_mode ? std::cos(x) : (float)std::cos((double)x); }
 inline float f_sin(float x) { return g_trig_mode ? std::sin(x) : (float)std::sin((double)x); }
@@ -131,6 +144,7 @@ unsigned max_level(int bit_depth) { return (1u << bit_depth) - 1u; }
 extern "C" {
 
 void orc_set_trig_mode(int mode) { g_trig_mode = mode; }
+void orc_set_chroma_round(int mode) { g_chroma_round = mode; }
 
 /* Colour loader: image_loading.cpp:74-145 read_color_YUV, chroma upsample
  * resizeUV (process_input_frame.cu:22-81, srcX = x * (inW/outW), no
@@ -297,6 +311,96 @@ int orc_warp(const rvsb_camera* in, const rvsb_camera* vt, const float* depth, f
         }
     if (wrap) *wrap = (vt->projection == RVSB_PROJ_EQUIRECTANGULAR && vt->full_hor_range) ? 1 : 0;
     return RVSB_OK;
+}
+
+/* The camera-model steps one at a time, as the reference's unit tests
+ * exercise them (unit_test.cpp:90-308): image positions
+ * (Unprojector::generateImagePos, Unprojector.cpp:63-74 and
+ * EquirectangularUnprojector.cpp:87-98), unprojection and projection of
+ * the camera `c` (no pose).  uv: H*W*2, depth: H*W, xyz: H*W*3. */
+int orc_image_pos(const rvsb_camera* c, float* uv) {
+    if (!c || !uv) return RVSB_E_ARG;
+    for (int i = 0; i < c->height; ++i)
+        for (int j = 0; j < c->width; ++j) {
+            size_t o = ((size_t)i * c->width + j) * 2;
+            uv[o] = j + 0.5f;
+            uv[o + 1] = i + 0.5f;
+        }
+    if (c->projection == RVSB_PROJ_EQUIRECTANGULAR)
+        for (int j = 0; j < c->width; ++j) {
+            uv[(size_t)j * 2 + 1] = 1e-3f;
+            uv[((size_t)(c->height - 1) * c->width + j) * 2 + 1] = c->height - 1e-3f;
+        }
+    return RVSB_OK;
+}
+
+int orc_unproject(const rvsb_camera* c, const float* uv, const float* depth, float* xyz) {
+    if (!c || !uv || !depth || !xyz) return RVSB_E_ARG;
+    const int w = c->width, h = c->height;
+    const float radperdeg = 0.01745329252f;
+    for (size_t p = 0; p < (size_t)w * h; ++p) {
+        const float u = uv[p * 2], v = uv[p * 2 + 1], d = depth[p];
+        if (c->projection == RVSB_PROJ_EQUIRECTANGULAR) {
+            const float phi0 = radperdeg * c->hor_range[1];
+            const float theta0 = radperdeg * c->ver_range[1];
+            const float dphi_du = -radperdeg * (c->hor_range[1] - c->hor_range[0]) / w;
+            const float dtheta_dv = -radperdeg * (c->ver_range[1] - c->ver_range[0]) / h;
+            const float phi = phi0 + dphi_du * u, theta = theta0 + dtheta_dv * v;
+            const float ct = f_cos(theta);
+            const float a = ct * f_cos(phi), b = ct * f_sin(phi), cc = f_sin(theta);
+            xyz[p * 3] = d * a;
+            xyz[p * 3 + 1] = d * b;
+            xyz[p * 3 + 2] = d * cc;
+        } else if (d > 0.f) {
+            xyz[p * 3] = d;
+            xyz[p * 3 + 1] = -(d / c->focal[0]) * (u - c->principle_point[0]);
+            xyz[p * 3 + 2] = -(d / c->focal[1]) * (v - c->principle_point[1]);
+        } else {
+            xyz[p * 3] = xyz[p * 3 + 1] = xyz[p * 3 + 2] = kNaN;
+        }
+    }
+    return RVSB_OK;
+}
+
+int orc_project(const rvsb_camera* c, const float* xyz, float* uv, float* depth, int* wrap) {
+    if (!c || !xyz || !uv || !depth) return RVSB_E_ARG;
+    const int w = c->width, h = c->height;
+    const float degperrad = 57.295779513f;
+    for (size_t p = 0; p < (size_t)w * h; ++p) {
+        const float* y = xyz + p * 3;
+        if (c->projection == RVSB_PROJ_EQUIRECTANGULAR) {
+            const float u0 = w * c->hor_range[1] / (c->hor_range[1] - c->hor_range[0]);
+            const float v0 = h * c->ver_range[1] / (c->ver_range[1] - c->ver_range[0]);
+            const float du_dphi = -degperrad * w / (c->hor_range[1] - c->hor_range[0]);
+            const float dv_dtheta = -degperrad * h / (c->ver_range[1] - c->ver_range[0]);
+            double s2 = 0.0;
+            for (int k = 0; k < 3; ++k) s2 += (double)y[k] * (double)y[k];
+            const float radius = (float)std::sqrt(s2);
+            depth[p] = radius;
+            const float phi = f_atan2(y[1], y[0]);
+            const float theta = f_asin(y[2] / radius);
+            uv[p * 2] = u0 + du_dphi * phi;
+            uv[p * 2 + 1] = v0 + dv_dtheta * theta;
+        } else if (y[0] > 0.f) {
+            uv[p * 2] = -c->focal[0] * y[1] / y[0] + c->principle_point[0];
+            uv[p * 2 + 1] = -c->focal[1] * y[2] / y[0] + c->principle_point[1];
+            depth[p] = y[0];
+        } else {
+            uv[p * 2] = uv[p * 2 + 1] = depth[p] = kNaN;
+        }
+    }
+    if (wrap) *wrap = (c->projection == RVSB_PROJ_EQUIRECTANGULAR && c->full_hor_range) ? 1 : 0;
+    return RVSB_OK;
+}
+
+/* cv::norm(Vec2f a, Vec2f b) as valid_tri uses it (transform.cpp:63-65). */
+double orc_edge_norm(const float* a, const float* b) {
+    double s = 0.0;
+    for (int k = 0; k < 2; ++k) {
+        double v = (double)(a[k] - b[k]);
+        s += v * v;
+    }
+    return std::sqrt(s);
 }
 
 }  // extern "C"
@@ -570,7 +674,7 @@ int orc_inpaint(const float* color, const float* quality, int w, int h, float* o
  * (image_writing.cpp:142-180: static_cast<ushort>(v * max_level)), then
  * write_color_YUV (image_writing.cpp:72-89): Y as is, U and V through
  * cv::resize(0.5, 0.5, INTER_LINEAR) of the quantised uint16 planes, which
- * at an exact 2x reduction is the rounded 2x2 mean (a+b+c+d+2) >> 2.
+ * at an exact 2x reduction is the rounded 2x2 mean (quarter_round).
  * out: Y (w*h) then U and V ((w/2)*(h/2) each).  w and h must be even. */
 int orc_write_yuv420(const float* color, int w, int h, int bits, uint16_t* out) {
     if (!color || !out || w <= 0 || h <= 0 || (w & 1) || (h & 1) || bits < 9 || bits > 16)
@@ -590,7 +694,7 @@ int orc_write_yuv420(const float* color, int w, int h, int bits, uint16_t* out) 
                 size_t p10 = p00 + (size_t)w * 3;
                 size_t p11 = p10 + 3;
                 unsigned s = (unsigned)q[p00] + q[p01] + q[p10] + q[p11];
-                dst[(size_t)y * cw + x] = (uint16_t)((s + 2) >> 2);
+                dst[(size_t)y * cw + x] = quarter_round(s);
             }
     }
     return RVSB_OK;

@@ -271,6 +271,8 @@ void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_param
     T.blend_exp_int = 0;
     if (p.blending_factor == std::floor(p.blending_factor) && p.blending_factor >= 2.f && p.blending_factor <= 16.f)
         T.blend_exp_int = (int)p.blending_factor;
+    T.chroma_ties_up = p.chroma_rounding == RVSB_CHROMA_TIES_UP;
+    sc->ws->shape.chroma_ties_up = T.chroma_ties_up;
 
     T.ntx = ws.shape.ntx;
     T.nty = ws.shape.nty;
@@ -283,6 +285,9 @@ void validate_params(const rvsb_synth_params* p) {
     if (!(p->blending_factor > 0.f) || !std::isfinite(p->blending_factor))
         throw Unsupported("BlendingFactor must be a positive finite number");
     if (p->precision != 1.f) throw Unsupported("Precision other than 1 is not supported");
+    if (p->chroma_rounding != RVSB_CHROMA_TIES_EVEN && p->chroma_rounding != RVSB_CHROMA_TIES_UP)
+        throw ArgError("chroma_rounding must be RVSB_CHROMA_TIES_EVEN or RVSB_CHROMA_TIES_UP");
+    if (p->reserved != 0) throw ArgError("reserved synthesis parameter must be 0");
 }
 
 // `frame` (optional): raw device planes of every input view for this call;
@@ -664,6 +669,7 @@ void rvsb_config_synth_params(const rvsb_config* c, rvsb_synth_params* out) {
     std::memset(out, 0, sizeof(*out));
     out->blending_factor = c->cfg.blending_factor;
     out->precision = c->cfg.precision;
+    out->chroma_rounding = RVSB_CHROMA_TIES_EVEN;
 }
 
 rvsb_status rvsb_config_virtual_camera_at(const rvsb_config* c, int i, int frame, rvsb_camera* out) {

@@ -283,6 +283,15 @@ __device__ __forceinline__ float blend_pow(float x, float e, int e_int) {
     return powf(x, e);
 }
 
+// cv::resize(0.5, 0.5, INTER_LINEAR) of a uint16 plane at one output
+// sample (image_writing.cpp:83-84): the 2x2 sum s over 4, rounded; ties go
+// up in OpenCV's own code and to even in its IPP build.
+__device__ __forceinline__ uint16_t quarter_round(uint32_t s, int ties_up) {
+    const uint32_t q = s >> 2, r = s & 3u;
+    const uint32_t up = ties_up ? (r >= 2u) : ((r > 2u) | ((r == 2u) & q));
+    return (uint16_t)(q + (up & 1u));
+}
+
 // static_cast<ushort>(v * max_level) (image_writing.cpp:165-172).
 __device__ __forceinline__ uint32_t quantize(float c, unsigned max_val) {
     const uint32_t q = __float2uint_rz(__fmul_rn(c, (float)max_val));

@@ -51,6 +51,7 @@ struct DevTarget {
     float blend_exp;                      // BlendingFactor
     float inv_blend_exp;                  // 1.0f / BlendingFactor
     int blend_exp_int;                    // BlendingFactor when it is an integer in [2, 16], else 0
+    int chroma_ties_up;                   // output chroma mean: 1 rounds ties up, 0 to even
     int ntx, nty;                         // output tiles
     int n_views;
     int bin_capacity;

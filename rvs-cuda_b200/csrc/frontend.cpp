@@ -158,7 +158,7 @@ double Node::asDouble() const {
     return v_->number;
 }
 
-// JsonParser.cpp:281-290: rounds to nearest and rejects only a positive
+// JsonParser.cpp:303-314: rounds to nearest and rejects only a positive
 // rounding error above 1e-6.
 int Node::asInt() const {
     double value = asDouble();

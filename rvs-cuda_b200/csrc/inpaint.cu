@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(
 // Writes the 2x2 output blocks of the region that hold at least one hole.
 __global__ void inpaint_write_kernel(int wo, int ho, const DevStatus* __restrict__ st,
                                      const uint64_t* __restrict__ codes, uint16_t* __restrict__ out_y,
-                                     uint16_t* __restrict__ out_u, uint16_t* __restrict__ out_v) {
+                                     uint16_t* __restrict__ out_u, uint16_t* __restrict__ out_v, int ties_up) {
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
     const int bx0 = rg.x0 / 2, by0 = rg.y0 / 2;
@@ -402,8 +402,8 @@ __global__ void inpaint_write_kernel(int wo, int ho, const DevStatus* __restrict
                         ((c11 >> 16) & 0xffff);
     const uint32_t sv = (uint32_t)((c00 >> 32) & 0xffff) + ((c01 >> 32) & 0xffff) + ((c10 >> 32) & 0xffff) +
                         ((c11 >> 32) & 0xffff);
-    out_u[co] = (uint16_t)((su + 2) >> 2);
-    out_v[co] = (uint16_t)((sv + 2) >> 2);
+    out_u[co] = quarter_round(su, ties_up);
+    out_v[co] = quarter_round(sv, ties_up);
 }
 
 }  // namespace
@@ -420,7 +420,7 @@ void launch_inpaint(const SynthBuffers& b, const LaunchShape& sh, const DebugPtr
     inpaint_col1_kernel<<<(wo + 31) / 32, 1024, 0, s>>>(wo, ho, b.status, b.codes, b.holes, b.scan_b, b.scan_c,
                                                        b.scan_d, b.scan_a, dbg.inpaint_source);
     inpaint_write_kernel<<<dim3((wo / 2 + 127) / 128, (ho + 1) / 2), 128, 0, s>>>(wo, ho, b.status, b.codes, out_y,
-                                                                               out_u, out_v);
+                                                                               out_u, out_v, sh.chroma_ties_up);
 }
 
 }  // namespace rvsb

@@ -47,6 +47,7 @@ struct LaunchShape {
     int max_blocks;          // largest nbx * nby
     int wo, ho;
     int ntx, nty;
+    int chroma_ties_up;      // output chroma mean: 1 rounds ties up, 0 to even
     int input_w[MAX_VIEWS];  // per view (for the debug copy of warped vertices)
     int input_h[MAX_VIEWS];
     int64_t vert_offset[MAX_VIEWS];  // element offset of each view's vertices in the vertex arena

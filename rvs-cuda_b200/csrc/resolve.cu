@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(256) resolve_kernel(const __grid_constant__ Vi
                 sv += (uint32_t)((code[p] >> 32) & 0xffff);
             }
             const size_t co = (size_t)by * (T.wo / 2) + bx;
-            out_u[co] = (uint16_t)((su + 2) >> 2);
-            out_v[co] = (uint16_t)((sv + 2) >> 2);
+            out_u[co] = quarter_round(su, T.chroma_ties_up);
+            out_v[co] = quarter_round(sv, T.chroma_ties_up);
         }
     }
     // Bounding box of the holes: warp reduction, one atomic per warp.

@@ -50,12 +50,18 @@ bool read_at(const char* path, long offset_per_frame, int frame, std::vector<uin
 
 int main(int argc, char** argv) {
     std::string config_path;
+    int chroma_rounding = RVSB_CHROMA_TIES_EVEN;
     for (int i = 1; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--help")) {
             config_path.clear();
             break;
         }
         if (!std::strcmp(argv[i], "--cuda") || !std::strcmp(argv[i], "--b200")) continue;
+        // Output chroma rounding of an OpenCV built without IPP (ties up).
+        if (!std::strcmp(argv[i], "--chroma-ties-up")) {
+            chroma_rounding = RVSB_CHROMA_TIES_UP;
+            continue;
+        }
         if (!std::strcmp(argv[i], "--opengl") || !std::strcmp(argv[i], "--analyzer")) {
             std::fprintf(stderr, "%s is not supported by this backend\n", argv[i]);
             return 1;
@@ -68,7 +74,7 @@ int main(int argc, char** argv) {
         }
     }
     if (config_path.empty()) {
-        std::fprintf(stderr, "Usage: rvsb CONFIGURATION_FILE [--cuda]\n");
+        std::fprintf(stderr, "Usage: rvsb CONFIGURATION_FILE [--cuda] [--chroma-ties-up]\n");
         return 1;
     }
     char err[1024] = {0};
@@ -87,6 +93,7 @@ int main(int argc, char** argv) {
     rvsb_config_frames(cfg, &start, &n_frames, &n_out);
     rvsb_synth_params params;
     rvsb_config_synth_params(cfg, &params);
+    params.chroma_rounding = chroma_rounding;
     std::vector<rvsb_camera> cams(n_in);
     for (int i = 0; i < n_in; ++i) rvsb_config_input_camera(cfg, i, &cams[i]);
 

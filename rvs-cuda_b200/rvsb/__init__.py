@@ -98,10 +98,15 @@ def status_string(status):
     return load().rvsb_status_string(status).decode()
 
 
-def params(blending_factor=5.0, precision=1.0):
+CHROMA_TIES_EVEN = 0  # output chroma rounding of OpenCV built with IPP
+CHROMA_TIES_UP = 1    # ... and without it
+
+
+def params(blending_factor=5.0, precision=1.0, chroma_rounding=CHROMA_TIES_EVEN):
     p = SynthParams()
     p.blending_factor = blending_factor
     p.precision = precision
+    p.chroma_rounding = chroma_rounding
     return p
 
 

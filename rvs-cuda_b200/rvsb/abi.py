@@ -81,7 +81,8 @@ class SynthParams(ctypes.Structure):
     _fields_ = [
         ("blending_factor", ctypes.c_float),
         ("precision", ctypes.c_float),
-        ("reserved", ctypes.c_int32 * 2),
+        ("chroma_rounding", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

@@ -16,7 +16,7 @@ def to_u16(t, shape):
     return t.cpu().numpy().view(np.uint16).reshape(shape)
 
 
-def gpu_synthesize(ctx, inputs, planes, target, exponent, debug=False, scene=None):
+def gpu_synthesize(ctx, inputs, planes, target, exponent, debug=False, scene=None, params=None):
     """Synthesises `target` on the GPU.  Returns (Y, U, V) uint16 arrays and,
     with debug=True, a dict of intermediate results."""
     import torch
@@ -26,7 +26,7 @@ def gpu_synthesize(ctx, inputs, planes, target, exponent, debug=False, scene=Non
             sc.upload(i, [np.ascontiguousarray(a, np.uint16) for a in p], on_device=False)
     wo, ho = target.width, target.height
     out = yuv_planes_torch(wo, ho)
-    p = rvsb.params(exponent)
+    p = params if params is not None else rvsb.params(exponent)
     dbg = None
     if debug:
         n = len(inputs)
