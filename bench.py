@@ -287,7 +287,7 @@ def main():
     rk = dominant if dominant in algorithmic else "raster"
     achieved = algorithmic[rk] / (stage_avg[rk] / 1000.0) / 1e9
     traffic = None
-    prof_path = os.path.join(ROOT, "profiles", "tile_kernel_traffic.json")
+    prof_path = os.path.join(ROOT, "profiles", "kernel_dram_traffic.json")
     if os.path.exists(prof_path):
         try:
             traffic = json.load(open(prof_path)).get(rk)
