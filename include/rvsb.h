@@ -287,6 +287,23 @@ rvsb_status rvsb_scene_set_profiling(rvsb_scene* scene, int enable);
 int rvsb_scene_stage_times(rvsb_scene* scene, float* ms, int max_stages);
 const char* rvsb_stage_name(int stage);
 
+/* Inpainting sources of a hole mask, computed without allocating memory.
+ * This entry point has no counterpart in the reference.  It runs the
+ * nearest-pixel inpainting scans of the synthesis (compute_nearest,
+ * rvs/src/inpainting.cpp:104-136) over `holes` (width*height bytes in device
+ * memory, nonzero = hole) and writes, for every pixel, the (x, y) of the
+ * pixel whose colour the reference's inpainting copies into it (a non-hole
+ * gets itself) to `sources` (width*height pairs of int32 in device memory).
+ * It is for callers that must not allocate device memory while running;
+ * its scratch is one static device array of 20 MiB, so images are limited
+ * to 524,288 pixels (e.g. 960x540) and larger ones fail with RVSB_E_ARG and
+ * a message in `err`.  The first call on each device (with it current) does
+ * a one-time set-up and should precede any stream capture.  Calls on one
+ * device share the scratch: calls that overlap in time race, so order them
+ * (for example on one stream).  Work is issued on `stream`. */
+rvsb_status rvsb_inpaint_sources_noalloc(const uint8_t* holes, int width, int height, int32_t* sources,
+                                         void* stream, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

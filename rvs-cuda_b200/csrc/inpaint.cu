@@ -423,4 +423,18 @@ void launch_inpaint(const SynthBuffers& b, const LaunchShape& sh, const DebugPtr
                                                                                out_u, out_v, sh.chroma_ties_up);
 }
 
+// The scans alone (no output write) over `holes` with caller-provided
+// scratch: status, codes and four scan buffers of w*h words each; the
+// chosen source of every hole goes to `sources`.
+void launch_inpaint_scans(const DevStatus* st, const uint8_t* holes, uint64_t* codes, uint64_t* const scan[4], int w,
+                          int h, int32_t* sources, cudaStream_t s) {
+    const int rows_per_cta = 8;  // 8 warps of 32
+    inpaint_row0_kernel<<<(h + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(w, h, st, holes, scan[0]);
+    inpaint_col0_kernel<<<(w + 31) / 32, 1024, 0, s>>>(w, h, st, holes, scan[0], scan[1]);
+    inpaint_seed1_kernel<<<dim3((w + 255) / 256, h), 256, 0, s>>>(w, h, st, holes, scan[1], scan[2], scan[3]);
+    inpaint_row1_kernel<<<(h + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(w, h, st, scan[2], scan[0]);
+    inpaint_col1_kernel<<<(w + 31) / 32, 1024, 0, s>>>(w, h, st, codes, holes, scan[1], scan[2], scan[3], scan[0],
+                                                       sources);
+}
+
 }  // namespace rvsb

@@ -59,6 +59,10 @@ struct LaunchShape {
 void launch_decode_color(const uint16_t* y, const uint16_t* u, const uint16_t* v, int w, int h, uint64_t* out,
                          cudaStream_t s);
 
+// Inpainting scans only, on caller-provided scratch (see inpaint.cu).
+void launch_inpaint_scans(const DevStatus* st, const uint8_t* holes, uint64_t* codes, uint64_t* const scan[4], int w,
+                          int h, int32_t* sources, cudaStream_t s);
+
 // `events` (optional) holds 2 * NUM_STAGES events recorded around the stages.
 constexpr int NUM_STAGES = 6;
 int launch_synthesis(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& shape, const DebugPtrs& dbg,

@@ -26,7 +26,7 @@ EXPORTED = [
     "rvsb_config_synth_params", "rvsb_config_virtual_camera_at", "rvsb_relative_pose", "rvsb_scene_create",
     "rvsb_scene_destroy", "rvsb_scene_upload", "rvsb_synthesize", "rvsb_synthesize_host",
     "rvsb_synthesize_debug", "rvsb_synthesize_frame", "rvsb_scene_last_launch_count", "rvsb_scene_set_profiling",
-    "rvsb_scene_stage_times", "rvsb_stage_name",
+    "rvsb_scene_stage_times", "rvsb_stage_name", "rvsb_inpaint_sources_noalloc",
 ]
 
 STAGES = ["warp", "bin", "raster", "inpaint", "total", "resolve"]
@@ -90,6 +90,8 @@ def load():
     L.rvsb_scene_stage_times.argtypes = [c_p, P(ctypes.c_float), ctypes.c_int]
     L.rvsb_stage_name.argtypes = [ctypes.c_int]
     L.rvsb_stage_name.restype = ctypes.c_char_p
+    L.rvsb_inpaint_sources_noalloc.argtypes = [c_p, ctypes.c_int, ctypes.c_int, c_p, c_p, ctypes.c_char_p,
+                                               ctypes.c_size_t]
     _lib = L
     return L
 
@@ -241,6 +243,17 @@ def _stream(s):
     if isinstance(s, int):
         return s
     return s.cuda_stream
+
+
+def inpaint_sources_noalloc(holes, width, height, sources, stream=None):
+    """rvsb_inpaint_sources_noalloc: device hole mask (uint8, nonzero =
+    hole) -> device (x, y) int32 source per pixel, without allocation."""
+    L = load()
+    err = ctypes.create_string_buffer(512)
+    st = L.rvsb_inpaint_sources_noalloc(_ptr(holes), int(width), int(height), _ptr(sources), _stream(stream),
+                                        err, 512)
+    if st != RVSB_OK:
+        raise RvsbError(st, err.value.decode())
 
 
 def relative_pose(cin, cvirt):
