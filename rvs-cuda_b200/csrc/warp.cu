@@ -8,9 +8,9 @@ namespace {
 
 using namespace dev;
 
-constexpr int VT_W = 4 * BLOCK_W;  // vertex tile: 32 x 8 vertices per CTA
-constexpr int VT_H = 2 * BLOCK_H;
-static_assert(VT_W * VT_H == 256, "one vertex per thread");
+constexpr int VT = 32;             // vertex tile: 32 x 32 vertices per CTA
+constexpr int ROWS = VT / 8;       // vertex rows per thread (8 warps)
+static_assert(ROWS == BLOCK_H && VT == 4 * BLOCK_W, "a warp covers one row of 4 binning blocks");
 
 // A vertex can be part of a rasterised triangle only if it passes the
 // emission tests of transform.cpp:161-167 (depth > 0, u > 0) and has finite
@@ -34,90 +34,129 @@ __device__ int4 to_pixel_box(float x0, float y0, float x1, float y1, int wo, int
     return r;
 }
 
-// Grid (ceil(W/32), ceil(H/8), n_views), 256 threads.  Round 1: one vertex
-// per thread, written to the vertex buffer and to shared memory.  Round 2:
-// the extra column and row the tile's blocks need (and, for a horizontal
-// wrap, column W-1) are computed by the first warps, not written.  Then
-// one warp per binning block reduces its (BLOCK_W+1) x (BLOCK_H+1) vertices.
+// Bounding-box contribution of one vertex: (x, y) when it can belong to a
+// rasterised triangle, else NaN (which fminf / fmaxf skip).
+__device__ __forceinline__ float2 box_point(float4 p, bool wrap) {
+    return bbox_vertex_ok(p, wrap) ? make_float2(p.x, p.y) : make_float2(qnan(), qnan());
+}
+
+struct Box {
+    float x0 = INFINITY, y0 = INFINITY, x1 = -INFINITY, y1 = -INFINITY;
+    __device__ void add(float2 q) {
+        x0 = fminf(x0, q.x); y0 = fminf(y0, q.y);
+        x1 = fmaxf(x1, q.x); y1 = fmaxf(y1, q.y);
+    }
+    __device__ void add(const Box& b) {
+        x0 = fminf(x0, b.x0); y0 = fminf(y0, b.y0);
+        x1 = fmaxf(x1, b.x1); y1 = fmaxf(y1, b.y1);
+    }
+    __device__ Box shfl_xor(int o) const {
+        Box b;
+        b.x0 = __shfl_xor_sync(0xffffffffu, x0, o); b.y0 = __shfl_xor_sync(0xffffffffu, y0, o);
+        b.x1 = __shfl_xor_sync(0xffffffffu, x1, o); b.y1 = __shfl_xor_sync(0xffffffffu, y1, o);
+        return b;
+    }
+    __device__ Box shfl_down(int o) const {
+        Box b;
+        b.x0 = __shfl_down_sync(0xffffffffu, x0, o); b.y0 = __shfl_down_sync(0xffffffffu, y0, o);
+        b.x1 = __shfl_down_sync(0xffffffffu, x1, o); b.y1 = __shfl_down_sync(0xffffffffu, y1, o);
+        return b;
+    }
+};
+
+// Grid (ceil(W/32), ceil(H/32), n_views), 256 threads.  Thread (lane, warp)
+// warps the vertices of column j0 + lane, rows i0 + 4*warp .. +3, writes
+// them and keeps the bounding box of its column.  The row below the tile,
+// the column right of it and, for a horizontal wrap, column W-1 are warped
+// as well (not written) and exchanged through shared memory.  Warp `warp`
+// then reduces the boxes of binning-block row by = 8*blockIdx.y + warp: the
+// (BLOCK_W + 1) x (BLOCK_H + 1) vertices of block bx are the columns of
+// lanes 8*b .. 8*b + 8, rows 4*warp .. 4*warp + 4.
 __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ ViewTable tab) {
-    __shared__ float4 sv[VT_H + 1][VT_W + 1];
-    __shared__ float4 sw[VT_H + 1];  // column W-1 (wrap seams)
+    __shared__ float2 s_top[8][VT];        // first row of each warp (row 4*w)
+    __shared__ float2 s_row[VT + 1];       // row i0 + 32, columns j0 .. j0 + 32
+    __shared__ float2 s_col[VT + 1];       // column j0 + 32, rows i0 .. i0 + 32
+    __shared__ float2 s_seam[VT + 1];      // column W - 1, rows i0 .. i0 + 32 (wrap)
     const DevView& V = tab.v[blockIdx.z];
     const DevTarget& T = tab.t;
-    const int j0 = blockIdx.x * VT_W, i0 = blockIdx.y * VT_H;
+    const int j0 = blockIdx.x * VT, i0 = blockIdx.y * VT;
     if (j0 >= V.w || i0 >= V.h) return;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool wrap = T.wrap != 0;
-    const float4 none = make_float4(qnan(), qnan(), qnan(), 0.f);
-    {
-        const int tx = tid % VT_W, ty = tid / VT_W;
-        const int i = i0 + ty, j = j0 + tx;
-        float4 p = none;
+    const bool seam = wrap && blockIdx.x == 0;
+    const int j = j0 + lane;
+    Box col;
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+        const int i = i0 + warp * ROWS + r;
+        float2 q = make_float2(qnan(), qnan());
         if (i < V.h && j < V.w) {
-            p = warp_vertex(V, T, i, j);
+            const float4 p = warp_vertex(V, T, i, j);
             V.vert[(size_t)i * V.w + j] = p;
+            q = box_point(p, wrap);
         }
-        sv[ty][tx] = p;
+        col.add(q);
+        if (r == 0) s_top[warp][lane] = q;
     }
-    // Round 2: row VT_H (VT_W + 1 vertices), column VT_W (VT_H vertices),
-    // column W-1 (VT_H + 1 vertices, wrap only).
-    const int n_extra = (VT_W + 1) + VT_H + ((wrap && blockIdx.x == 0) ? VT_H + 1 : 0);
-    if (tid < n_extra) {
-        int i, j, ty, tx;
-        bool seam = false;
-        if (tid <= VT_W) {
-            ty = VT_H; tx = tid;
-        } else if (tid < VT_W + 1 + VT_H) {
-            ty = tid - (VT_W + 1); tx = VT_W;
-        } else {
-            ty = tid - (VT_W + 1 + VT_H); tx = 0; seam = true;
+    // Extra vertices: warps 0-1 the row below (33), warp 2 the column to the
+    // right (32; its row-32 vertex is the row's last), warps 3-4 the seam.
+    {
+        int i = -1, jj = -1, slot = -1;
+        if (tid <= VT) {
+            i = i0 + VT; jj = j0 + tid; slot = 0;
+        } else if (tid >= 64 && tid < 64 + VT) {
+            i = i0 + (tid - 64); jj = j0 + VT; slot = 1;
+        } else if (seam && tid >= 96 && tid <= 96 + VT) {
+            i = i0 + (tid - 96); jj = V.w - 1; slot = 2;
         }
-        i = i0 + ty;
-        j = seam ? V.w - 1 : j0 + tx;
-        float4 p = none;
-        if (i < V.h && j < V.w) p = warp_vertex(V, T, i, j);
-        if (seam)
-            sw[ty] = p;
-        else
-            sv[ty][tx] = p;
+        if (slot >= 0) {
+            float2 q = make_float2(qnan(), qnan());
+            if (i < V.h && jj < V.w) q = box_point(warp_vertex(V, T, i, jj), wrap);
+            if (slot == 0) {
+                s_row[tid] = q;
+                if (tid == VT) s_col[VT] = q;
+            } else if (slot == 1) {
+                s_col[tid - 64] = q;
+            } else {
+                s_seam[tid - 96] = q;
+            }
+        }
     }
     __syncthreads();
-    // One warp per binning block of the tile (4 x 2 blocks).
-    const int warp = tid >> 5, lane = tid & 31;
-    const int lbx = warp & 3, lby = warp >> 2;
-    const int bx = blockIdx.x * 4 + lbx, by = blockIdx.y * 2 + lby;
-    if (bx >= V.nbx || by >= V.nby) return;
-    float x0 = INFINITY, y0 = INFINITY, x1 = -INFINITY, y1 = -INFINITY;
-    constexpr int NV = (BLOCK_W + 1) * (BLOCK_H + 1);
-    for (int k = lane; k < NV; k += 32) {
-        const int r = lby * BLOCK_H + k / (BLOCK_W + 1), c = lbx * BLOCK_W + k % (BLOCK_W + 1);
-        const float4 p = sv[r][c];
-        if (bbox_vertex_ok(p, wrap)) {
-            x0 = fminf(x0, p.x); y0 = fminf(y0, p.y);
-            x1 = fmaxf(x1, p.x); y1 = fmaxf(y1, p.y);
-        }
-    }
-    if (wrap && bx == 0 && lane <= BLOCK_H) {
-        const float4 p = sw[lby * BLOCK_H + lane];
-        if (bbox_vertex_ok(p, wrap)) {
-            x0 = fminf(x0, p.x); y0 = fminf(y0, p.y);
-            x1 = fmaxf(x1, p.x); y1 = fmaxf(y1, p.y);
-        }
-    }
+    // Row 4*warp + 4 of this column closes the column's box.
+    col.add(warp < 7 ? s_top[warp + 1][lane] : s_row[lane]);
+    // Column 8*b + 8 of each block: the next group's first lane, or the
+    // column right of the tile for the last group.
+    Box right;
+    {
+        const Box nb = col.shfl_down(8);
+        if (lane < 24) {
+            right = nb;
+        } else {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        x0 = fminf(x0, __shfl_xor_sync(0xffffffffu, x0, o));
-        y0 = fminf(y0, __shfl_xor_sync(0xffffffffu, y0, o));
-        x1 = fmaxf(x1, __shfl_xor_sync(0xffffffffu, x1, o));
-        y1 = fmaxf(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+            for (int r = 0; r <= ROWS; ++r) right.add(s_col[warp * ROWS + r]);
+        }
     }
-    if (lane == 0) V.bbox[by * V.nbx + bx] = to_pixel_box(x0, y0, x1, y1, T.wo, T.ho);
+    Box blk = col;
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) blk.add(blk.shfl_xor(o));
+    const int b = lane >> 3;
+    const int bx = blockIdx.x * 4 + b, by = blockIdx.y * 8 + warp;
+    if ((lane & 7) == 0 && bx < V.nbx && by < V.nby) {
+        Box out = blk;
+        out.add(right);
+        if (seam && b == 0) {
+#pragma unroll
+            for (int r = 0; r <= ROWS; ++r) out.add(s_seam[warp * ROWS + r]);
+        }
+        V.bbox[by * V.nbx + bx] = to_pixel_box(out.x0, out.y0, out.x1, out.y1, T.wo, T.ho);
+    }
 }
 
 }  // namespace
 
 void launch_warp(const ViewTable& tab, const LaunchShape& sh, cudaStream_t s) {
-    dim3 grid((sh.max_w + VT_W - 1) / VT_W, (sh.max_h + VT_H - 1) / VT_H, sh.n_views);
+    dim3 grid((sh.max_w + VT - 1) / VT, (sh.max_h + VT - 1) / VT, sh.n_views);
     warp_kernel<<<grid, 256, 0, s>>>(tab);
 }
 
