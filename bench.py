@@ -273,16 +273,19 @@ def main():
     stage_avg = {k: v / args.steps for k, v in stage_acc.items()}
     stage_avg["upload_decode"] = statistics.mean(step_ms) - stage_avg["total"]
     # Algorithmic bytes per launch: warp 14 B per input pixel (depth read +
-    # warped u, v, z write); blend (10N + 4) B per output pixel (per view
-    # colour 3 x u16 + weight fp32, output YUV420 + mask); the raster reads
-    # the warped mesh, 12 B per input pixel.
+    # warped u, v, z write); the raster kernel reads the warped mesh (12 B
+    # per input pixel) and, with the blend fused into it, (10N + 4) B per
+    # output pixel (per view colour 3 x u16 + weight fp32, output YUV420 +
+    # mask); the inpainting passes are charged the output write (4 B per
+    # output pixel).
+    blend_bytes = (10 * n_views + 4) * n_out
     algorithmic = {
         "warp": 14 * n_in,
-        "raster": 12 * n_in,
-        "resolve": (10 * n_views + 4) * n_out,
+        "raster": 12 * n_in + blend_bytes,
+        "inpaint": 4 * n_out,
     }
-    kernel_names = {"warp": "warp_kernel", "raster": "raster_kernel", "resolve": "resolve_kernel"}
-    dominant = max(("warp", "bin", "raster", "resolve", "inpaint"), key=lambda k: stage_avg[k])
+    kernel_names = {"warp": "warp_kernel", "raster": "raster_kernel", "inpaint": "inpaint_*_kernel"}
+    dominant = max(("warp", "bin", "raster", "inpaint"), key=lambda k: stage_avg[k])
     peak, peak_kind = measured_peaks()
     rk = dominant if dominant in algorithmic else "raster"
     achieved = algorithmic[rk] / (stage_avg[rk] / 1000.0) / 1e9
@@ -301,10 +304,6 @@ def main():
     stage_roof = {k: {"ms": stage_avg[k], "GBs": algorithmic[k] / (stage_avg[k] / 1000.0) / 1e9,
                       "frac": algorithmic[k] / (stage_avg[k] / 1000.0) / 1e9 / peak}
                   for k in algorithmic}
-    blend_ms = stage_avg["resolve"] + stage_avg["inpaint"]
-    stage_roof["blend_inpaint_write"] = {
-        "ms": blend_ms, "GBs": algorithmic["resolve"] / (blend_ms / 1000.0) / 1e9,
-        "frac": algorithmic["resolve"] / (blend_ms / 1000.0) / 1e9 / peak}
     triangles = 2 * sum((c.width - 1) * (c.height - 1) for c in wl.inputs)
     stage_roof["raster"]["triangles_per_s"] = triangles / (stage_avg["raster"] / 1000.0)
 

@@ -278,9 +278,10 @@ int rvsb_scene_last_launch_count(const rvsb_scene* scene);
 
 /* Per-stage timing with CUDA events recorded on the launch stream (the
  * per-stage timers that replace the reference's whole-run clock(),
- * rvs/src/view_synthesis.cpp:149-166).  Stages: 0 warp, 1 bin, 2 raster,
- * 3 inpaint, 4 whole synthesis, 5 resolve (+ blend + quantise). */
-#define RVSB_NUM_STAGES 6
+ * rvs/src/view_synthesis.cpp:149-166).  Stages: 0 warp, 1 bin, 2 raster
+ * (with the resolve, blend and quantisation of every tile), 3 inpaint,
+ * 4 whole synthesis. */
+#define RVSB_NUM_STAGES 5
 rvsb_status rvsb_scene_set_profiling(rvsb_scene* scene, int enable);
 /* Milliseconds per stage of the most recent profiled synthesis; call after
  * its stream has completed.  Returns the number of values written, or -1. */

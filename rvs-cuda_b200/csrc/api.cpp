@@ -81,7 +81,7 @@ struct DevMem {
 
 struct Workspace {
     int wo = 0, ho = 0;
-    DevMem status, counts, offsets, cursor, list, keys, codes, holes, scan[4], vert, bbox;
+    DevMem status, counts, offsets, cursor, list, codes, holes, scan[4], vert, bbox;
     SynthBuffers b;
     LaunchShape shape{};
     ViewTable table{};
@@ -177,7 +177,6 @@ void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
     ws->cursor.alloc(ctx, nbins * sizeof(int));
     ws->list.alloc(ctx, (size_t)capacity * sizeof(int));
     const size_t npix = (size_t)wo * ho;
-    ws->keys.alloc(ctx, npix * n * sizeof(uint64_t));
     ws->codes.alloc(ctx, npix * sizeof(uint64_t));
     ws->holes.alloc(ctx, npix);
     for (auto& s : ws->scan) s.alloc(ctx, npix * sizeof(uint64_t));
@@ -188,7 +187,6 @@ void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
     b.cursor = ws->cursor.as<int>();
     b.list = ws->list.as<int>();
     b.capacity = capacity;
-    b.keys = ws->keys.as<uint64_t>();
     b.codes = ws->codes.as<uint64_t>();
     b.holes = ws->holes.as<uint8_t>();
     b.scan_a = ws->scan[0].as<uint64_t>();
@@ -526,7 +524,7 @@ int rvsb_scene_stage_times(rvsb_scene* sc, float* ms, int max_stages) {
 }
 
 const char* rvsb_stage_name(int stage) {
-    static const char* names[NUM_STAGES] = {"warp", "bin", "raster", "inpaint", "total", "resolve"};
+    static const char* names[NUM_STAGES] = {"warp", "bin", "raster", "inpaint", "total"};
     return (stage >= 0 && stage < NUM_STAGES) ? names[stage] : "";
 }
 

@@ -16,7 +16,6 @@ struct SynthBuffers {
     int* cursor = nullptr;         // ntiles * n_views
     int* list = nullptr;           // bin list, `capacity` entries
     int capacity = 0;
-    uint64_t* keys = nullptr;      // n_views * Wo*Ho raster keys (winning fragment per pixel)
     uint64_t* codes = nullptr;     // Wo*Ho packed output codes + hole bit
     uint8_t* holes = nullptr;      // Wo*Ho hole mask (1 = no view covers the pixel)
     uint64_t* scan_a = nullptr;    // Wo*Ho inpainting scratch
@@ -64,7 +63,7 @@ void launch_inpaint_scans(const DevStatus* st, const uint8_t* holes, uint64_t* c
                           int h, int32_t* sources, cudaStream_t s);
 
 // `events` (optional) holds 2 * NUM_STAGES events recorded around the stages.
-constexpr int NUM_STAGES = 6;
+constexpr int NUM_STAGES = 5;
 int launch_synthesis(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& shape, const DebugPtrs& dbg,
                      uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t stream,
                      cudaEvent_t* events = nullptr);

@@ -6,9 +6,8 @@ namespace rvsb {
 
 void launch_warp(const ViewTable& tab, const LaunchShape& sh, cudaStream_t s);
 void launch_bin(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, cudaStream_t s);
-void launch_raster(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, cudaStream_t s);
-void launch_resolve(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, const DebugPtrs& dbg,
-                    uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t s);
+void launch_raster(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, const DebugPtrs& dbg,
+                   uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t s);
 void launch_inpaint(const SynthBuffers& b, const LaunchShape& sh, const DebugPtrs& dbg, uint16_t* out_y,
                     uint16_t* out_u, uint16_t* out_v, cudaStream_t s);
 
@@ -41,17 +40,14 @@ int launch_synthesis(const SynthBuffers& b, const ViewTable& tab, const LaunchSh
     launch_bin(b, tab, sh, s);
     mark(3);
     mark(4);
-    launch_raster(b, tab, sh, s);
+    launch_raster(b, tab, sh, dbg, out_y, out_u, out_v, s);
     mark(5);
-    mark(10);
-    launch_resolve(b, tab, sh, dbg, out_y, out_u, out_v, s);
-    mark(11);
     mark(6);
     launch_inpaint(b, sh, dbg, out_y, out_u, out_v, s);
     mark(7);
     mark(9);
     if (cudaPeekAtLastError() != cudaSuccess) return -1;
-    return 1 + 1 + 3 + 1 + 1 + 6;
+    return 1 + 1 + 3 + 1 + 6;
 }
 
 }  // namespace rvsb

@@ -1,8 +1,10 @@
 // Raster stage: one CTA per output tile rasterises every binned input block
-// into 64-bit z-buffers in shared memory (a group of views at a time) and
-// writes each view's final keys (winning fragment per output pixel).
+// into 64-bit z-buffers in shared memory (a group of views at a time),
+// resolves each view's winning fragment per pixel and blends it into the
+// tile's accumulators, then quantises and writes the tile.
 #include "device_common.cuh"
 #include "kernels.hpp"
+#include "resolve.cuh"
 
 namespace rvsb {
 namespace {
@@ -174,27 +176,159 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
     }
 }
 
+constexpr size_t kZbBytes = sizeof(unsigned long long) * VG * TILE * TILE;
+constexpr size_t kEntBytes = sizeof(int) * ENT;
+constexpr size_t kAccBytes = sizeof(float) * 4 * TILE * TILE;
+constexpr size_t kSmemBytes = kZbBytes + kEntBytes + kAccBytes;
+
+// Resolves and blends the views g0 .. g0 + gn - 1 of the tile, one pixel per
+// thread and step, into the accumulators (c0, c1, c2, q per pixel).
+__device__ __forceinline__ void resolve_group(const ViewTable& tab, int g0, int gn, int tx0, int ty0,
+                                              const unsigned long long (*zb)[TILE * TILE], float (*acc)[TILE * TILE],
+                                              const DebugPtrs& dbg) {
+    const DevTarget& T = tab.t;
+    const size_t npo = (size_t)T.wo * T.ho;
+    for (int p = threadIdx.x; p < TILE * TILE; p += TILE_THREADS) {
+        const int x = tx0 + (p & (TILE - 1)), y = ty0 + p / TILE;
+        if (x >= T.wo || y >= T.ho) continue;
+        BlendAcc a = {0.f, 0.f, 0.f, 0.f};
+        if (g0 > 0) {
+            a.c0 = acc[0][p]; a.c1 = acc[1][p]; a.c2 = acc[2][p]; a.q = acc[3][p];
+        }
+        for (int k = 0; k < gn; ++k) {
+            const int v = g0 + k;
+            const Fragment f = resolve_fragment(tab.v[v], zb[k][p], x, y);
+            const float qv = __fdiv_rn(f.validity, f.depth);
+            if (dbg.view_color || dbg.view_depth || dbg.view_validity) {
+                const size_t o = (size_t)y * T.wo + x;
+                if (dbg.view_color) {
+                    float* c = dbg.view_color + ((size_t)v * npo + o) * 3;
+                    c[0] = f.col.x; c[1] = f.col.y; c[2] = f.col.z;
+                }
+                if (dbg.view_depth) dbg.view_depth[(size_t)v * npo + o] = f.depth;
+                if (dbg.view_validity) dbg.view_validity[(size_t)v * npo + o] = f.validity;
+            }
+            blend_view(a, v, f, qv, T);
+        }
+        acc[0][p] = a.c0; acc[1][p] = a.c1; acc[2][p] = a.c2; acc[3][p] = a.q;
+    }
+}
+
+// Quantises the tile (image_writing.cpp:142-180), one 2x2 block per thread:
+// packed codes and the hole mask for the inpainting passes, the 4:2:0
+// samples of blocks without holes, and the bounding box of the holes.
+__device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0, const float (*acc)[TILE * TILE],
+                                          DevStatus* st, uint64_t* codes, uint8_t* holes, uint16_t* out_y,
+                                          uint16_t* out_u, uint16_t* out_v, const DebugPtrs& dbg) {
+    const int t = threadIdx.x;
+    const int lx = 2 * (t % (TILE / 2)), ly = 2 * (t / (TILE / 2));
+    const int x0 = tx0 + lx, y0 = ty0 + ly;
+    const bool inside = x0 < T.wo && y0 < T.ho;
+    uint64_t code[4] = {0, 0, 0, 0};
+    bool any_hole = false;
+    if (inside) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int sp = (ly + (p >> 1)) * TILE + lx + (p & 1);
+            const float c0 = acc[0][sp], c1 = acc[1][sp], c2 = acc[2][sp], q = acc[3][sp];
+            const bool hole = !(q > 0.f);
+            any_hole |= hole;
+            code[p] = (uint64_t)quantize(c0, T.max_val) | ((uint64_t)quantize(c1, T.max_val) << 16) |
+                      ((uint64_t)quantize(c2, T.max_val) << 32) | (hole ? kHoleBit : 0ull);
+            const int x = x0 + (p & 1), y = y0 + (p >> 1);
+            const size_t o = (size_t)y * T.wo + x;
+            if (dbg.blend_color) {
+                dbg.blend_color[o * 3 + 0] = c0;
+                dbg.blend_color[o * 3 + 1] = c1;
+                dbg.blend_color[o * 3 + 2] = c2;
+            }
+            if (dbg.blend_quality) dbg.blend_quality[o] = (T.n_views == 1 || !(q > 0.f)) ? q : powf(q, T.inv_blend_exp);
+            if (dbg.inpaint_source) {
+                dbg.inpaint_source[o * 2 + 0] = x;
+                dbg.inpaint_source[o * 2 + 1] = y;
+            }
+        }
+        const size_t o = (size_t)y0 * T.wo + x0;
+        reinterpret_cast<ulonglong2*>(codes + o)[0] = make_ulonglong2(code[0], code[1]);
+        reinterpret_cast<ulonglong2*>(codes + o + T.wo)[0] = make_ulonglong2(code[2], code[3]);
+        auto hole_of = [](uint64_t c) -> uint16_t { return (c & kHoleBit) ? 1 : 0; };
+        reinterpret_cast<uint16_t*>(holes + o)[0] = (uint16_t)(hole_of(code[0]) | (hole_of(code[1]) << 8));
+        reinterpret_cast<uint16_t*>(holes + o + T.wo)[0] = (uint16_t)(hole_of(code[2]) | (hole_of(code[3]) << 8));
+        if (!any_hole) {
+            reinterpret_cast<uint32_t*>(out_y + o)[0] = (uint32_t)(code[0] & 0xffff) | ((uint32_t)(code[1] & 0xffff) << 16);
+            reinterpret_cast<uint32_t*>(out_y + o + T.wo)[0] =
+                (uint32_t)(code[2] & 0xffff) | ((uint32_t)(code[3] & 0xffff) << 16);
+            uint32_t su = 0, sv = 0;
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                su += (uint32_t)((code[p] >> 16) & 0xffff);
+                sv += (uint32_t)((code[p] >> 32) & 0xffff);
+            }
+            const size_t co = (size_t)(y0 / 2) * (T.wo / 2) + x0 / 2;
+            out_u[co] = quarter_round(su, T.chroma_ties_up);
+            out_v[co] = quarter_round(sv, T.chroma_ties_up);
+        }
+    }
+    // Bounding box of the holes: warp reduction, one atomic per warp.
+    int hx0 = INT_MAX, hy0 = INT_MAX, hx1 = INT_MIN, hy1 = INT_MIN;
+    if (any_hole) {
+        const bool left = (code[0] & kHoleBit) || (code[2] & kHoleBit);
+        const bool right = (code[1] & kHoleBit) || (code[3] & kHoleBit);
+        const bool top = (code[0] & kHoleBit) || (code[1] & kHoleBit);
+        const bool bottom = (code[2] & kHoleBit) || (code[3] & kHoleBit);
+        hx0 = left ? x0 : x0 + 1;
+        hx1 = right ? x0 + 1 : x0;
+        hy0 = top ? y0 : y0 + 1;
+        hy1 = bottom ? y0 + 1 : y0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, any_hole);
+    if (m) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            hx0 = min(hx0, __shfl_xor_sync(0xffffffffu, hx0, o));
+            hy0 = min(hy0, __shfl_xor_sync(0xffffffffu, hy0, o));
+            hx1 = max(hx1, __shfl_xor_sync(0xffffffffu, hx1, o));
+            hy1 = max(hy1, __shfl_xor_sync(0xffffffffu, hy1, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&st->hole_x0, hx0);
+            atomicMin(&st->hole_y0, hy0);
+            atomicMax(&st->hole_x1, hx1);
+            atomicMax(&st->hole_y1, hy1);
+            atomicAdd(&st->n_holes, 1);
+        }
+    }
+}
+
 // Grid: one CTA per TILE x TILE output tile.  Views are processed in groups
 // of VG: clear the group's shared z-buffers, stage the group's bin entries
 // (view, block) in shared memory, rasterise them (one warp per block), then
-// write the keys of the tile for each view of the group.
+// resolve and blend the group's views into the tile's accumulators.  After
+// the last group the tile is quantised and written.
 __global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_constant__ ViewTable tab,
                                                                   const int* __restrict__ counts,
                                                                   const int* __restrict__ offsets,
                                                                   const int* __restrict__ list,
-                                                                  const DevStatus* __restrict__ st,
-                                                                  uint64_t* __restrict__ keys) {
-    __shared__ unsigned long long zb[VG][TILE * TILE];
+                                                                  DevStatus* __restrict__ st,
+                                                                  uint64_t* __restrict__ codes,
+                                                                  uint8_t* __restrict__ holes,
+                                                                  uint16_t* __restrict__ out_y,
+                                                                  uint16_t* __restrict__ out_u,
+                                                                  uint16_t* __restrict__ out_v, DebugPtrs dbg) {
+    // Dynamic shared memory: the group's z-buffers, the staged bin entries
+    // and the tile's blend accumulators.
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    auto zb = reinterpret_cast<unsigned long long(*)[TILE * TILE]>(s_raw);
+    int* s_ent = reinterpret_cast<int*>(s_raw + kZbBytes);
+    auto acc = reinterpret_cast<float(*)[TILE * TILE]>(s_raw + kZbBytes + kEntBytes);
     __shared__ int s_pref[VG + 1];
     __shared__ int s_off[VG];
-    __shared__ int s_ent[ENT];
     const DevTarget& T = tab.t;
     const int tile = blockIdx.x;
     const int tx0 = (tile % T.ntx) * TILE, ty0 = (tile / T.ntx) * TILE;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool overflow = st->bin_overflow != 0;
     const bool wrap = T.wrap != 0;
-    const size_t npo = (size_t)T.wo * T.ho;
 
     for (int g0 = 0; g0 < T.n_views; g0 += VG) {
         const int gn = min(VG, T.n_views - g0);
@@ -241,19 +375,22 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_co
             }
             __syncthreads();
         }
-        for (int k = 0; k < gn; ++k)
-            for (int p = tid; p < TILE * TILE; p += TILE_THREADS) {
-                const int x = tx0 + (p & (TILE - 1)), y = ty0 + p / TILE;
-                if (x < T.wo && y < T.ho) keys[(size_t)(g0 + k) * npo + (size_t)y * T.wo + x] = zb[k][p];
-            }
+        resolve_group(tab, g0, gn, tx0, ty0, zb, acc, dbg);
         __syncthreads();
     }
+    write_tile(T, tx0, ty0, acc, st, codes, holes, out_y, out_u, out_v, dbg);
 }
 
 }  // namespace
 
-void launch_raster(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, cudaStream_t s) {
-    raster_kernel<<<sh.ntx * sh.nty, TILE_THREADS, 0, s>>>(tab, b.counts, b.offsets, b.list, b.status, b.keys);
+void launch_raster(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, const DebugPtrs& dbg,
+                   uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t s) {
+    static_assert(kZbBytes % 16 == 0 && kEntBytes % 16 == 0, "shared-memory carve alignment");
+    // The attribute is per function and device; setting it before each
+    // launch is a cheap host call and keeps multi-device use correct.
+    cudaFuncSetAttribute(raster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    raster_kernel<<<sh.ntx * sh.nty, TILE_THREADS, kSmemBytes, s>>>(tab, b.counts, b.offsets, b.list, b.status,
+                                                                     b.codes, b.holes, out_y, out_u, out_v, dbg);
 }
 
 }  // namespace rvsb

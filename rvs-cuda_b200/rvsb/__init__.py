@@ -29,7 +29,7 @@ EXPORTED = [
     "rvsb_scene_stage_times", "rvsb_stage_name", "rvsb_inpaint_sources_noalloc",
 ]
 
-STAGES = ["warp", "bin", "raster", "inpaint", "total", "resolve"]
+STAGES = ["warp", "bin", "raster", "inpaint", "total"]
 
 _lib = None
 
