@@ -172,6 +172,42 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world):
+    """Views/s of rvsb_synthesize_batch on the resident scene: `slots` seeded
+    poses of the same distribution per batch (one CUDA graph replay), inputs
+    resident, L2 flushed between batches outside the timed events."""
+    import torch
+    import rvsb
+    from rvsb import scenes
+    targets = scenes.plain_1080p(n_targets=slots + 1).targets[1:]
+    p = rvsb.params(wl.blending_factor)
+    batch = rvsb.Batch(scene, slots, graphs=True)
+    batch.reserve(targets[0].width, targets[0].height)
+    outs = [[torch.empty(n, dtype=torch.int16, device="cuda")
+             for n in (c.width * c.height, (c.width // 2) * (c.height // 2), (c.width // 2) * (c.height // 2))]
+            for c in targets]
+    for _ in range(3):
+        batch.synthesize(targets, p, outs, stream=stream)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch.synthesize(targets, p, outs, stream=stream)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    launches = batch.last_launch_count()
+    batch.close()
+    from rvsb import replicas
+    total = replicas.max_over_ranks(sum(ms) / 1000.0, world)
+    return {"value": world * slots * steps / total, "unit": UNIT, "slots": slots, "batches": steps,
+            "ms_per_batch": statistics.mean(ms), "ms_per_view": statistics.mean(ms) / slots,
+            "launches_per_batch": launches, "graphs": True,
+            "workload": f"plain_1080p scene, {slots} seeded poses per batch"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -180,6 +216,8 @@ def main():
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--e2e-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-slots", type=int, default=16)
+    ap.add_argument("--batch-steps", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -264,6 +302,7 @@ def main():
     barrier(world)
     e2e_total = allreduce_max(sum(e2e_ms) / 1000.0, world)
     e2e_value = world * args.e2e_steps / e2e_total
+    batched = measure_batched(ctx, scene, wl, args.batch_slots, args.batch_steps, flush, stream, world)
     clocks = sampler.stop()
 
     # Roofline of the dominant kernel (per launch, averaged over the timed steps).
@@ -327,6 +366,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "p50_ms": percentile(e2e_ms, 50), "p99_ms": percentile(e2e_ms, 99),
                     "call": "rvsb_synthesize_host (pinned host buffers)"},
+            "batched": batched,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,

@@ -276,6 +276,36 @@ rvsb_status rvsb_synthesize_debug(rvsb_scene* scene, const rvsb_camera* virt,
  * (for launch accounting). */
 int rvsb_scene_last_launch_count(const rvsb_scene* scene);
 
+/* ----------------------------------------------------------------------- */
+/* Batches: many virtual views of one resident scene                       */
+/* ----------------------------------------------------------------------- */
+
+/* The reference synthesises one virtual view per Pipeline::computeView call
+ * (rvs/src/Pipeline.cpp:169-345), frame after frame.  A batch runs up to
+ * `max_slots` virtual views of the same uploaded input views together: each
+ * kernel covers every slot in one launch, so a group of views costs the
+ * launches of one view, and with graphs enabled the group's launch sequence
+ * is captured once per shape and replayed.  Outputs are identical to one
+ * rvsb_synthesize call per view.  Each slot holds its own workspace (grown
+ * on first use, or up front with rvsb_batch_reserve).  Calls on one batch
+ * must be ordered (one stream, or the caller waits between them). */
+typedef struct rvsb_batch rvsb_batch;
+
+rvsb_status rvsb_batch_create(rvsb_scene* scene, int max_slots, rvsb_batch** out);
+void rvsb_batch_destroy(rvsb_batch* batch);
+/* Allocates every slot's workspace for outputs up to max_width x max_height
+ * now, so later calls of that size do not allocate. */
+rvsb_status rvsb_batch_reserve(rvsb_batch* batch, int max_width, int max_height);
+/* Capture each batch shape into a CUDA graph and replay it (default off). */
+rvsb_status rvsb_batch_set_graphs(rvsb_batch* batch, int enable);
+/* n virtual views (outputs may differ in size and projection), processed in
+ * groups of max_slots on `stream`. */
+rvsb_status rvsb_synthesize_batch(rvsb_batch* batch, const rvsb_camera* virts, int n,
+                                  const rvsb_synth_params* params, const rvsb_yuv420* outs, void* stream);
+int rvsb_batch_last_launch_count(const rvsb_batch* batch);
+rvsb_status rvsb_batch_set_profiling(rvsb_batch* batch, int enable);
+int rvsb_batch_stage_times(rvsb_batch* batch, float* ms, int max_stages);
+
 /* Per-stage timing with CUDA events recorded on the launch stream (the
  * per-stage timers that replace the reference's whole-run clock(),
  * rvs/src/view_synthesis.cpp:149-166).  Stages: 0 warp, 1 bin, 2 raster

@@ -10,102 +10,16 @@
 #include <vector>
 
 #include "camera.hpp"
+#include "engine.hpp"
 #include "frontend.hpp"
 #include "kernels.hpp"
 #include "rvsb.h"
 
 using namespace rvsb;
 
-struct rvsb_context {
-    int device = 0;
-    size_t budget = 0;
-    size_t in_use = 0;
-    std::string last_error;
-    std::mutex mu;
-    rvsb_scene* host_scene = nullptr;  // scene reused by rvsb_synthesize_host
-    void* host_out = nullptr;          // device output staging of rvsb_synthesize_host
-    size_t host_out_bytes = 0;
-};
-
-namespace {
-
-struct CudaError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-struct BudgetError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-struct ArgError : std::runtime_error {
-    using std::runtime_error::runtime_error;
-};
-
-void check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-// Device allocation counted against the context's HBM budget.
-struct DevMem {
-    rvsb_context* ctx = nullptr;
-    void* ptr = nullptr;
-    size_t bytes = 0;
-
-    DevMem() = default;
-    DevMem(const DevMem&) = delete;
-    DevMem& operator=(const DevMem&) = delete;
-    ~DevMem() { release(); }
-
-    void alloc(rvsb_context* c, size_t n) {
-        release();
-        if (n == 0) n = 16;
-        if (c->in_use + n > c->budget)
-            throw BudgetError("request of " + std::to_string(n) + " bytes exceeds the HBM budget (" +
-                              std::to_string(c->in_use) + " of " + std::to_string(c->budget) + " in use)");
-        check(cudaMalloc(&ptr, n), "cudaMalloc");
-        ctx = c;
-        bytes = n;
-        c->in_use += n;
-    }
-    void release() {
-        if (ptr) {
-            cudaFree(ptr);
-            ctx->in_use -= bytes;
-        }
-        ptr = nullptr;
-        bytes = 0;
-    }
-    template <class T>
-    T* as() const {
-        return static_cast<T*>(ptr);
-    }
-};
-
-struct Workspace {
-    int wo = 0, ho = 0;
-    DevMem status, counts, offsets, cursor, list, codes, holes, scan[4], vert, bbox;
-    SynthBuffers b;
-    LaunchShape shape{};
-    ViewTable table{};
-    std::vector<int64_t> vert_off, bbox_off;
-};
-
-}  // namespace
-
-struct rvsb_scene {
-    rvsb_context* ctx = nullptr;
-    std::vector<rvsb_camera> cams;
-    std::vector<std::unique_ptr<DevMem>> planes;  // 4 per view: y, u, v, depth
-    std::vector<std::unique_ptr<DevMem>> erp;     // 2 per view: rows, cols (ERP inputs)
-    std::vector<std::unique_ptr<DevMem>> color;   // 1 per view: decoded colour words
-    std::vector<bool> uploaded;
-    std::unique_ptr<Workspace> ws;
-    int last_launches = 0;
-    bool profiling = false;
-    bool profiled = false;
-    cudaEvent_t events[2 * NUM_STAGES] = {};
-    ~rvsb_scene() {
-        for (auto& e : events)
-            if (e) cudaEventDestroy(e);
-    }
+struct rvsb_batch {
+    rvsb_scene* scene = nullptr;
+    std::unique_ptr<BatchCore> core;
 };
 
 namespace {
@@ -143,141 +57,6 @@ size_t plane_bytes(const rvsb_camera& c, int k) {
     return (k == 1 || k == 2) ? (size_t)(c.width / 2) * (c.height / 2) * 2 : n * 2;
 }
 
-int nblocks_x(int w) { return (w - 1 + BLOCK_W - 1) / BLOCK_W; }
-int nblocks_y(int h) { return (h - 1 + BLOCK_H - 1) / BLOCK_H; }
-
-void ensure_workspace(rvsb_scene* sc, int wo, int ho) {
-    if (sc->ws && sc->ws->wo == wo && sc->ws->ho == ho) return;
-    sc->ws.reset();
-    auto ws = std::make_unique<Workspace>();
-    rvsb_context* ctx = sc->ctx;
-    const int n = (int)sc->cams.size();
-    ws->wo = wo;
-    ws->ho = ho;
-    int64_t nvert = 0, nbb = 0;
-    int max_w = 0, max_h = 0, max_blocks = 0;
-    for (const auto& c : sc->cams) {
-        ws->vert_off.push_back(nvert);
-        ws->bbox_off.push_back(nbb);
-        nvert += (int64_t)c.width * c.height;
-        const int nb = nblocks_x(c.width) * nblocks_y(c.height);
-        nbb += nb;
-        max_w = std::max(max_w, c.width);
-        max_h = std::max(max_h, c.height);
-        max_blocks = std::max(max_blocks, nb);
-    }
-    const int ntx = (wo + TILE - 1) / TILE, nty = (ho + TILE - 1) / TILE;
-    const size_t nbins = (size_t)ntx * nty * n;
-    const int capacity = (int)std::min<int64_t>(INT32_MAX / 2, std::max<int64_t>(1 << 16, nbb * 8 + nbins));
-    ws->vert.alloc(ctx, (size_t)nvert * sizeof(float4));
-    ws->bbox.alloc(ctx, (size_t)nbb * sizeof(int4));
-    ws->status.alloc(ctx, sizeof(DevStatus));
-    ws->counts.alloc(ctx, nbins * sizeof(int));
-    ws->offsets.alloc(ctx, nbins * sizeof(int));
-    ws->cursor.alloc(ctx, nbins * sizeof(int));
-    ws->list.alloc(ctx, (size_t)capacity * sizeof(int));
-    const size_t npix = (size_t)wo * ho;
-    ws->codes.alloc(ctx, npix * sizeof(uint64_t));
-    ws->holes.alloc(ctx, npix);
-    for (auto& s : ws->scan) s.alloc(ctx, npix * sizeof(uint64_t));
-    SynthBuffers& b = ws->b;
-    b.status = ws->status.as<DevStatus>();
-    b.counts = ws->counts.as<int>();
-    b.offsets = ws->offsets.as<int>();
-    b.cursor = ws->cursor.as<int>();
-    b.list = ws->list.as<int>();
-    b.capacity = capacity;
-    b.codes = ws->codes.as<uint64_t>();
-    b.holes = ws->holes.as<uint8_t>();
-    b.scan_a = ws->scan[0].as<uint64_t>();
-    b.scan_b = ws->scan[1].as<uint64_t>();
-    b.scan_c = ws->scan[2].as<uint64_t>();
-    b.scan_d = ws->scan[3].as<uint64_t>();
-    LaunchShape& sh = ws->shape;
-    sh.n_views = n;
-    sh.max_w = max_w;
-    sh.max_h = max_h;
-    sh.max_blocks = max_blocks;
-    sh.wo = wo;
-    sh.ho = ho;
-    sh.ntx = ntx;
-    sh.nty = nty;
-    for (int v = 0; v < n && v < MAX_VIEWS; ++v) {
-        sh.input_w[v] = sc->cams[v].width;
-        sh.input_h[v] = sc->cams[v].height;
-        sh.vert_offset[v] = ws->vert_off[v];
-    }
-    sc->ws = std::move(ws);
-}
-
-void fill_tables(rvsb_scene* sc, const rvsb_camera& virt, const rvsb_synth_params& p) {
-    Workspace& ws = *sc->ws;
-    const int n = (int)sc->cams.size();
-    for (int v = 0; v < n; ++v) {
-        const rvsb_camera& c = sc->cams[v];
-        DevView& V = ws.table.v[v];
-        std::memset(&V, 0, sizeof(V));
-        V.w = c.width;
-        V.h = c.height;
-        V.proj = c.projection;
-        V.bits_color = c.bit_depth_color;
-        V.f0 = c.focal[0];
-        V.f1 = c.focal[1];
-        V.p0 = c.principle_point[0];
-        V.p1 = c.principle_point[1];
-        V.near_ = c.depth_range[0];
-        V.far_ = c.depth_range[1];
-        V.depth_scale = 1.0f / (float)((1u << c.bit_depth_depth) - 1u);
-        V.has_invalid = c.has_invalid_depth;
-        V.color_scale = 1.0f / (float)((1u << c.bit_depth_color) - 1u);
-        V.cw = c.width / 2;
-        V.ch = c.height / 2;
-        V.chroma_sx = (float)V.cw / c.width;
-        V.chroma_sy = (float)V.ch / c.height;
-        relative_pose(c, virt, V.R, V.t);
-        V.py = sc->planes[v * 4 + 0]->as<uint16_t>();
-        V.pu = sc->planes[v * 4 + 1]->as<uint16_t>();
-        V.pv = sc->planes[v * 4 + 2]->as<uint16_t>();
-        V.pd = sc->planes[v * 4 + 3]->as<uint16_t>();
-        if (c.projection == RVSB_PROJ_EQUIRECTANGULAR) {
-            V.erp_row = sc->erp[v * 2 + 0]->as<float>();
-            V.erp_col = sc->erp[v * 2 + 1]->as<float>();
-        }
-        V.color = sc->color[v]->as<uint64_t>();
-        V.vert = ws.vert.as<float4>() + ws.vert_off[v];
-        V.bbox = ws.bbox.as<int4>() + ws.bbox_off[v];
-        V.tri_shift = 2;
-        while ((1 << (V.tri_shift - 2)) < c.width - 1) ++V.tri_shift;
-        V.nbx = nblocks_x(c.width);
-        V.nby = nblocks_y(c.height);
-    }
-    DevTarget& T = ws.table.t;
-    std::memset(&T, 0, sizeof(T));
-    T.wo = virt.width;
-    T.ho = virt.height;
-    T.proj = virt.projection;
-    T.wrap = (virt.projection == RVSB_PROJ_EQUIRECTANGULAR && virt.full_hor_range) ? 1 : 0;
-    T.f0 = virt.focal[0];
-    T.f1 = virt.focal[1];
-    T.p0 = virt.principle_point[0];
-    T.p1 = virt.principle_point[1];
-    if (virt.projection == RVSB_PROJ_EQUIRECTANGULAR) erp_projector_constants(virt, T.u0, T.v0, T.du_dphi, T.dv_dtheta);
-    T.bits = virt.bit_depth_color;
-    T.max_val = (1u << virt.bit_depth_color) - 1u;
-    T.blend_exp = p.blending_factor;
-    T.inv_blend_exp = 1.0f / p.blending_factor;
-    T.blend_exp_int = 0;
-    if (p.blending_factor == std::floor(p.blending_factor) && p.blending_factor >= 2.f && p.blending_factor <= 16.f)
-        T.blend_exp_int = (int)p.blending_factor;
-    T.chroma_ties_up = p.chroma_rounding == RVSB_CHROMA_TIES_UP;
-    sc->ws->shape.chroma_ties_up = T.chroma_ties_up;
-
-    T.ntx = ws.shape.ntx;
-    T.nty = ws.shape.nty;
-    T.n_views = n;
-    T.bin_capacity = ws.b.capacity;
-}
-
 void validate_params(const rvsb_synth_params* p) {
     if (!p) throw ArgError("null synthesis parameters");
     if (!(p->blending_factor > 0.f) || !std::isfinite(p->blending_factor))
@@ -288,6 +67,19 @@ void validate_params(const rvsb_synth_params* p) {
     if (p->reserved != 0) throw ArgError("reserved synthesis parameter must be 0");
 }
 
+void validate_request(const rvsb_scene* sc, const rvsb_camera* virt, const rvsb_synth_params* params,
+                      const rvsb_yuv420* out) {
+    if (!virt || !out || !out->y || !out->u || !out->v) throw ArgError("null camera or output planes");
+    validate_params(params);
+    if (const char* why = camera_problem(*virt, true)) throw ArgError(std::string("virtual camera: ") + why);
+    (void)sc;
+}
+
+BatchCore& single_core(rvsb_scene* sc) {
+    if (!sc->single) sc->single = std::make_unique<BatchCore>(sc->ctx, 1);
+    return *sc->single;
+}
+
 // `frame` (optional): raw device planes of every input view for this call;
 // their colour is decoded into the scene and their depth read in place.
 rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_synth_params* params,
@@ -296,9 +88,7 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
     if (!sc) return RVSB_E_ARG;
     rvsb_context* ctx = sc->ctx;
     return guarded(ctx, [&]() -> rvsb_status {
-        if (!virt || !out || !out->y || !out->u || !out->v) throw ArgError("null camera or output planes");
-        validate_params(params);
-        if (const char* why = camera_problem(*virt, true)) throw ArgError(std::string("virtual camera: ") + why);
+        validate_request(sc, virt, params, out);
         if (frame) {
             for (size_t v = 0; v < sc->cams.size(); ++v)
                 if (!frame[v].y || !frame[v].u || !frame[v].v || !frame[v].depth) throw ArgError("null plane");
@@ -307,41 +97,41 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
                 if (!sc->uploaded[v]) throw ArgError("input view " + std::to_string(v) + " was not uploaded");
         }
         check(cudaSetDevice(ctx->device), "cudaSetDevice");
-        ensure_workspace(sc, virt->width, virt->height);
-        Workspace& ws = *sc->ws;
-        fill_tables(sc, *virt, *params);
         cudaStream_t s = static_cast<cudaStream_t>(stream);
+        BatchCore& core = single_core(sc);
         int decodes = 0;
         if (frame) {
             for (size_t v = 0; v < sc->cams.size(); ++v) {
                 const rvsb_camera& c = sc->cams[v];
                 launch_decode_color(frame[v].y, frame[v].u, frame[v].v, c.width, c.height,
                                     sc->color[v]->as<uint64_t>(), s);
-                ws.table.v[v].pd = frame[v].depth;
                 ++decodes;
             }
             check(cudaPeekAtLastError(), "decode colour");
         }
-        DebugPtrs dbg;
+        SlotRequest r;
+        r.scene = sc;
+        r.virt = *virt;
+        r.params = *params;
+        r.out = *out;
+        r.frame = frame;
         if (dbg_out) {
-            dbg.warped_uvz = dbg_out->warped_uvz;
-            dbg.view_color = dbg_out->view_color;
-            dbg.view_depth = dbg_out->view_depth;
-            dbg.view_validity = dbg_out->view_validity;
-            dbg.blend_color = dbg_out->blend_color;
-            dbg.blend_quality = dbg_out->blend_quality;
-            dbg.inpaint_source = dbg_out->inpaint_source;
+            r.dbg.warped_uvz = dbg_out->warped_uvz;
+            r.dbg.view_color = dbg_out->view_color;
+            r.dbg.view_depth = dbg_out->view_depth;
+            r.dbg.view_validity = dbg_out->view_validity;
+            r.dbg.blend_color = dbg_out->blend_color;
+            r.dbg.blend_quality = dbg_out->blend_quality;
+            r.dbg.inpaint_source = dbg_out->inpaint_source;
         }
-        int launches = launch_synthesis(ws.b, ws.table, ws.shape, dbg, out->y, out->u, out->v, s,
-                                        sc->profiling ? sc->events : nullptr);
-        sc->profiled = sc->profiling;
-        if (launches < 0) check(cudaGetLastError(), "kernel launch");
-        if (dbg.warped_uvz) {
+        const int launches = core.run(&r, 1, s);
+        if (r.dbg.warped_uvz) {
             size_t off = 0;
+            SlotWorkspace& ws = core.workspace(0);
             for (size_t v = 0; v < sc->cams.size(); ++v) {
                 const size_t nv = (size_t)sc->cams[v].width * sc->cams[v].height;
-                check(cudaMemcpyAsync(dbg.warped_uvz + off * 4, ws.vert.as<float4>() + ws.vert_off[v],
-                                      nv * sizeof(float4), cudaMemcpyDeviceToDevice, s),
+                check(cudaMemcpyAsync(r.dbg.warped_uvz + off * 4, ws.vert.as<float4>() + off, nv * sizeof(float4),
+                                      cudaMemcpyDeviceToDevice, s),
                       "copy warped vertices");
                 off += nv;
             }
@@ -504,23 +294,95 @@ rvsb_status rvsb_scene_set_profiling(rvsb_scene* sc, int enable) {
     if (!sc) return RVSB_E_ARG;
     return guarded(sc->ctx, [&]() -> rvsb_status {
         check(cudaSetDevice(sc->ctx->device), "cudaSetDevice");
-        if (enable && !sc->events[0])
-            for (auto& e : sc->events) check(cudaEventCreate(&e), "cudaEventCreate");
-        sc->profiling = enable != 0;
+        single_core(sc).set_profiling(enable != 0);
         return RVSB_OK;
     });
 }
 
 int rvsb_scene_stage_times(rvsb_scene* sc, float* ms, int max_stages) {
-    if (!sc || !ms || !sc->profiled) return -1;
-    const int n = std::min(max_stages, (int)NUM_STAGES);
-    for (int k = 0; k < n; ++k) {
-        if (cudaEventElapsedTime(&ms[k], sc->events[2 * k], sc->events[2 * k + 1]) != cudaSuccess) {
-            cudaGetLastError();
-            return -1;
+    if (!sc || !ms || !sc->single) return -1;
+    return sc->single->stage_times(ms, max_stages);
+}
+
+// ---------------------------------------------------------------------------
+// Batches
+// ---------------------------------------------------------------------------
+
+rvsb_status rvsb_batch_create(rvsb_scene* scene, int max_slots, rvsb_batch** out) {
+    if (!scene || !out || max_slots <= 0 || max_slots > 1024) return RVSB_E_ARG;
+    *out = nullptr;
+    return guarded(scene->ctx, [&]() -> rvsb_status {
+        check(cudaSetDevice(scene->ctx->device), "cudaSetDevice");
+        auto b = std::make_unique<rvsb_batch>();
+        b->scene = scene;
+        b->core = std::make_unique<BatchCore>(scene->ctx, max_slots);
+        *out = b.release();
+        return RVSB_OK;
+    });
+}
+
+void rvsb_batch_destroy(rvsb_batch* batch) {
+    if (!batch) return;
+    cudaSetDevice(batch->scene->ctx->device);
+    cudaDeviceSynchronize();
+    delete batch;
+}
+
+rvsb_status rvsb_batch_reserve(rvsb_batch* batch, int max_width, int max_height) {
+    if (!batch || max_width <= 0 || max_height <= 0) return RVSB_E_ARG;
+    return guarded(batch->scene->ctx, [&]() -> rvsb_status {
+        check(cudaSetDevice(batch->scene->ctx->device), "cudaSetDevice");
+        for (int k = 0; k < batch->core->slots(); ++k)
+            batch->core->workspace(k).ensure(batch->scene->ctx, batch->scene, max_width, max_height);
+        return RVSB_OK;
+    });
+}
+
+rvsb_status rvsb_batch_set_graphs(rvsb_batch* batch, int enable) {
+    if (!batch) return RVSB_E_ARG;
+    batch->core->set_graphs(enable != 0);
+    return RVSB_OK;
+}
+
+rvsb_status rvsb_batch_set_profiling(rvsb_batch* batch, int enable) {
+    if (!batch) return RVSB_E_ARG;
+    return guarded(batch->scene->ctx, [&]() -> rvsb_status {
+        check(cudaSetDevice(batch->scene->ctx->device), "cudaSetDevice");
+        batch->core->set_profiling(enable != 0);
+        return RVSB_OK;
+    });
+}
+
+int rvsb_batch_stage_times(rvsb_batch* batch, float* ms, int max_stages) {
+    return batch ? batch->core->stage_times(ms, max_stages) : -1;
+}
+
+int rvsb_batch_last_launch_count(const rvsb_batch* batch) { return batch ? batch->core->last_launches() : 0; }
+
+rvsb_status rvsb_synthesize_batch(rvsb_batch* batch, const rvsb_camera* virts, int n,
+                                  const rvsb_synth_params* params, const rvsb_yuv420* outs, void* stream) {
+    if (!batch || !virts || !outs || n <= 0) return RVSB_E_ARG;
+    rvsb_scene* sc = batch->scene;
+    return guarded(sc->ctx, [&]() -> rvsb_status {
+        for (size_t v = 0; v < sc->cams.size(); ++v)
+            if (!sc->uploaded[v]) throw ArgError("input view " + std::to_string(v) + " was not uploaded");
+        for (int k = 0; k < n; ++k) validate_request(sc, &virts[k], params, &outs[k]);
+        check(cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        BatchCore& core = *batch->core;
+        std::vector<SlotRequest> reqs(std::min(n, core.slots()));
+        for (int k0 = 0; k0 < n; k0 += core.slots()) {
+            const int m = std::min(core.slots(), n - k0);
+            for (int k = 0; k < m; ++k) {
+                reqs[k].scene = sc;
+                reqs[k].virt = virts[k0 + k];
+                reqs[k].params = *params;
+                reqs[k].out = outs[k0 + k];
+            }
+            core.run(reqs.data(), m, s);
         }
-    }
-    return n;
+        return RVSB_OK;
+    });
 }
 
 const char* rvsb_stage_name(int stage) {

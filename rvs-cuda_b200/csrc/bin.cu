@@ -7,9 +7,13 @@
 namespace rvsb {
 namespace {
 
-__global__ void bin_count_kernel(const __grid_constant__ ViewTable tab, int* __restrict__ counts,
-                                 DevStatus* __restrict__ st) {
+// Grid (ceil(max_blocks / 256), max_views, slots): one thread per binning
+// block of view blockIdx.y of slot blockIdx.z.
+template <class Tabs>
+__global__ void bin_count_kernel(const __grid_constant__ Tabs tabs) {
+    const SlotTable& tab = tabs.at(blockIdx.z);
     const int v = blockIdx.y;
+    if (v >= tab.t.n_views) return;
     const DevView& V = tab.v[v];
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= V.nbx * V.nby) return;
@@ -17,16 +21,21 @@ __global__ void bin_count_kernel(const __grid_constant__ ViewTable tab, int* __r
     if (bb.x > bb.z || bb.y > bb.w) return;
     const int ntx = tab.t.ntx, n = tab.t.n_views;
     const int tx0 = bb.x / TILE, tx1 = bb.z / TILE, ty0 = bb.y / TILE, ty1 = bb.w / TILE;
+    int* counts = tab.b.counts;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) atomicAdd(&counts[(ty * ntx + tx) * n + v], 1);
-    atomicAdd(&st->bin_total, (tx1 - tx0 + 1) * (ty1 - ty0 + 1));
+    atomicAdd(&tab.b.status->bin_total, (tx1 - tx0 + 1) * (ty1 - ty0 + 1));
 }
 
-// Exclusive scan of the bin counts (one CTA of 1024 threads).
-__global__ void __launch_bounds__(1024) bin_scan_kernel(const int* __restrict__ counts, int* __restrict__ offsets,
-                                                        int* __restrict__ cursor, int n, int capacity,
-                                                        DevStatus* __restrict__ st) {
+// Exclusive scan of one slot's bin counts (one CTA of 1024 threads per slot).
+template <class Tabs>
+__global__ void __launch_bounds__(1024) bin_scan_kernel(const __grid_constant__ Tabs tabs) {
     __shared__ int warp_sums[32];
+    const SlotTable& tab = tabs.at(blockIdx.x);
+    const int* counts = tab.b.counts;
+    int* offsets = tab.b.offsets;
+    int* cursor = tab.b.cursor;
+    const int n = tab.t.ntx * tab.t.nty * tab.t.n_views;
     const int tid = threadIdx.x;
     const int per = (n + 1023) / 1024;
     const int beg = min(n, tid * per), end = min(n, beg + per);
@@ -57,13 +66,14 @@ __global__ void __launch_bounds__(1024) bin_scan_kernel(const int* __restrict__ 
         cursor[k] = run;
         run += counts[k];
     }
-    if (tid == 0 && st->bin_total > capacity) st->bin_overflow = 1;
+    if (tid == 0 && tab.b.status->bin_total > tab.b.capacity) tab.b.status->bin_overflow = 1;
 }
 
-__global__ void bin_fill_kernel(const __grid_constant__ ViewTable tab, int* __restrict__ cursor,
-                                int* __restrict__ list, const DevStatus* __restrict__ st) {
-    if (st->bin_overflow) return;
+template <class Tabs>
+__global__ void bin_fill_kernel(const __grid_constant__ Tabs tabs) {
+    const SlotTable& tab = tabs.at(blockIdx.z);
     const int v = blockIdx.y;
+    if (v >= tab.t.n_views || tab.b.status->bin_overflow) return;
     const DevView& V = tab.v[v];
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= V.nbx * V.nby) return;
@@ -71,6 +81,8 @@ __global__ void bin_fill_kernel(const __grid_constant__ ViewTable tab, int* __re
     if (bb.x > bb.z || bb.y > bb.w) return;
     const int ntx = tab.t.ntx, n = tab.t.n_views;
     const int tx0 = bb.x / TILE, tx1 = bb.z / TILE, ty0 = bb.y / TILE, ty1 = bb.w / TILE;
+    int* cursor = tab.b.cursor;
+    int* list = tab.b.list;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
             const int pos = atomicAdd(&cursor[(ty * ntx + tx) * n + v], 1);
@@ -80,13 +92,15 @@ __global__ void bin_fill_kernel(const __grid_constant__ ViewTable tab, int* __re
 
 }  // namespace
 
-void launch_bin(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, cudaStream_t s) {
-    const int ntiles = sh.ntx * sh.nty;
-    cudaMemsetAsync(b.counts, 0, sizeof(int) * (size_t)ntiles * sh.n_views, s);
-    dim3 grid((sh.max_blocks + 255) / 256, sh.n_views);
-    bin_count_kernel<<<grid, 256, 0, s>>>(tab, b.counts, b.status);
-    bin_scan_kernel<<<1, 1024, 0, s>>>(b.counts, b.offsets, b.cursor, ntiles * sh.n_views, b.capacity, b.status);
-    bin_fill_kernel<<<grid, 256, 0, s>>>(tab, b.cursor, b.list, b.status);
+template <class Tabs>
+void launch_bin(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
+    dim3 grid((sh.max_blocks + 255) / 256, sh.max_views, sh.slots);
+    bin_count_kernel<<<grid, 256, 0, s>>>(tabs);
+    bin_scan_kernel<<<sh.slots, 1024, 0, s>>>(tabs);
+    bin_fill_kernel<<<grid, 256, 0, s>>>(tabs);
 }
+
+template void launch_bin<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);
+template void launch_bin<TablePtr>(const TablePtr&, const BatchShape&, cudaStream_t);
 
 }  // namespace rvsb

@@ -57,23 +57,59 @@ struct DevTarget {
     int bin_capacity;
 };
 
-// Largest number of input views of one synthesis; the whole table travels
-// as a kernel parameter (constant bank), not through global memory.
+// Largest number of input views of one synthesis.
 constexpr int MAX_VIEWS = 16;
 
-struct ViewTable {
-    DevTarget t;
-    DevView v[MAX_VIEWS];
-};
-static_assert(sizeof(ViewTable) <= 4000, "kernel parameter space");
-
-// Status words written by the kernels (device memory, zeroed per call).
+// Status words written by the kernels (device memory, reset per call).
 struct DevStatus {
     int bin_total;      // number of (tile, view, block) entries
     int bin_overflow;   // 1 when bin_total exceeded the list capacity
     int hole_x0, hole_y0, hole_x1, hole_y1;   // bounding box of holes (x0 > x1: none)
     int n_holes;
     int pad;
+};
+
+// Optional intermediate outputs (device pointers, may be null).
+struct DebugPtrs {
+    float* warped_uvz = nullptr;
+    float* view_color = nullptr;
+    float* view_depth = nullptr;
+    float* view_validity = nullptr;
+    float* blend_color = nullptr;
+    float* blend_quality = nullptr;
+    int32_t* inpaint_source = nullptr;
+    bool any() const {
+        return warped_uvz || view_color || view_depth || view_validity || blend_color ||
+               blend_quality || inpaint_source;
+    }
+};
+
+// Device buffers of one slot's workspace.
+struct SlotBuffers {
+    DevStatus* status;   // 1 entry
+    int* counts;         // ntiles * n_views
+    int* offsets;        // ntiles * n_views
+    int* cursor;         // ntiles * n_views
+    int* list;           // bin list, `capacity` entries
+    int capacity;
+    int pad;
+    uint64_t* codes;     // Wo*Ho packed output codes + hole bit
+    uint8_t* holes;      // Wo*Ho hole mask (1 = no view covers the pixel)
+    uint64_t* scan[4];   // Wo*Ho inpainting scratch each
+};
+
+// Everything one synthesis (one virtual view) needs on the device.  A batch
+// keeps one table per slot in device memory; every kernel of the batch reads
+// the table of its slot (a grid dimension), so the launch sequence of a
+// batch is fixed and the per-call data travels in one copy of the tables.
+struct SlotTable {
+    DevTarget t;
+    SlotBuffers b;
+    uint16_t* out_y;
+    uint16_t* out_u;
+    uint16_t* out_v;
+    DebugPtrs dbg;
+    DevView v[MAX_VIEWS];
 };
 
 }  // namespace rvsb

@@ -1,0 +1,306 @@
+// Host engine: device memory, slot workspaces, slot tables and batch launches.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "camera.hpp"
+#include "frontend.hpp"
+
+namespace rvsb {
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void DevMem::alloc(rvsb_context* c, size_t n) {
+    release();
+    if (n == 0) n = 16;
+    {
+        std::lock_guard<std::mutex> lock(c->mem_mu);
+        if (c->in_use + n > c->budget)
+            throw BudgetError("request of " + std::to_string(n) + " bytes exceeds the HBM budget (" +
+                              std::to_string(c->in_use) + " of " + std::to_string(c->budget) + " in use)");
+        c->in_use += n;
+    }
+    const cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        std::lock_guard<std::mutex> lock(c->mem_mu);
+        c->in_use -= n;
+        check(e, "cudaMalloc");
+    }
+    ctx = c;
+    bytes = n;
+}
+
+void DevMem::release() {
+    if (ptr) {
+        cudaFree(ptr);
+        std::lock_guard<std::mutex> lock(ctx->mem_mu);
+        ctx->in_use -= bytes;
+    }
+    ptr = nullptr;
+    bytes = 0;
+}
+
+int nblocks_x(int w) { return (w - 1 + BLOCK_W - 1) / BLOCK_W; }
+int nblocks_y(int h) { return (h - 1 + BLOCK_H - 1) / BLOCK_H; }
+
+namespace {
+
+struct SlotNeeds {
+    size_t vert, bbox, out, bins, list;
+};
+
+SlotNeeds needs_of(const rvsb_scene* sc, int wo, int ho) {
+    SlotNeeds n{};
+    for (const auto& c : sc->cams) {
+        n.vert += (size_t)c.width * c.height;
+        n.bbox += (size_t)nblocks_x(c.width) * nblocks_y(c.height);
+    }
+    n.out = (size_t)wo * ho;
+    n.bins = (size_t)((wo + TILE - 1) / TILE) * ((ho + TILE - 1) / TILE) * sc->cams.size();
+    n.list = std::min<size_t>(INT32_MAX / 2, std::max<size_t>(1 << 16, n.bbox * 8 + n.bins));
+    return n;
+}
+
+}  // namespace
+
+size_t SlotWorkspace::bytes_for(const rvsb_scene* sc, int wo, int ho) {
+    const SlotNeeds n = needs_of(sc, wo, ho);
+    return sizeof(DevStatus) + n.vert * sizeof(float4) + n.bbox * sizeof(int4) + 3 * n.bins * sizeof(int) +
+           n.list * sizeof(int) + n.out * (sizeof(uint64_t) * 5 + 1);
+}
+
+void SlotWorkspace::ensure(rvsb_context* ctx, const rvsb_scene* sc, int wo, int ho) {
+    const SlotNeeds n = needs_of(sc, wo, ho);
+    if (!status.ptr) status.alloc(ctx, sizeof(DevStatus));
+    if (n.vert > cap_vert) {
+        vert.alloc(ctx, n.vert * sizeof(float4));
+        cap_vert = n.vert;
+    }
+    if (n.bbox > cap_bbox) {
+        bbox.alloc(ctx, n.bbox * sizeof(int4));
+        cap_bbox = n.bbox;
+    }
+    if (n.bins > cap_bins) {
+        counts.alloc(ctx, n.bins * sizeof(int));
+        offsets.alloc(ctx, n.bins * sizeof(int));
+        cursor.alloc(ctx, n.bins * sizeof(int));
+        cap_bins = n.bins;
+    }
+    if (n.list > cap_list) {
+        list.alloc(ctx, n.list * sizeof(int));
+        cap_list = n.list;
+    }
+    if (n.out > cap_out) {
+        codes.alloc(ctx, n.out * sizeof(uint64_t));
+        holes.alloc(ctx, n.out);
+        for (auto& s : scan) s.alloc(ctx, n.out * sizeof(uint64_t));
+        cap_out = n.out;
+    }
+}
+
+BatchCore::BatchCore(rvsb_context* ctx, int slots) : ctx_(ctx), slots_(slots) {
+    if (slots <= 0) throw ArgError("a batch needs at least one slot");
+    prepare_kernels();
+    for (int k = 0; k < slots; ++k) ws_.push_back(std::make_unique<SlotWorkspace>());
+    tables_.alloc(ctx, sizeof(SlotTable) * (size_t)slots);
+    for (int b = 0; b < 2; ++b) {
+        void* p = nullptr;
+        check(cudaHostAlloc(&p, sizeof(SlotTable) * (size_t)slots, cudaHostAllocDefault), "cudaHostAlloc");
+        staging_[b] = static_cast<SlotTable*>(p);
+        check(cudaEventCreateWithFlags(&copied_[b], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    check(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+BatchCore::~BatchCore() {
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.second.exec);
+    for (int b = 0; b < 2; ++b) {
+        if (copied_[b]) {
+            cudaEventSynchronize(copied_[b]);
+            cudaEventDestroy(copied_[b]);
+        }
+        if (staging_[b]) cudaFreeHost(staging_[b]);
+    }
+    for (auto& e : events_)
+        if (e) cudaEventDestroy(e);
+    if (capture_) cudaStreamDestroy(capture_);
+}
+
+void BatchCore::set_profiling(bool on) {
+    if (on && !events_[0])
+        for (auto& e : events_) check(cudaEventCreate(&e), "cudaEventCreate");
+    profiling_ = on;
+}
+
+int BatchCore::stage_times(float* ms, int max_stages) const {
+    if (!profiled_ || !ms) return -1;
+    const int n = std::min(max_stages, (int)NUM_STAGES);
+    for (int k = 0; k < n; ++k) {
+        if (cudaEventElapsedTime(&ms[k], events_[2 * k], events_[2 * k + 1]) != cudaSuccess) {
+            cudaGetLastError();
+            return -1;
+        }
+    }
+    return n;
+}
+
+void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r) {
+    std::memset(&T, 0, sizeof(T));
+    const rvsb_scene* sc = r.scene;
+    SlotWorkspace& ws = *ws_[k];
+    const rvsb_camera& virt = r.virt;
+    const rvsb_synth_params& p = r.params;
+    const int n = (int)sc->cams.size();
+    size_t voff = 0, boff = 0;
+    for (int v = 0; v < n; ++v) {
+        const rvsb_camera& c = sc->cams[v];
+        DevView& V = T.v[v];
+        V.w = c.width;
+        V.h = c.height;
+        V.proj = c.projection;
+        V.bits_color = c.bit_depth_color;
+        V.f0 = c.focal[0];
+        V.f1 = c.focal[1];
+        V.p0 = c.principle_point[0];
+        V.p1 = c.principle_point[1];
+        V.near_ = c.depth_range[0];
+        V.far_ = c.depth_range[1];
+        V.depth_scale = 1.0f / (float)((1u << c.bit_depth_depth) - 1u);
+        V.has_invalid = c.has_invalid_depth;
+        V.color_scale = 1.0f / (float)((1u << c.bit_depth_color) - 1u);
+        V.cw = c.width / 2;
+        V.ch = c.height / 2;
+        V.chroma_sx = (float)V.cw / c.width;
+        V.chroma_sy = (float)V.ch / c.height;
+        relative_pose(c, virt, V.R, V.t);
+        V.py = sc->planes[v * 4 + 0]->as<uint16_t>();
+        V.pu = sc->planes[v * 4 + 1]->as<uint16_t>();
+        V.pv = sc->planes[v * 4 + 2]->as<uint16_t>();
+        V.pd = r.frame ? r.frame[v].depth : sc->planes[v * 4 + 3]->as<uint16_t>();
+        if (c.projection == RVSB_PROJ_EQUIRECTANGULAR) {
+            V.erp_row = sc->erp[v * 2 + 0]->as<float>();
+            V.erp_col = sc->erp[v * 2 + 1]->as<float>();
+        }
+        V.color = sc->color[v]->as<uint64_t>();
+        V.vert = ws.vert.as<float4>() + voff;
+        V.bbox = ws.bbox.as<int4>() + boff;
+        V.tri_shift = 2;
+        while ((1 << (V.tri_shift - 2)) < c.width - 1) ++V.tri_shift;
+        V.nbx = nblocks_x(c.width);
+        V.nby = nblocks_y(c.height);
+        voff += (size_t)c.width * c.height;
+        boff += (size_t)V.nbx * V.nby;
+    }
+    DevTarget& D = T.t;
+    D.wo = virt.width;
+    D.ho = virt.height;
+    D.proj = virt.projection;
+    D.wrap = (virt.projection == RVSB_PROJ_EQUIRECTANGULAR && virt.full_hor_range) ? 1 : 0;
+    D.f0 = virt.focal[0];
+    D.f1 = virt.focal[1];
+    D.p0 = virt.principle_point[0];
+    D.p1 = virt.principle_point[1];
+    if (virt.projection == RVSB_PROJ_EQUIRECTANGULAR) erp_projector_constants(virt, D.u0, D.v0, D.du_dphi, D.dv_dtheta);
+    D.bits = virt.bit_depth_color;
+    D.max_val = (1u << virt.bit_depth_color) - 1u;
+    D.blend_exp = p.blending_factor;
+    D.inv_blend_exp = 1.0f / p.blending_factor;
+    D.blend_exp_int = 0;
+    if (p.blending_factor == std::floor(p.blending_factor) && p.blending_factor >= 2.f && p.blending_factor <= 16.f)
+        D.blend_exp_int = (int)p.blending_factor;
+    D.chroma_ties_up = p.chroma_rounding == RVSB_CHROMA_TIES_UP;
+    D.ntx = (virt.width + TILE - 1) / TILE;
+    D.nty = (virt.height + TILE - 1) / TILE;
+    D.n_views = n;
+    D.bin_capacity = (int)ws.cap_list;
+    SlotBuffers& B = T.b;
+    B.status = ws.status.as<DevStatus>();
+    B.counts = ws.counts.as<int>();
+    B.offsets = ws.offsets.as<int>();
+    B.cursor = ws.cursor.as<int>();
+    B.list = ws.list.as<int>();
+    B.capacity = (int)ws.cap_list;
+    B.codes = ws.codes.as<uint64_t>();
+    B.holes = ws.holes.as<uint8_t>();
+    for (int s = 0; s < 4; ++s) B.scan[s] = ws.scan[s].as<uint64_t>();
+    T.out_y = r.out.y;
+    T.out_u = r.out.u;
+    T.out_v = r.out.v;
+    T.dbg = r.dbg;
+}
+
+int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
+    if (n <= 0 || n > slots_) throw ArgError("batch of " + std::to_string(n) + " requests for " +
+                                             std::to_string(slots_) + " slots");
+    BatchShape sh;
+    sh.slots = n;
+    for (int k = 0; k < n; ++k) {
+        const SlotRequest& r = reqs[k];
+        ws_[k]->ensure(ctx_, r.scene, r.virt.width, r.virt.height);
+        const int nv = (int)r.scene->cams.size();
+        sh.max_views = std::max(sh.max_views, nv);
+        for (const auto& c : r.scene->cams) {
+            sh.max_w = std::max(sh.max_w, c.width);
+            sh.max_h = std::max(sh.max_h, c.height);
+            sh.max_blocks = std::max(sh.max_blocks, nblocks_x(c.width) * nblocks_y(c.height));
+        }
+        const int ntiles = ((r.virt.width + TILE - 1) / TILE) * ((r.virt.height + TILE - 1) / TILE);
+        sh.max_wo = std::max(sh.max_wo, r.virt.width);
+        sh.max_ho = std::max(sh.max_ho, r.virt.height);
+        sh.max_tiles = std::max(sh.max_tiles, ntiles);
+        sh.max_bins = std::max(sh.max_bins, ntiles * nv);
+    }
+    if (n == 1 && !use_graphs_) {
+        // A single synthesis: the table travels as a kernel parameter.
+        TableParam tp;
+        fill(tp.t, 0, reqs[0]);
+        const int launches = launch_batch(tp, sh, s, profiling_ ? events_ : nullptr);
+        if (launches < 0) check(cudaGetLastError(), "kernel launch");
+        profiled_ = profiling_;
+        last_launches_ = launches;
+        return launches;
+    }
+    // The staging buffer is reused every other call: its previous copy must
+    // have been consumed.
+    check(cudaEventSynchronize(copied_[cur_]), "wait for table staging");
+    for (int k = 0; k < n; ++k) fill(staging_[cur_][k], k, reqs[k]);
+    check(cudaMemcpyAsync(tables_.ptr, staging_[cur_], sizeof(SlotTable) * (size_t)n, cudaMemcpyHostToDevice, s),
+          "upload slot tables");
+    check(cudaEventRecord(copied_[cur_], s), "record table upload");
+    cur_ ^= 1;
+    const TablePtr tabs{tables_.as<SlotTable>()};
+    int launches;
+    if (use_graphs_ && !profiling_) {
+        const std::vector<int> key = {sh.slots, sh.max_views, sh.max_w, sh.max_h, sh.max_blocks,
+                                      sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins};
+        auto it = graphs_.find(key);
+        if (it == graphs_.end()) {
+            cudaGraph_t g = nullptr;
+            check(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal), "begin capture");
+            const int nl = launch_batch(tabs, sh, capture_, nullptr);
+            const cudaError_t ec = cudaStreamEndCapture(capture_, &g);
+            if (nl < 0) check(cudaGetLastError(), "kernel launch (capture)");
+            check(ec, "end capture");
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            check(ei, "graph instantiate");
+            it = graphs_.emplace(key, Graph{exec, nl}).first;
+        }
+        check(cudaGraphLaunch(it->second.exec, s), "graph launch");
+        launches = it->second.launches;
+    } else {
+        launches = launch_batch(tabs, sh, s, profiling_ ? events_ : nullptr);
+        if (launches < 0) check(cudaGetLastError(), "kernel launch");
+    }
+    profiled_ = profiling_;
+    last_launches_ = launches;
+    return launches;
+}
+
+}  // namespace rvsb

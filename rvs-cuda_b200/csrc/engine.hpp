@@ -1,0 +1,149 @@
+// Host engine under the C ABI: device memory accounting, input scenes,
+// slot workspaces and batch launches (slot tables, CUDA graphs).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.hpp"
+#include "rvsb.h"
+
+namespace rvsb {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct BudgetError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ArgError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t e, const char* what);
+
+}  // namespace rvsb
+
+struct rvsb_context {
+    int device = 0;
+    size_t budget = 0;
+    size_t in_use = 0;
+    std::string last_error;
+    std::mutex mu;                     // serialises rvsb_synthesize_host
+    std::mutex mem_mu;                 // guards in_use
+    rvsb_scene* host_scene = nullptr;  // scene reused by rvsb_synthesize_host
+    void* host_out = nullptr;          // device output staging of rvsb_synthesize_host
+    size_t host_out_bytes = 0;
+};
+
+namespace rvsb {
+
+// Device allocation counted against the context's HBM budget.
+struct DevMem {
+    rvsb_context* ctx = nullptr;
+    void* ptr = nullptr;
+    size_t bytes = 0;
+
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    ~DevMem() { release(); }
+
+    void alloc(rvsb_context* c, size_t n);
+    void release();
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+// Buffers of one synthesis slot, grown on demand to the largest request
+// seen: the warped vertices and block boxes of every input view, the bins,
+// and the output-sized codes, hole mask and inpainting scratch.
+struct SlotWorkspace {
+    DevMem status, counts, offsets, cursor, list, codes, holes, scan[4], vert, bbox;
+    size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0;
+
+    // Bytes a slot needs for `scene` at output size wo x ho.
+    static size_t bytes_for(const rvsb_scene* scene, int wo, int ho);
+    void ensure(rvsb_context* ctx, const rvsb_scene* scene, int wo, int ho);
+};
+
+// Number of binning blocks of a view (BLOCK_W x BLOCK_H quads).
+int nblocks_x(int w);
+int nblocks_y(int h);
+
+// One synthesis request of a batch.
+struct SlotRequest {
+    const rvsb_scene* scene = nullptr;
+    rvsb_camera virt{};
+    rvsb_synth_params params{};
+    rvsb_yuv420 out{};
+    DebugPtrs dbg{};
+    const rvsb_view_planes* frame = nullptr;  // optional raw device planes (depth read in place)
+};
+
+// Slot tables in device memory, their pinned host staging, and the launch
+// of a batch of up to `slots` requests.  Calls on one core must be ordered
+// (one stream, or the caller waits): the device tables are reused.
+class BatchCore {
+public:
+    BatchCore(rvsb_context* ctx, int slots);
+    ~BatchCore();
+    BatchCore(const BatchCore&) = delete;
+    BatchCore& operator=(const BatchCore&) = delete;
+
+    int slots() const { return slots_; }
+    SlotWorkspace& workspace(int k) { return *ws_[k]; }
+
+    // Sizes the slot workspaces for the requests, fills and uploads their
+    // tables and issues the batch on `stream`.  Returns the kernel launches.
+    int run(const SlotRequest* reqs, int n, cudaStream_t stream);
+
+    void set_graphs(bool on) { use_graphs_ = on; }
+    void set_profiling(bool on);
+    // Milliseconds per stage of the last profiled run (stream complete).
+    int stage_times(float* ms, int max_stages) const;
+    int last_launches() const { return last_launches_; }
+
+private:
+    void fill(SlotTable& t, int k, const SlotRequest& r);
+
+    rvsb_context* ctx_;
+    int slots_;
+    std::vector<std::unique_ptr<SlotWorkspace>> ws_;
+    DevMem tables_;
+    SlotTable* staging_[2] = {nullptr, nullptr};
+    cudaEvent_t copied_[2] = {nullptr, nullptr};
+    int cur_ = 0;
+    bool use_graphs_ = false;
+    cudaStream_t capture_ = nullptr;  // private stream the graphs are captured on
+    struct Graph {
+        cudaGraphExec_t exec;
+        int launches;
+    };
+    std::map<std::vector<int>, Graph> graphs_;
+    bool profiling_ = false;
+    bool profiled_ = false;
+    cudaEvent_t events_[2 * NUM_STAGES] = {};
+    int last_launches_ = 0;
+};
+
+}  // namespace rvsb
+
+struct rvsb_scene {
+    rvsb_context* ctx = nullptr;
+    std::vector<rvsb_camera> cams;
+    std::vector<std::unique_ptr<rvsb::DevMem>> planes;  // 4 per view: y, u, v, depth
+    std::vector<std::unique_ptr<rvsb::DevMem>> erp;     // 2 per view: rows, cols (ERP inputs)
+    std::vector<std::unique_ptr<rvsb::DevMem>> color;   // 1 per view: decoded colour words
+    std::vector<bool> uploaded;
+    std::unique_ptr<rvsb::BatchCore> single;            // the per-view calls: a batch of one
+    int last_launches = 0;
+};

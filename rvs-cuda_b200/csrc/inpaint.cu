@@ -41,6 +41,49 @@ struct Region {
     bool empty;
 };
 
+// The buffers of one image the passes work on.
+struct InpaintImage {
+    int wo, ho;
+    const DevStatus* st;       // hole count and bounding box
+    const uint8_t* holes;      // wo*ho, nonzero = hole
+    uint64_t* codes;           // wo*ho packed codes (the fill copies them)
+    uint64_t* scan[4];         // wo*ho words each
+    int32_t* sources;          // optional: (x, y) source of every hole
+    uint16_t* out_y;
+    uint16_t* out_u;
+    uint16_t* out_v;
+    int ties_up;               // output chroma rounding
+};
+
+// Image of slot blockIdx.z of a batch.
+template <class Tabs>
+struct FromTables {
+    Tabs tabs;
+    __device__ InpaintImage operator()() const {
+        const SlotTable& t = tabs.at(blockIdx.z);
+        InpaintImage im;
+        im.wo = t.t.wo;
+        im.ho = t.t.ho;
+        im.st = t.b.status;
+        im.holes = t.b.holes;
+        im.codes = t.b.codes;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) im.scan[k] = t.b.scan[k];
+        im.sources = t.dbg.inpaint_source;
+        im.out_y = t.out_y;
+        im.out_u = t.out_u;
+        im.out_v = t.out_v;
+        im.ties_up = t.t.chroma_ties_up;
+        return im;
+    }
+};
+
+// One image given directly (kernel parameter).
+struct Direct {
+    InpaintImage im;
+    __device__ InpaintImage operator()() const { return im; }
+};
+
 __device__ __forceinline__ Region hole_region(const DevStatus* st, int wo, int ho) {
     Region r;
     r.empty = st->n_holes == 0;
@@ -79,8 +122,13 @@ __device__ __forceinline__ unsigned long long warp_incl_min_rev(unsigned long lo
 
 // Sweep 0, rows (forward): R(p) = lexmin over q.x <= p.x of
 // (C(q).d + p.x - q.x, C(q).src).  One warp per row of the region.
-__global__ void inpaint_row0_kernel(int wo, int ho, const DevStatus* __restrict__ st,
-                                    const uint8_t* __restrict__ holes, uint64_t* __restrict__ R) {
+template <class Src>
+__global__ void inpaint_row0_kernel(const __grid_constant__ Src src) {
+    const InpaintImage im = src();
+    const int wo = im.wo, ho = im.ho;
+    const DevStatus* __restrict__ st = im.st;
+    const uint8_t* __restrict__ holes = im.holes;
+    uint64_t* __restrict__ R = im.scan[0];
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
     const int lane = threadIdx.x & 31;
@@ -136,10 +184,14 @@ __device__ __forceinline__ unsigned long long col0_key(uint64_t r, int y) {
 
 // Sweep 0, columns (forward): D0, S0 (p) = lexmin over q.y <= p.y of
 // (R(q).d + p.y - q.y, src).  Output packed (D0, S0) per pixel.
-__global__ void __launch_bounds__(1024) inpaint_col0_kernel(int wo, int ho, const DevStatus* __restrict__ st,
-                                                            const uint8_t* __restrict__ holes,
-                                                            const uint64_t* __restrict__ R,
-                                                            uint64_t* __restrict__ DS) {
+template <class Src>
+__global__ void __launch_bounds__(1024) inpaint_col0_kernel(const __grid_constant__ Src src) {
+    const InpaintImage im = src();
+    const int wo = im.wo, ho = im.ho;
+    const DevStatus* __restrict__ st = im.st;
+    const uint8_t* __restrict__ holes = im.holes;
+    const uint64_t* __restrict__ R = im.scan[0];
+    uint64_t* __restrict__ DS = im.scan[1];
     __shared__ unsigned long long seg[32][33];
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
@@ -202,9 +254,15 @@ __device__ __forceinline__ uint64_t ds_at(const uint64_t* DS, const Region& rg, 
 // Sweep 1 seeds: T(q) = best of stay (D0(q), S0(q)), left (D0+1, S0 of left),
 // up (D0+1, S0 of up) with priority stay > left > up; T'(q) the same without
 // stay.  Non-holes: (0, q).
-__global__ void inpaint_seed1_kernel(int wo, int ho, const DevStatus* __restrict__ st,
-                                     const uint8_t* __restrict__ holes, const uint64_t* __restrict__ DS,
-                                     uint64_t* __restrict__ Tq, uint64_t* __restrict__ Tp) {
+template <class Src>
+__global__ void inpaint_seed1_kernel(const __grid_constant__ Src src) {
+    const InpaintImage im = src();
+    const int wo = im.wo, ho = im.ho;
+    const DevStatus* __restrict__ st = im.st;
+    const uint8_t* __restrict__ holes = im.holes;
+    const uint64_t* __restrict__ DS = im.scan[1];
+    uint64_t* __restrict__ Tq = im.scan[2];
+    uint64_t* __restrict__ Tp = im.scan[3];
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
     const int x = rg.x0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -235,8 +293,13 @@ __global__ void inpaint_seed1_kernel(int wo, int ho, const DevStatus* __restrict
 
 // Sweep 1, rows (backward, exclusive): RR(x, y) = min over q.x > x of
 // (T(q).d + q.x, q.x).  One warp per row.
-__global__ void inpaint_row1_kernel(int wo, int ho, const DevStatus* __restrict__ st,
-                                    const uint64_t* __restrict__ Tq, uint64_t* __restrict__ RR) {
+template <class Src>
+__global__ void inpaint_row1_kernel(const __grid_constant__ Src src) {
+    const InpaintImage im = src();
+    const int wo = im.wo, ho = im.ho;
+    const DevStatus* __restrict__ st = im.st;
+    const uint64_t* __restrict__ Tq = im.scan[2];
+    uint64_t* __restrict__ RR = im.scan[0];
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
     const int lane = threadIdx.x & 31;
@@ -271,10 +334,18 @@ __global__ void inpaint_row1_kernel(int wo, int ho, const DevStatus* __restrict_
 // Sweep 1, columns (backward): for each hole p choose its sweep-1 source
 // and copy that pixel's codes (the fill of inpaint_color,
 // inpainting.cpp:191-198).
-__global__ void __launch_bounds__(1024) inpaint_col1_kernel(
-    int wo, int ho, const DevStatus* __restrict__ st, uint64_t* __restrict__ codes, const uint8_t* __restrict__ holes,
-    const uint64_t* __restrict__ DS, const uint64_t* __restrict__ Tq, const uint64_t* __restrict__ Tp,
-    const uint64_t* __restrict__ RR, int32_t* __restrict__ dbg_source) {
+template <class Src>
+__global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constant__ Src src) {
+    const InpaintImage im = src();
+    const int wo = im.wo, ho = im.ho;
+    const DevStatus* __restrict__ st = im.st;
+    uint64_t* __restrict__ codes = im.codes;
+    const uint8_t* __restrict__ holes = im.holes;
+    const uint64_t* __restrict__ DS = im.scan[1];
+    const uint64_t* __restrict__ Tq = im.scan[2];
+    const uint64_t* __restrict__ Tp = im.scan[3];
+    const uint64_t* __restrict__ RR = im.scan[0];
+    int32_t* __restrict__ dbg_source = im.sources;
     __shared__ unsigned long long seg_col[32][33];
     __shared__ unsigned long long seg_off[32][33];
     const Region rg = hole_region(st, wo, ho);
@@ -381,9 +452,16 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(
 }
 
 // Writes the 2x2 output blocks of the region that hold at least one hole.
-__global__ void inpaint_write_kernel(int wo, int ho, const DevStatus* __restrict__ st,
-                                     const uint64_t* __restrict__ codes, uint16_t* __restrict__ out_y,
-                                     uint16_t* __restrict__ out_u, uint16_t* __restrict__ out_v, int ties_up) {
+template <class Src>
+__global__ void inpaint_write_kernel(const __grid_constant__ Src src) {
+    const InpaintImage im = src();
+    const int wo = im.wo, ho = im.ho;
+    const DevStatus* __restrict__ st = im.st;
+    const uint64_t* __restrict__ codes = im.codes;
+    uint16_t* __restrict__ out_y = im.out_y;
+    uint16_t* __restrict__ out_u = im.out_u;
+    uint16_t* __restrict__ out_v = im.out_v;
+    const int ties_up = im.ties_up;
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
     const int bx0 = rg.x0 / 2, by0 = rg.y0 / 2;
@@ -406,35 +484,42 @@ __global__ void inpaint_write_kernel(int wo, int ho, const DevStatus* __restrict
     out_v[co] = quarter_round(sv, ties_up);
 }
 
-}  // namespace
-
-void launch_inpaint(const SynthBuffers& b, const LaunchShape& sh, const DebugPtrs& dbg, uint16_t* out_y,
-                    uint16_t* out_u, uint16_t* out_v, cudaStream_t s) {
+// The five scan passes of `src` (grid z = images), sized for max_w x max_h.
+template <class Src>
+void launch_scans(const Src& src, int max_w, int max_h, int images, cudaStream_t s) {
     const int rows_per_cta = 8;  // 8 warps of 32
-    const int wo = sh.wo, ho = sh.ho;
-    inpaint_row0_kernel<<<(ho + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(wo, ho, b.status, b.holes, b.scan_a);
-    inpaint_col0_kernel<<<(wo + 31) / 32, 1024, 0, s>>>(wo, ho, b.status, b.holes, b.scan_a, b.scan_b);
-    inpaint_seed1_kernel<<<dim3((wo + 255) / 256, ho), 256, 0, s>>>(wo, ho, b.status, b.holes, b.scan_b, b.scan_c,
-                                                                  b.scan_d);
-    inpaint_row1_kernel<<<(ho + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(wo, ho, b.status, b.scan_c, b.scan_a);
-    inpaint_col1_kernel<<<(wo + 31) / 32, 1024, 0, s>>>(wo, ho, b.status, b.codes, b.holes, b.scan_b, b.scan_c,
-                                                       b.scan_d, b.scan_a, dbg.inpaint_source);
-    inpaint_write_kernel<<<dim3((wo / 2 + 127) / 128, (ho + 1) / 2), 128, 0, s>>>(wo, ho, b.status, b.codes, out_y,
-                                                                               out_u, out_v, sh.chroma_ties_up);
+    inpaint_row0_kernel<<<dim3((max_h + rows_per_cta - 1) / rows_per_cta, 1, images), 256, 0, s>>>(src);
+    inpaint_col0_kernel<<<dim3((max_w + 31) / 32, 1, images), 1024, 0, s>>>(src);
+    inpaint_seed1_kernel<<<dim3((max_w + 255) / 256, max_h, images), 256, 0, s>>>(src);
+    inpaint_row1_kernel<<<dim3((max_h + rows_per_cta - 1) / rows_per_cta, 1, images), 256, 0, s>>>(src);
+    inpaint_col1_kernel<<<dim3((max_w + 31) / 32, 1, images), 1024, 0, s>>>(src);
 }
 
-// The scans alone (no output write) over `holes` with caller-provided
-// scratch: status, codes and four scan buffers of w*h words each; the
-// chosen source of every hole goes to `sources`.
-void launch_inpaint_scans(const DevStatus* st, const uint8_t* holes, uint64_t* codes, uint64_t* const scan[4], int w,
+}  // namespace
+
+template <class Tabs>
+void launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
+    const FromTables<Tabs> src{tabs};
+    launch_scans(src, sh.max_wo, sh.max_ho, sh.slots, s);
+    inpaint_write_kernel<<<dim3((sh.max_wo / 2 + 127) / 128, (sh.max_ho + 1) / 2, sh.slots), 128, 0, s>>>(src);
+}
+
+template void launch_inpaint<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);
+template void launch_inpaint<TablePtr>(const TablePtr&, const BatchShape&, cudaStream_t);
+
+void launch_inpaint_scans(DevStatus* st, const uint8_t* holes, uint64_t* codes, uint64_t* const scan[4], int w,
                           int h, int32_t* sources, cudaStream_t s) {
-    const int rows_per_cta = 8;  // 8 warps of 32
-    inpaint_row0_kernel<<<(h + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(w, h, st, holes, scan[0]);
-    inpaint_col0_kernel<<<(w + 31) / 32, 1024, 0, s>>>(w, h, st, holes, scan[0], scan[1]);
-    inpaint_seed1_kernel<<<dim3((w + 255) / 256, h), 256, 0, s>>>(w, h, st, holes, scan[1], scan[2], scan[3]);
-    inpaint_row1_kernel<<<(h + rows_per_cta - 1) / rows_per_cta, 256, 0, s>>>(w, h, st, scan[2], scan[0]);
-    inpaint_col1_kernel<<<(w + 31) / 32, 1024, 0, s>>>(w, h, st, codes, holes, scan[1], scan[2], scan[3], scan[0],
-                                                       sources);
+    Direct src;
+    src.im.wo = w;
+    src.im.ho = h;
+    src.im.st = st;
+    src.im.holes = holes;
+    src.im.codes = codes;
+    for (int k = 0; k < 4; ++k) src.im.scan[k] = scan[k];
+    src.im.sources = sources;
+    src.im.out_y = src.im.out_u = src.im.out_v = nullptr;
+    src.im.ties_up = 0;
+    launch_scans(src, w, h, 1, s);
 }
 
 }  // namespace rvsb

@@ -1,53 +1,71 @@
-// Orchestration of one synthesis on a stream.
+// Orchestration of one batch of syntheses on a stream.  Every kernel covers
+// all slots of the batch in one launch (the slot is a grid dimension), so a
+// batch costs the same 12 launches as a single view and the sequence can be
+// captured in a CUDA graph.
 #include "device_common.cuh"
 #include "kernels.hpp"
 
 namespace rvsb {
 
-void launch_warp(const ViewTable& tab, const LaunchShape& sh, cudaStream_t s);
-void launch_bin(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, cudaStream_t s);
-void launch_raster(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, const DebugPtrs& dbg,
-                   uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t s);
-void launch_inpaint(const SynthBuffers& b, const LaunchShape& sh, const DebugPtrs& dbg, uint16_t* out_y,
-                    uint16_t* out_u, uint16_t* out_v, cudaStream_t s);
+template <class Tabs>
+void launch_warp(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
+template <class Tabs>
+void launch_bin(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
+template <class Tabs>
+void launch_raster(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
+template <class Tabs>
+void launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 
 namespace {
 
-__global__ void status_init_kernel(DevStatus* st) {
-    st->bin_total = 0;
-    st->bin_overflow = 0;
-    st->hole_x0 = INT_MAX;
-    st->hole_y0 = INT_MAX;
-    st->hole_x1 = INT_MIN;
-    st->hole_y1 = INT_MIN;
-    st->n_holes = 0;
+// Per slot: the empty status and zero bin counts.  Grid (ceil(max_bins /
+// 256), slots).
+template <class Tabs>
+__global__ void slot_init_kernel(const __grid_constant__ Tabs tabs) {
+    const SlotTable& tab = tabs.at(blockIdx.y);
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nbins = tab.t.ntx * tab.t.nty * tab.t.n_views;
+    if (k < nbins) tab.b.counts[k] = 0;
+    if (k == 0) {
+        DevStatus* st = tab.b.status;
+        st->bin_total = 0;
+        st->bin_overflow = 0;
+        st->hole_x0 = INT_MAX;
+        st->hole_y0 = INT_MAX;
+        st->hole_x1 = INT_MIN;
+        st->hole_y1 = INT_MIN;
+        st->n_holes = 0;
+        st->pad = 0;
+    }
 }
 
 }  // namespace
 
-int launch_synthesis(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, const DebugPtrs& dbg,
-                     uint16_t* out_y,
-                     uint16_t* out_u, uint16_t* out_v, cudaStream_t s, cudaEvent_t* ev) {
+template <class Tabs>
+int launch_batch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s, cudaEvent_t* ev) {
     auto mark = [&](int k) {
         if (ev) cudaEventRecord(ev[k], s);
     };
     mark(8);
-    status_init_kernel<<<1, 1, 0, s>>>(b.status);
+    slot_init_kernel<<<dim3((sh.max_bins + 255) / 256, sh.slots), 256, 0, s>>>(tabs);
     mark(0);
-    launch_warp(tab, sh, s);
+    launch_warp(tabs, sh, s);
     mark(1);
     mark(2);
-    launch_bin(b, tab, sh, s);
+    launch_bin(tabs, sh, s);
     mark(3);
     mark(4);
-    launch_raster(b, tab, sh, dbg, out_y, out_u, out_v, s);
+    launch_raster(tabs, sh, s);
     mark(5);
     mark(6);
-    launch_inpaint(b, sh, dbg, out_y, out_u, out_v, s);
+    launch_inpaint(tabs, sh, s);
     mark(7);
     mark(9);
     if (cudaPeekAtLastError() != cudaSuccess) return -1;
     return 1 + 1 + 3 + 1 + 6;
 }
+
+template int launch_batch<TableParam>(const TableParam&, const BatchShape&, cudaStream_t, cudaEvent_t*);
+template int launch_batch<TablePtr>(const TablePtr&, const BatchShape&, cudaStream_t, cudaEvent_t*);
 
 }  // namespace rvsb

@@ -183,7 +183,7 @@ constexpr size_t kSmemBytes = kZbBytes + kEntBytes + kAccBytes;
 
 // Resolves and blends the views g0 .. g0 + gn - 1 of the tile, one pixel per
 // thread and step, into the accumulators (c0, c1, c2, q per pixel).
-__device__ __forceinline__ void resolve_group(const ViewTable& tab, int g0, int gn, int tx0, int ty0,
+__device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int gn, int tx0, int ty0,
                                               const unsigned long long (*zb)[TILE * TILE], float (*acc)[TILE * TILE],
                                               const DebugPtrs& dbg) {
     const DevTarget& T = tab.t;
@@ -300,21 +300,14 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
     }
 }
 
-// Grid: one CTA per TILE x TILE output tile.  Views are processed in groups
+// Grid (max tiles, slots): one CTA per TILE x TILE output tile of a slot.
+// Views are processed in groups
 // of VG: clear the group's shared z-buffers, stage the group's bin entries
 // (view, block) in shared memory, rasterise them (one warp per block), then
 // resolve and blend the group's views into the tile's accumulators.  After
 // the last group the tile is quantised and written.
-__global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_constant__ ViewTable tab,
-                                                                  const int* __restrict__ counts,
-                                                                  const int* __restrict__ offsets,
-                                                                  const int* __restrict__ list,
-                                                                  DevStatus* __restrict__ st,
-                                                                  uint64_t* __restrict__ codes,
-                                                                  uint8_t* __restrict__ holes,
-                                                                  uint16_t* __restrict__ out_y,
-                                                                  uint16_t* __restrict__ out_u,
-                                                                  uint16_t* __restrict__ out_v, DebugPtrs dbg) {
+template <class Tabs>
+__global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_constant__ Tabs tabs) {
     // Dynamic shared memory: the group's z-buffers, the staged bin entries
     // and the tile's blend accumulators.
     extern __shared__ __align__(16) unsigned char s_raw[];
@@ -323,11 +316,16 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_co
     auto acc = reinterpret_cast<float(*)[TILE * TILE]>(s_raw + kZbBytes + kEntBytes);
     __shared__ int s_pref[VG + 1];
     __shared__ int s_off[VG];
+    const SlotTable& tab = tabs.at(blockIdx.y);
     const DevTarget& T = tab.t;
     const int tile = blockIdx.x;
+    if (tile >= T.ntx * T.nty) return;
+    const int* __restrict__ counts = tab.b.counts;
+    const int* __restrict__ offsets = tab.b.offsets;
+    const int* __restrict__ list = tab.b.list;
     const int tx0 = (tile % T.ntx) * TILE, ty0 = (tile / T.ntx) * TILE;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool overflow = st->bin_overflow != 0;
+    const bool overflow = tab.b.status->bin_overflow != 0;
     const bool wrap = T.wrap != 0;
 
     for (int g0 = 0; g0 < T.n_views; g0 += VG) {
@@ -375,22 +373,26 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_co
             }
             __syncthreads();
         }
-        resolve_group(tab, g0, gn, tx0, ty0, zb, acc, dbg);
+        resolve_group(tab, g0, gn, tx0, ty0, zb, acc, tab.dbg);
         __syncthreads();
     }
-    write_tile(T, tx0, ty0, acc, st, codes, holes, out_y, out_u, out_v, dbg);
+    write_tile(T, tx0, ty0, acc, tab.b.status, tab.b.codes, tab.b.holes, tab.out_y, tab.out_u, tab.out_v, tab.dbg);
 }
 
 }  // namespace
 
-void launch_raster(const SynthBuffers& b, const ViewTable& tab, const LaunchShape& sh, const DebugPtrs& dbg,
-                   uint16_t* out_y, uint16_t* out_u, uint16_t* out_v, cudaStream_t s) {
+void prepare_kernels() {
     static_assert(kZbBytes % 16 == 0 && kEntBytes % 16 == 0, "shared-memory carve alignment");
-    // The attribute is per function and device; setting it before each
-    // launch is a cheap host call and keeps multi-device use correct.
-    cudaFuncSetAttribute(raster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
-    raster_kernel<<<sh.ntx * sh.nty, TILE_THREADS, kSmemBytes, s>>>(tab, b.counts, b.offsets, b.list, b.status,
-                                                                     b.codes, b.holes, out_y, out_u, out_v, dbg);
+    cudaFuncSetAttribute(raster_kernel<TableParam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    cudaFuncSetAttribute(raster_kernel<TablePtr>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
 }
+
+template <class Tabs>
+void launch_raster(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
+    raster_kernel<<<dim3(sh.max_tiles, sh.slots), TILE_THREADS, kSmemBytes, s>>>(tabs);
+}
+
+template void launch_raster<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);
+template void launch_raster<TablePtr>(const TablePtr&, const BatchShape&, cudaStream_t);
 
 }  // namespace rvsb

@@ -64,7 +64,7 @@ struct Box {
     }
 };
 
-// Grid (ceil(W/32), ceil(H/32), n_views), 256 threads.  Thread (lane, warp)
+// Grid (ceil(W/32), ceil(H/32), slots * max_views), 256 threads.  Thread (lane, warp)
 // warps the vertices of column j0 + lane, rows i0 + 4*warp .. +3, writes
 // them and keeps the bounding box of its column.  The row below the tile,
 // the column right of it and, for a horizontal wrap, column W-1 are warped
@@ -72,13 +72,17 @@ struct Box {
 // then reduces the boxes of binning-block row by = 8*blockIdx.y + warp: the
 // (BLOCK_W + 1) x (BLOCK_H + 1) vertices of block bx are the columns of
 // lanes 8*b .. 8*b + 8, rows 4*warp .. 4*warp + 4.
-__global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ ViewTable tab) {
+template <class Tabs>
+__global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs tabs, int max_views) {
     __shared__ float2 s_top[8][VT];        // first row of each warp (row 4*w)
     __shared__ float2 s_row[VT + 1];       // row i0 + 32, columns j0 .. j0 + 32
     __shared__ float2 s_col[VT + 1];       // column j0 + 32, rows i0 .. i0 + 32
     __shared__ float2 s_seam[VT + 1];      // column W - 1, rows i0 .. i0 + 32 (wrap)
-    const DevView& V = tab.v[blockIdx.z];
+    const SlotTable& tab = tabs.at(blockIdx.z / max_views);
+    const int view = blockIdx.z % max_views;
     const DevTarget& T = tab.t;
+    if (view >= T.n_views) return;
+    const DevView& V = tab.v[view];
     const int j0 = blockIdx.x * VT, i0 = blockIdx.y * VT;
     if (j0 >= V.w || i0 >= V.h) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -155,9 +159,13 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ ViewT
 
 }  // namespace
 
-void launch_warp(const ViewTable& tab, const LaunchShape& sh, cudaStream_t s) {
-    dim3 grid((sh.max_w + VT - 1) / VT, (sh.max_h + VT - 1) / VT, sh.n_views);
-    warp_kernel<<<grid, 256, 0, s>>>(tab);
+template <class Tabs>
+void launch_warp(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
+    dim3 grid((sh.max_w + VT - 1) / VT, (sh.max_h + VT - 1) / VT, sh.slots * sh.max_views);
+    warp_kernel<<<grid, 256, 0, s>>>(tabs, sh.max_views);
 }
+
+template void launch_warp<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);
+template void launch_warp<TablePtr>(const TablePtr&, const BatchShape&, cudaStream_t);
 
 }  // namespace rvsb

@@ -27,6 +27,8 @@ EXPORTED = [
     "rvsb_scene_destroy", "rvsb_scene_upload", "rvsb_synthesize", "rvsb_synthesize_host",
     "rvsb_synthesize_debug", "rvsb_synthesize_frame", "rvsb_scene_last_launch_count", "rvsb_scene_set_profiling",
     "rvsb_scene_stage_times", "rvsb_stage_name", "rvsb_inpaint_sources_noalloc",
+    "rvsb_batch_create", "rvsb_batch_destroy", "rvsb_batch_reserve", "rvsb_batch_set_graphs",
+    "rvsb_synthesize_batch", "rvsb_batch_last_launch_count", "rvsb_batch_set_profiling", "rvsb_batch_stage_times",
 ]
 
 STAGES = ["warp", "bin", "raster", "inpaint", "total"]
@@ -90,6 +92,15 @@ def load():
     L.rvsb_scene_stage_times.argtypes = [c_p, P(ctypes.c_float), ctypes.c_int]
     L.rvsb_stage_name.argtypes = [ctypes.c_int]
     L.rvsb_stage_name.restype = ctypes.c_char_p
+    L.rvsb_batch_create.argtypes = [c_p, ctypes.c_int, P(c_p)]
+    L.rvsb_batch_destroy.argtypes = [c_p]
+    L.rvsb_batch_destroy.restype = None
+    L.rvsb_batch_reserve.argtypes = [c_p, ctypes.c_int, ctypes.c_int]
+    L.rvsb_batch_set_graphs.argtypes = [c_p, ctypes.c_int]
+    L.rvsb_synthesize_batch.argtypes = [c_p, P(Camera), ctypes.c_int, P(SynthParams), P(Yuv420), c_p]
+    L.rvsb_batch_last_launch_count.argtypes = [c_p]
+    L.rvsb_batch_set_profiling.argtypes = [c_p, ctypes.c_int]
+    L.rvsb_batch_stage_times.argtypes = [c_p, P(ctypes.c_float), ctypes.c_int]
     L.rvsb_inpaint_sources_noalloc.argtypes = [c_p, ctypes.c_int, ctypes.c_int, c_p, c_p, ctypes.c_char_p,
                                                ctypes.c_size_t]
     _lib = L
@@ -215,6 +226,58 @@ class Scene:
     def close(self):
         if self.h:
             self.ctx.lib.rvsb_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """rvsb_batch: up to `slots` virtual views of one scene per launch group."""
+
+    def __init__(self, scene, slots, graphs=False):
+        self.scene = scene
+        self.ctx = scene.ctx
+        h = ctypes.c_void_p()
+        self.ctx.check(self.ctx.lib.rvsb_batch_create(scene.h, int(slots), ctypes.byref(h)))
+        self.h = h
+        self.slots = slots
+        if graphs:
+            self.set_graphs(True)
+
+    def reserve(self, max_width, max_height):
+        return self.ctx.check(self.ctx.lib.rvsb_batch_reserve(self.h, int(max_width), int(max_height)))
+
+    def set_graphs(self, on=True):
+        return self.ctx.check(self.ctx.lib.rvsb_batch_set_graphs(self.h, 1 if on else 0))
+
+    def set_profiling(self, on=True):
+        return self.ctx.check(self.ctx.lib.rvsb_batch_set_profiling(self.h, 1 if on else 0))
+
+    def stage_times(self):
+        buf = (ctypes.c_float * len(STAGES))()
+        n = self.ctx.lib.rvsb_batch_stage_times(self.h, buf, len(STAGES))
+        if n < 0:
+            raise RvsbError(-1, "no profiled batch")
+        return {STAGES[i]: buf[i] for i in range(n)}
+
+    def last_launch_count(self):
+        return self.ctx.lib.rvsb_batch_last_launch_count(self.h)
+
+    def synthesize(self, virts, p, outs, stream=None):
+        """virts: cameras; outs: one (y, u, v) device triple per camera."""
+        n = len(virts)
+        cams = (Camera * n)(*virts)
+        ys = (Yuv420 * n)(*[Yuv420(*(_ptr(a) for a in o)) for o in outs])
+        return self.ctx.check(self.ctx.lib.rvsb_synthesize_batch(self.h, cams, n, ctypes.byref(p), ys,
+                                                                 _stream(stream)))
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.rvsb_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -181,19 +181,21 @@ def plain_small(scale=1.0, seed=0x5EED0001):
     return Workload("plain_small", sc, inputs, targets)
 
 
-def plain_1080p(scale=1.0, seed=0x5EED0002):
+def plain_1080p(scale=1.0, seed=0x5EED0002, n_targets=1):
     """4 perspective inputs 1920x1080 (f = 1500) on a 2x2 grid, 0.15 m
-    spacing; 1 target at a seeded pose inside the grid (+-7.5 cm in y and z,
-    +-10 cm in x, +-5 degrees)."""
+    spacing; targets at seeded poses inside the grid (+-7.5 cm in y and z,
+    +-10 cm in x, +-5 degrees); the first is the plain workload's view."""
     w, h = _even(1920 * scale), _even(1080 * scale)
     f = 1500.0 * w / 1920.0
     sc = _front_scene(seed, 6, 4, 1.0, 8.0, 0.3)
     rng = Rng(seed ^ 0xABCDEF)
     inputs = [abi.make_camera(abi.PERSPECTIVE, w, h, (0, y, z), (0, 0, 0), (0.5, 10.0), (f, f))
               for z in (0.075, -0.075) for y in (0.075, -0.075)]
-    pos = (rng.uniform(-0.1, 0.1), rng.uniform(-0.075, 0.075), rng.uniform(-0.075, 0.075))
-    rot = (rng.uniform(-5, 5), rng.uniform(-5, 5), rng.uniform(-5, 5))
-    targets = [abi.make_camera(abi.PERSPECTIVE, w, h, pos, rot, (0.5, 10.0), (f, f))]
+    targets = []
+    for _ in range(n_targets):
+        pos = (rng.uniform(-0.1, 0.1), rng.uniform(-0.075, 0.075), rng.uniform(-0.075, 0.075))
+        rot = (rng.uniform(-5, 5), rng.uniform(-5, 5), rng.uniform(-5, 5))
+        targets.append(abi.make_camera(abi.PERSPECTIVE, w, h, pos, rot, (0.5, 10.0), (f, f)))
     return Workload("plain_1080p", sc, inputs, targets)
 
 

@@ -1,0 +1,102 @@
+"""Batches (rvsb_synthesize_batch): every slot's output is bit-identical to
+the per-view call for the same camera, whatever the batch composition
+(mixed output sizes and projections, partial groups), with and without
+CUDA graphs."""
+import copy
+
+import numpy as np
+import pytest
+
+import oracle as O
+import rvsb
+from rvsb import abi, scenes
+from helpers import assert_parity, to_u16, yuv_planes_torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _upload(ctx, wl):
+    sc = rvsb.Scene(ctx, wl.inputs)
+    for i, p in enumerate(wl.planes):
+        sc.upload(i, [np.ascontiguousarray(a, np.uint16) for a in p], on_device=False)
+    return sc
+
+
+def _yuv(out, cam):
+    wo, ho = cam.width, cam.height
+    return (to_u16(out[0], (ho, wo)), to_u16(out[1], (ho // 2, wo // 2)), to_u16(out[2], (ho // 2, wo // 2)))
+
+
+def _single(sc, cam, p):
+    import torch
+    out = yuv_planes_torch(cam.width, cam.height)
+    sc.synthesize(cam, p, out)
+    torch.cuda.synchronize()
+    return _yuv(out, cam)
+
+
+def _targets_small(wl):
+    base = wl.targets[0]
+    cams = []
+    for k in range(5):
+        c = copy.deepcopy(base)
+        c.position[1] += 0.01 * (k - 2)
+        c.rotation[0] += 1.5 * (k - 2)
+        if k == 1:  # a smaller output
+            c.width, c.height = 64, 36
+            c.focal[0] = c.focal[1] = c.focal[0] * 64 / base.width
+            c.principle_point[0], c.principle_point[1] = 32.0, 18.0
+        if k == 3:  # a 360-degree output
+            c = abi.make_camera(abi.EQUIRECTANGULAR, 128, 64, tuple(base.position), (10.0, 0, 0), (0.3, 20.0))
+        cams.append(c)
+    return cams
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+@pytest.mark.parametrize("slots", [1, 3, 8])
+def test_batch_matches_single(ctx, graphs, slots):
+    import torch
+    wl = scenes.random_pose_small(n_views=3, w=96, h=54, seed=51)
+    sc = _upload(ctx, wl)
+    cams = _targets_small(wl)
+    p = rvsb.params(5.0)
+    expected = [_single(sc, c, p) for c in cams]
+    b = rvsb.Batch(sc, slots, graphs=graphs)
+    for rep in range(2):  # the second pass replays the captured graphs
+        outs = [yuv_planes_torch(c.width, c.height) for c in cams]
+        b.synthesize(cams, p, outs)
+        torch.cuda.synchronize()
+        for c, o, e in zip(cams, outs, expected):
+            for x, y in zip(_yuv(o, c), e):
+                np.testing.assert_array_equal(x, y)
+    assert b.last_launch_count() == 12
+    b.close()
+
+
+def test_batch_matches_oracle(ctx):
+    import torch
+    wl = scenes.random_pose_small(n_views=2, w=96, h=54, seed=52)
+    sc = _upload(ctx, wl)
+    cams = _targets_small(wl)[:3]
+    outs = [yuv_planes_torch(c.width, c.height) for c in cams]
+    b = rvsb.Batch(sc, 4, graphs=True)
+    b.synthesize(cams, rvsb.params(5.0), outs)
+    torch.cuda.synchronize()
+    for c, o in zip(cams, outs):
+        assert_parity(_yuv(o, c), O.synthesize(wl.inputs, wl.planes, c, 5.0))
+
+
+def test_batch_1080p_matches_single(ctx):
+    import torch
+    wl = scenes.plain_1080p(n_targets=6)
+    sc = _upload(ctx, wl)
+    p = rvsb.params(wl.blending_factor)
+    expected = [_single(sc, c, p) for c in wl.targets]
+    b = rvsb.Batch(sc, 4, graphs=True)
+    b.reserve(1920, 1080)
+    outs = [yuv_planes_torch(c.width, c.height) for c in wl.targets]
+    b.synthesize(wl.targets, p, outs)
+    torch.cuda.synchronize()
+    for c, o, e in zip(wl.targets, outs, expected):
+        for x, y in zip(_yuv(o, c), e):
+            np.testing.assert_array_equal(x, y)
