@@ -208,6 +208,103 @@ def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world):
             "workload": f"plain_1080p scene, {slots} seeded poses per batch"}
 
 
+def serving_targets(workloads, n, seed=0x5E7E):
+    """n requests of the serving mix: scene set chosen uniformly, output
+    960x540 / 1920x1080 perspective / 4096x2048 equirectangular in ratio
+    5:4:1, pose drawn around the scene set's own target poses."""
+    import copy
+    import random
+    from rvsb import abi
+    rng = random.Random(seed)
+    out = []
+    for _ in range(n):
+        s = rng.randrange(len(workloads))
+        base = copy.deepcopy(rng.choice(workloads[s].targets))
+        r = rng.random()
+        pos = [base.position[k] + rng.uniform(-0.02, 0.02) for k in range(3)]
+        if r < 0.1:
+            near_far = tuple(base.depth_range)
+            cam = abi.make_camera(abi.EQUIRECTANGULAR, 4096, 2048, pos, (rng.uniform(-180, 180), 0, 0), near_far)
+            cls = "erp4096x2048"
+        else:
+            w, h = (960, 540) if r < 0.6 else (1920, 1080)
+            if base.projection == abi.EQUIRECTANGULAR:
+                f = w / 2.0
+            else:
+                f = base.focal[0] * w / base.width
+            rot = (base.rotation[0] + rng.uniform(-2, 2), base.rotation[1], base.rotation[2])
+            cam = abi.make_camera(abi.PERSPECTIVE, w, h, pos, rot, tuple(base.depth_range), (f, f))
+            cls = f"{w}x{h}"
+        out.append((s, cam, cls))
+    return out
+
+
+def measure_served(ctx, seconds, rate, lanes, max_batch, p):
+    """Open-loop serving: Poisson arrivals at `rate` requests/s for `seconds`
+    on the three resident scene sets (2 x 960x540, 4 x 1920x1080, 4 x ERP
+    4096x2048 inputs).  Returns views/s and latency percentiles."""
+    import random
+    import numpy as np
+    import torch
+    import rvsb
+    from rvsb import scenes
+    wls = [scenes.plain_small(), scenes.plain_1080p(n_targets=8), scenes.batched_erp(n_targets=64)]
+    scs = []
+    for wl in wls:
+        scenes.cache_planes(wl, CACHE)
+        sc = rvsb.Scene(ctx, wl.inputs)
+        for i, planes in enumerate(wl.planes):
+            sc.upload(i, [np.ascontiguousarray(a, np.uint16) for a in planes], on_device=False)
+        scs.append(sc)
+    srv = rvsb.Server(ctx, lanes=lanes, max_batch=max_batch)
+    ids = [srv.add_scene(sc) for sc in scs]
+    for sid in ids:
+        srv.reserve(sid, 1920, 1080)
+        srv.reserve(sid, 4096, 2048)
+    n = int(seconds * rate)
+    reqs = serving_targets(wls, n)
+    ring = {}
+    for cls, (w, h) in (("960x540", (960, 540)), ("1920x1080", (1920, 1080)), ("erp4096x2048", (4096, 2048))):
+        ring[cls] = [[torch.empty(k, dtype=torch.int16, device="cuda") for k in (w * h, w * h // 4, w * h // 4)]
+                     for _ in range(16)]
+    # warm-up: a few requests of each class on each scene set
+    for k, (s, cam, cls) in enumerate(reqs[:24]):
+        srv.submit(ids[s], cam, p, ring[cls][k % 16])
+    srv.drain(600000)
+    srv.poll(100000)
+    torch.cuda.synchronize()
+    rng = random.Random(0xA221)
+    t_next = time.perf_counter()
+    submitted = 0
+    for k, (s, cam, cls) in enumerate(reqs):
+        t_next += rng.expovariate(rate)
+        while True:
+            d = t_next - time.perf_counter()
+            if d <= 0:
+                break
+            if d > 2e-4:
+                time.sleep(d - 1e-4)
+        srv.submit(ids[s], cam, p, ring[cls][k % 16])
+        submitted += 1
+    srv.drain(600000)
+    res = srv.poll(n + 16)
+    srv.close()
+    for sc in scs:
+        sc.close()
+    lat = sorted((r[5] - r[3]) * 1000.0 for r in res if r[1] == 0)
+    t0 = min(r[3] for r in res)
+    t1 = max(r[5] for r in res)
+    per_class = {}
+    by_id = {r[0]: r for r in res}
+    return {"value": len(lat) / (t1 - t0), "unit": UNIT, "requests": len(res), "failed": sum(r[1] != 0 for r in res),
+            "offered_rate": rate, "seconds": seconds, "lanes": lanes, "max_batch": max_batch,
+            "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99), "max_ms": lat[-1] if lat else None,
+            "mean_batch": statistics.mean(r[2] for r in res),
+            "mix": "scene sets 2x960x540 / 4x1920x1080 / 4xERP4096x2048 uniform; outputs 960x540 : 1920x1080 : "
+                   "ERP 4096x2048 = 5:4:1; Poisson arrivals; 60 GB budget",
+            "duration_note": f"{seconds:g} s of arrivals (the serving configuration names 60 s)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -218,6 +315,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-slots", type=int, default=16)
     ap.add_argument("--batch-steps", type=int, default=8)
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-rate", type=float, default=500.0)
+    ap.add_argument("--serve-lanes", type=int, default=4)
+    ap.add_argument("--serve-batch", type=int, default=2)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -303,6 +404,9 @@ def main():
     e2e_total = allreduce_max(sum(e2e_ms) / 1000.0, world)
     e2e_value = world * args.e2e_steps / e2e_total
     batched = measure_batched(ctx, scene, wl, args.batch_slots, args.batch_steps, flush, stream, world)
+    served = None
+    if args.serve_seconds > 0:
+        served = measure_served(ctx, args.serve_seconds, args.serve_rate, args.serve_lanes, args.serve_batch, p)
     clocks = sampler.stop()
 
     # Roofline of the dominant kernel (per launch, averaged over the timed steps).
@@ -367,6 +471,7 @@ def main():
                     "p50_ms": percentile(e2e_ms, 50), "p99_ms": percentile(e2e_ms, 99),
                     "call": "rvsb_synthesize_host (pinned host buffers)"},
             "batched": batched,
+            "served": served,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,

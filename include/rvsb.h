@@ -306,6 +306,49 @@ int rvsb_batch_last_launch_count(const rvsb_batch* batch);
 rvsb_status rvsb_batch_set_profiling(rvsb_batch* batch, int enable);
 int rvsb_batch_stage_times(rvsb_batch* batch, float* ms, int max_stages);
 
+/* ----------------------------------------------------------------------- */
+/* Serving: requests on resident scenes, continuous batching               */
+/* ----------------------------------------------------------------------- */
+
+/* No counterpart in the reference, which renders the frames of one
+ * configuration in sequence (rvs/src/Application.cpp:53-65).  A server
+ * accepts virtual-camera requests at any time on scenes whose input views
+ * are resident, and a worker thread runs them on `lanes` independent batch
+ * slots groups (one stream each): whenever a lane is free it launches every
+ * waiting request that fits, up to `max_batch`, in arrival order, while the
+ * workspace bytes of the requests in flight stay within `hbm_budget_bytes`
+ * (0 = the context's budget).  Requests may mix scenes, output sizes and
+ * projections; each output is identical to the same request alone. */
+typedef struct rvsb_server rvsb_server;
+
+typedef struct rvsb_request_result {
+    uint64_t id;
+    int32_t status;      /* rvsb_status of the request */
+    int32_t batch_size;  /* requests launched together with it */
+    double submit_s;     /* times on the server's clock (seconds) */
+    double start_s;
+    double done_s;
+} rvsb_request_result;
+
+rvsb_status rvsb_server_create(rvsb_context* ctx, int lanes, int max_batch, size_t hbm_budget_bytes,
+                               rvsb_server** out);
+/* Registers a scene (all views uploaded); its id goes to *scene_id. */
+rvsb_status rvsb_server_add_scene(rvsb_server* server, rvsb_scene* scene, int* scene_id);
+/* Allocates every slot's workspace for this scene at outputs up to
+ * max_width x max_height, so serving does not allocate.  Only while idle. */
+rvsb_status rvsb_server_reserve(rvsb_server* server, int scene_id, int max_width, int max_height);
+/* Queues one request; `out` holds device planes the caller keeps valid
+ * until the request's result has been polled. */
+rvsb_status rvsb_server_submit(rvsb_server* server, int scene_id, const rvsb_camera* virt,
+                               const rvsb_synth_params* params, const rvsb_yuv420* out, uint64_t* request_id);
+/* Moves up to max_results finished requests into results; returns the count. */
+int rvsb_server_poll(rvsb_server* server, rvsb_request_result* results, int max_results);
+/* Waits until no request is waiting or running (RVSB_E_TIMEOUT otherwise). */
+rvsb_status rvsb_server_drain(rvsb_server* server, int timeout_ms);
+/* Seconds on the server's clock (the clock of the result times). */
+double rvsb_server_clock(const rvsb_server* server);
+void rvsb_server_destroy(rvsb_server* server);
+
 /* Per-stage timing with CUDA events recorded on the launch stream (the
  * per-stage timers that replace the reference's whole-run clock(),
  * rvs/src/view_synthesis.cpp:149-166).  Stages: 0 warp, 1 bin, 2 raster

@@ -19,7 +19,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["launch.cu", "decode.cu", "warp.cu", "bin.cu", "tile.cu", "inpaint.cu", "noalloc.cu"]
-CPP_SOURCES = ["api.cpp", "engine.cpp", "frontend.cpp", "camera.cpp"]
+CPP_SOURCES = ["api.cpp", "engine.cpp", "server.cpp", "frontend.cpp", "camera.cpp"]
 CLI_SOURCES = ["rvsb_cli.cpp"]
 SCENEGEN_SOURCES = ["scenegen.cpp"]
 

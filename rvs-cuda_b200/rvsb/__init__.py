@@ -29,6 +29,8 @@ EXPORTED = [
     "rvsb_scene_stage_times", "rvsb_stage_name", "rvsb_inpaint_sources_noalloc",
     "rvsb_batch_create", "rvsb_batch_destroy", "rvsb_batch_reserve", "rvsb_batch_set_graphs",
     "rvsb_synthesize_batch", "rvsb_batch_last_launch_count", "rvsb_batch_set_profiling", "rvsb_batch_stage_times",
+    "rvsb_server_create", "rvsb_server_add_scene", "rvsb_server_reserve", "rvsb_server_submit", "rvsb_server_poll",
+    "rvsb_server_drain", "rvsb_server_clock", "rvsb_server_destroy",
 ]
 
 STAGES = ["warp", "bin", "raster", "inpaint", "total"]
@@ -101,6 +103,16 @@ def load():
     L.rvsb_batch_last_launch_count.argtypes = [c_p]
     L.rvsb_batch_set_profiling.argtypes = [c_p, ctypes.c_int]
     L.rvsb_batch_stage_times.argtypes = [c_p, P(ctypes.c_float), ctypes.c_int]
+    L.rvsb_server_create.argtypes = [c_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t, P(c_p)]
+    L.rvsb_server_add_scene.argtypes = [c_p, c_p, P(ctypes.c_int)]
+    L.rvsb_server_reserve.argtypes = [c_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.rvsb_server_submit.argtypes = [c_p, ctypes.c_int, P(Camera), P(SynthParams), P(Yuv420), P(ctypes.c_uint64)]
+    L.rvsb_server_poll.argtypes = [c_p, P(RequestResult), ctypes.c_int]
+    L.rvsb_server_drain.argtypes = [c_p, ctypes.c_int]
+    L.rvsb_server_clock.argtypes = [c_p]
+    L.rvsb_server_clock.restype = ctypes.c_double
+    L.rvsb_server_destroy.argtypes = [c_p]
+    L.rvsb_server_destroy.restype = None
     L.rvsb_inpaint_sources_noalloc.argtypes = [c_p, ctypes.c_int, ctypes.c_int, c_p, c_p, ctypes.c_char_p,
                                                ctypes.c_size_t]
     _lib = L
@@ -278,6 +290,62 @@ class Batch:
     def close(self):
         if self.h:
             self.ctx.lib.rvsb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RequestResult(ctypes.Structure):
+    """rvsb_request_result."""
+
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("batch_size", ctypes.c_int32),
+                ("submit_s", ctypes.c_double), ("start_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+
+class Server:
+    """rvsb_server: requests on resident scenes with continuous batching."""
+
+    def __init__(self, ctx, lanes=4, max_batch=4, hbm_budget=0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = ctypes.c_void_p()
+        ctx.check(self.lib.rvsb_server_create(ctx.h, int(lanes), int(max_batch), int(hbm_budget), ctypes.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def add_scene(self, scene):
+        sid = ctypes.c_int()
+        self.ctx.check(self.lib.rvsb_server_add_scene(self.h, scene.h, ctypes.byref(sid)))
+        return sid.value
+
+    def reserve(self, scene_id, max_width, max_height):
+        return self.ctx.check(self.lib.rvsb_server_reserve(self.h, int(scene_id), int(max_width), int(max_height)))
+
+    def submit(self, scene_id, virt, p, out_planes):
+        out = Yuv420(*(_ptr(a) for a in out_planes))
+        rid = ctypes.c_uint64()
+        self.ctx.check(self.lib.rvsb_server_submit(self.h, int(scene_id), ctypes.byref(virt), ctypes.byref(p),
+                                                   ctypes.byref(out), ctypes.byref(rid)))
+        return rid.value
+
+    def poll(self, max_results=4096):
+        buf = (RequestResult * max_results)()
+        n = self.lib.rvsb_server_poll(self.h, buf, max_results)
+        return [(r.id, r.status, r.batch_size, r.submit_s, r.start_s, r.done_s) for r in buf[:n]]
+
+    def drain(self, timeout_ms=60000):
+        return self.ctx.check(self.lib.rvsb_server_drain(self.h, int(timeout_ms)))
+
+    def clock(self):
+        return self.lib.rvsb_server_clock(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.rvsb_server_destroy(self.h)
             self.h = None
 
     def __del__(self):
