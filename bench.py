@@ -208,6 +208,49 @@ def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world):
             "workload": f"plain_1080p scene, {slots} seeded poses per batch"}
 
 
+def measure_batched_workload(ctx, name, slots, flush, stream, reps=2):
+    """Views/s of a batched configuration: every target of the workload
+    synthesised with rvsb_synthesize_batch in groups of `slots` (one graph
+    replay per group), inputs resident; `reps` timed passes over all targets,
+    L2 flushed before each pass."""
+    import numpy as np
+    import torch
+    import rvsb
+    from rvsb import scenes
+    wl = scenes.WORKLOADS[name]()
+    scenes.cache_planes(wl, CACHE)
+    sc = rvsb.Scene(ctx, wl.inputs)
+    for i, planes in enumerate(wl.planes):
+        sc.upload(i, [np.ascontiguousarray(a, np.uint16) for a in planes], on_device=False)
+    p = rvsb.params(wl.blending_factor)
+    batch = rvsb.Batch(sc, slots, graphs=True)
+    batch.reserve(max(c.width for c in wl.targets), max(c.height for c in wl.targets))
+    outs = [[torch.empty(n, dtype=torch.int16, device="cuda")
+             for n in (c.width * c.height, (c.width // 2) * (c.height // 2), (c.width // 2) * (c.height // 2))]
+            for c in wl.targets]
+    batch.synthesize(wl.targets, p, outs, stream=stream)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch.synthesize(wl.targets, p, outs, stream=stream)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    n = len(wl.targets)
+    batch.close()
+    sc.close()
+    del outs
+    torch.cuda.empty_cache()
+    return {"value": n * reps / (sum(ms) / 1000.0), "unit": UNIT, "targets": n, "slots": slots,
+            "ms_per_view": statistics.mean(ms) / n,
+            "inputs": f"{len(wl.inputs)} x {wl.inputs[0].width}x{wl.inputs[0].height}"
+                      f" {'ERP' if wl.inputs[0].projection else 'perspective'}",
+            "outputs": sorted({f"{c.width}x{c.height}" for c in wl.targets})}
+
+
 def serving_targets(workloads, n, seed=0x5E7E):
     """n requests of the serving mix: scene set chosen uniformly, output
     960x540 / 1920x1080 perspective / 4096x2048 equirectangular in ratio
@@ -319,6 +362,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=500.0)
     ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=2)
+    ap.add_argument("--no-batched-configs", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -404,6 +448,12 @@ def main():
     e2e_total = allreduce_max(sum(e2e_ms) / 1000.0, world)
     e2e_value = world * args.e2e_steps / e2e_total
     batched = measure_batched(ctx, scene, wl, args.batch_slots, args.batch_steps, flush, stream, world)
+    batched_configs = None
+    if not args.no_batched_configs:
+        batched_configs = {
+            "batched_erp": measure_batched_workload(ctx, "batched_erp", 32, flush, stream),
+            "batched_mixed": measure_batched_workload(ctx, "batched_mixed", 64, flush, stream),
+        }
     served = None
     if args.serve_seconds > 0:
         served = measure_served(ctx, args.serve_seconds, args.serve_rate, args.serve_lanes, args.serve_batch, p)
@@ -472,6 +522,7 @@ def main():
                     "call": "rvsb_synthesize_host (pinned host buffers)"},
             "batched": batched,
             "served": served,
+            "batched_configs": batched_configs,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,

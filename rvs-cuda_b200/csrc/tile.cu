@@ -161,16 +161,38 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
             t.x1 = __shfl_sync(0xffffffffu, s.x1, src);
             t.y0 = __shfl_sync(0xffffffffu, s.y0, src);
             t.y1 = __shfl_sync(0xffffffffu, s.y1, src);
-            // One lane per row of the (tile-clipped) range: at most TILE rows.
+            // Candidate span of each row of the (tile-clipped) range, one lane
+            // per row (at most TILE rows), then the spans' pixels flattened
+            // over the warp: 32 candidates per round whatever the shape.
             const int y = t.y0 + lane;
-            if (y <= t.y1) {
-                int xl, xr;
-                row_span(t, cx, cy, y, xl, xr);
-                for (int x = xl; x <= xr; ++x) {
-                    float d;
-                    if (!test_pixel(t, cx, cy, za, zb_, zc, x, y, d)) continue;
-                    atomicMin(&zb[(y - ty0) * TILE + (x - tx0)], frag_key(d, invq, ttri));
+            int xl = 0, xr = -1;
+            if (y <= t.y1) row_span(t, cx, cy, y, xl, xr);
+            const int len = max(0, xr - xl + 1);
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int excl = incl - len;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int base = 0; base < total; base += 32) {
+                const int c = base + lane;
+                // Row of candidate c: the number of rows whose spans end at
+                // or before c (binary search over the inclusive prefix).
+                int row = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int probe = __shfl_sync(0xffffffffu, incl, row + step - 1);
+                    if (probe <= c) row += step;
                 }
+                const int rxl = __shfl_sync(0xffffffffu, xl, row);
+                const int rex = __shfl_sync(0xffffffffu, excl, row);
+                if (c >= total) continue;
+                const int x = rxl + (c - rex), yy = t.y0 + row;
+                float d;
+                if (!test_pixel(t, cx, cy, za, zb_, zc, x, yy, d)) continue;
+                atomicMin(&zb[(yy - ty0) * TILE + (x - tx0)], frag_key(d, invq, ttri));
             }
         }
     }
