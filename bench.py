@@ -182,6 +182,7 @@ def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world):
     targets = scenes.plain_1080p(n_targets=slots + 1).targets[1:]
     p = rvsb.params(wl.blending_factor)
     batch = rvsb.Batch(scene, slots, graphs=True)
+    batch.set_autotune(True)
     batch.reserve(targets[0].width, targets[0].height)
     outs = [[torch.empty(n, dtype=torch.int16, device="cuda")
              for n in (c.width * c.height, (c.width // 2) * (c.height // 2), (c.width // 2) * (c.height // 2))]
@@ -199,12 +200,13 @@ def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world):
         b.synchronize()
         ms.append(a.elapsed_time(b))
     launches = batch.last_launch_count()
+    variant = batch.last_raster_variant()
     batch.close()
     from rvsb import replicas
     total = replicas.max_over_ranks(sum(ms) / 1000.0, world)
     return {"value": world * slots * steps / total, "unit": UNIT, "slots": slots, "batches": steps,
             "ms_per_batch": statistics.mean(ms), "ms_per_view": statistics.mean(ms) / slots,
-            "launches_per_batch": launches, "graphs": True,
+            "launches_per_batch": launches, "graphs": True, "raster_variant": variant,
             "workload": f"plain_1080p scene, {slots} seeded poses per batch"}
 
 
@@ -224,6 +226,7 @@ def measure_batched_workload(ctx, name, slots, flush, stream, reps=2):
         sc.upload(i, [np.ascontiguousarray(a, np.uint16) for a in planes], on_device=False)
     p = rvsb.params(wl.blending_factor)
     batch = rvsb.Batch(sc, slots, graphs=True)
+    batch.set_autotune(True)
     batch.reserve(max(c.width for c in wl.targets), max(c.height for c in wl.targets))
     outs = [[torch.empty(n, dtype=torch.int16, device="cuda")
              for n in (c.width * c.height, (c.width // 2) * (c.height // 2), (c.width // 2) * (c.height // 2))]
@@ -240,11 +243,13 @@ def measure_batched_workload(ctx, name, slots, flush, stream, reps=2):
         b.synchronize()
         ms.append(a.elapsed_time(b))
     n = len(wl.targets)
+    variant = batch.last_raster_variant()
     batch.close()
     sc.close()
     del outs
     torch.cuda.empty_cache()
     return {"value": n * reps / (sum(ms) / 1000.0), "unit": UNIT, "targets": n, "slots": slots,
+            "raster_variant": variant,
             "ms_per_view": statistics.mean(ms) / n,
             "inputs": f"{len(wl.inputs)} x {wl.inputs[0].width}x{wl.inputs[0].height}"
                       f" {'ERP' if wl.inputs[0].projection else 'perspective'}",
@@ -395,6 +400,7 @@ def main():
     out = [torch.empty(n, dtype=torch.int16, device="cuda")
            for n in (wo * ho, (wo // 2) * (ho // 2), (wo // 2) * (ho // 2))]
     scene.set_profiling(True)
+    scene.set_autotune(True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def plain_step():

@@ -275,6 +275,9 @@ rvsb_status rvsb_synthesize_debug(rvsb_scene* scene, const rvsb_camera* virt,
 /* Kernel launches issued by the most recent synthesis call of the scene
  * (for launch accounting). */
 int rvsb_scene_last_launch_count(const rvsb_scene* scene);
+/* The raster autotuner (see rvsb_batch_set_autotune) for the per-view calls
+ * of this scene (default off). */
+rvsb_status rvsb_scene_set_autotune(rvsb_scene* scene, int enable);
 
 /* ----------------------------------------------------------------------- */
 /* Batches: many virtual views of one resident scene                       */
@@ -298,6 +301,17 @@ void rvsb_batch_destroy(rvsb_batch* batch);
 rvsb_status rvsb_batch_reserve(rvsb_batch* batch, int max_width, int max_height);
 /* Capture each batch shape into a CUDA graph and replay it (default off). */
 rvsb_status rvsb_batch_set_graphs(rvsb_batch* batch, int enable);
+/* Raster autotuner (default off): the first batch of each new shape (batch
+ * size bucket, largest input set and output, projections) is run once with
+ * every raster variant -- tile size 32x32, 64x32 or 32x16, views per shared
+ * z-buffer group, the stretched-triangle threshold and the bin entries
+ * staged per round -- and the fastest is kept for that shape.  All variants
+ * give identical outputs. */
+rvsb_status rvsb_batch_set_autotune(rvsb_batch* batch, int enable);
+/* Use one raster variant (0 .. 5) for every call, or -1 for the default or
+ * tuned one; the variant used by the last call. */
+rvsb_status rvsb_batch_set_raster_variant(rvsb_batch* batch, int variant);
+int rvsb_batch_last_raster_variant(const rvsb_batch* batch);
 /* n virtual views (outputs may differ in size and projection), processed in
  * groups of max_slots on `stream`. */
 rvsb_status rvsb_synthesize_batch(rvsb_batch* batch, const rvsb_camera* virts, int n,

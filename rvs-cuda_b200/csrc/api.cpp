@@ -344,6 +344,29 @@ rvsb_status rvsb_batch_set_graphs(rvsb_batch* batch, int enable) {
     return RVSB_OK;
 }
 
+rvsb_status rvsb_batch_set_autotune(rvsb_batch* batch, int enable) {
+    if (!batch) return RVSB_E_ARG;
+    batch->core->set_autotune(enable != 0);
+    return RVSB_OK;
+}
+
+rvsb_status rvsb_batch_set_raster_variant(rvsb_batch* batch, int variant) {
+    if (!batch || variant < -1 || variant >= NUM_RASTER_VARIANTS) return RVSB_E_ARG;
+    batch->core->force_variant(variant);
+    return RVSB_OK;
+}
+
+int rvsb_batch_last_raster_variant(const rvsb_batch* batch) { return batch ? batch->core->last_variant() : -1; }
+
+rvsb_status rvsb_scene_set_autotune(rvsb_scene* sc, int enable) {
+    if (!sc) return RVSB_E_ARG;
+    return guarded(sc->ctx, [&]() -> rvsb_status {
+        check(cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+        single_core(sc).set_autotune(enable != 0);
+        return RVSB_OK;
+    });
+}
+
 rvsb_status rvsb_batch_set_profiling(rvsb_batch* batch, int enable) {
     if (!batch) return RVSB_E_ARG;
     return guarded(batch->scene->ctx, [&]() -> rvsb_status {

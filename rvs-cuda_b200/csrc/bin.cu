@@ -20,7 +20,8 @@ __global__ void bin_count_kernel(const __grid_constant__ Tabs tabs) {
     const int4 bb = V.bbox[b];
     if (bb.x > bb.z || bb.y > bb.w) return;
     const int ntx = tab.t.ntx, n = tab.t.n_views;
-    const int tx0 = bb.x / TILE, tx1 = bb.z / TILE, ty0 = bb.y / TILE, ty1 = bb.w / TILE;
+    const int wl = tab.t.tile_wl, hl = tab.t.tile_hl;
+    const int tx0 = bb.x >> wl, tx1 = bb.z >> wl, ty0 = bb.y >> hl, ty1 = bb.w >> hl;
     int* counts = tab.b.counts;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) atomicAdd(&counts[(ty * ntx + tx) * n + v], 1);
@@ -80,7 +81,8 @@ __global__ void bin_fill_kernel(const __grid_constant__ Tabs tabs) {
     const int4 bb = V.bbox[b];
     if (bb.x > bb.z || bb.y > bb.w) return;
     const int ntx = tab.t.ntx, n = tab.t.n_views;
-    const int tx0 = bb.x / TILE, tx1 = bb.z / TILE, ty0 = bb.y / TILE, ty1 = bb.w / TILE;
+    const int wl = tab.t.tile_wl, hl = tab.t.tile_hl;
+    const int tx0 = bb.x >> wl, tx1 = bb.z >> wl, ty0 = bb.y >> hl, ty1 = bb.w >> hl;
     int* cursor = tab.b.cursor;
     int* list = tab.b.list;
     for (int ty = ty0; ty <= ty1; ++ty)

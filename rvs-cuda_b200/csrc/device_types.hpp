@@ -6,12 +6,15 @@
 namespace rvsb {
 
 // Tiling constants.  A binning block is BLOCK_W x BLOCK_H quads of an input
-// view (each quad = two triangles, transform.cpp:159-176); an output tile is
-// TILE x TILE pixels whose 64-bit z-buffer lives in shared memory.
+// view (each quad = two triangles, transform.cpp:159-176); an output tile
+// (its size is chosen per batch among the raster variants) holds 64-bit
+// z-buffers in shared memory and is processed by TILE_THREADS threads.
 constexpr int BLOCK_W = 8;
 constexpr int BLOCK_H = 4;
-constexpr int TILE = 32;
 constexpr int TILE_THREADS = 256;
+// Smallest tile of any raster variant (sizes the bin arrays).
+constexpr int MIN_TILE_W = 32;
+constexpr int MIN_TILE_H = 16;
 
 // Per input view parameters of one synthesis (device copy in a table).
 struct DevView {
@@ -52,6 +55,7 @@ struct DevTarget {
     float inv_blend_exp;                  // 1.0f / BlendingFactor
     int blend_exp_int;                    // BlendingFactor when it is an integer in [2, 16], else 0
     int chroma_ties_up;                   // output chroma mean: 1 rounds ties up, 0 to even
+    int tile_wl, tile_hl;                 // log2 of the tile width and height
     int ntx, nty;                         // output tiles
     int n_views;
     int bin_capacity;

@@ -61,7 +61,7 @@ SlotNeeds needs_of(const rvsb_scene* sc, int wo, int ho) {
         n.bbox += (size_t)nblocks_x(c.width) * nblocks_y(c.height);
     }
     n.out = (size_t)wo * ho;
-    n.bins = (size_t)((wo + TILE - 1) / TILE) * ((ho + TILE - 1) / TILE) * sc->cams.size();
+    n.bins = (size_t)((wo + MIN_TILE_W - 1) / MIN_TILE_W) * ((ho + MIN_TILE_H - 1) / MIN_TILE_H) * sc->cams.size();
     n.list = std::min<size_t>(INT32_MAX / 2, std::max<size_t>(1 << 16, n.bbox * 8 + n.bins));
     return n;
 }
@@ -115,6 +115,7 @@ BatchCore::BatchCore(rvsb_context* ctx, int slots) : ctx_(ctx), slots_(slots) {
         check(cudaEventCreateWithFlags(&copied_[b], cudaEventDisableTiming), "cudaEventCreate");
     }
     check(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : tune_ev_) check(cudaEventCreate(&e), "cudaEventCreate");
 }
 
 BatchCore::~BatchCore() {
@@ -129,6 +130,8 @@ BatchCore::~BatchCore() {
     for (auto& e : events_)
         if (e) cudaEventDestroy(e);
     if (capture_) cudaStreamDestroy(capture_);
+    for (auto& e : tune_ev_)
+        if (e) cudaEventDestroy(e);
 }
 
 void BatchCore::set_profiling(bool on) {
@@ -149,7 +152,15 @@ int BatchCore::stage_times(float* ms, int max_stages) const {
     return n;
 }
 
-void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r) {
+namespace {
+int log2i(int v) {
+    int l = 0;
+    while ((1 << l) < v) ++l;
+    return l;
+}
+}  // namespace
+
+void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
     std::memset(&T, 0, sizeof(T));
     const rvsb_scene* sc = r.scene;
     SlotWorkspace& ws = *ws_[k];
@@ -214,8 +225,11 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r) {
     if (p.blending_factor == std::floor(p.blending_factor) && p.blending_factor >= 2.f && p.blending_factor <= 16.f)
         D.blend_exp_int = (int)p.blending_factor;
     D.chroma_ties_up = p.chroma_rounding == RVSB_CHROMA_TIES_UP;
-    D.ntx = (virt.width + TILE - 1) / TILE;
-    D.nty = (virt.height + TILE - 1) / TILE;
+    const RasterVariant& rv = kRasterVariants[variant];
+    D.tile_wl = log2i(rv.tw);
+    D.tile_hl = log2i(rv.th);
+    D.ntx = (virt.width + rv.tw - 1) / rv.tw;
+    D.nty = (virt.height + rv.th - 1) / rv.th;
     D.n_views = n;
     D.bin_capacity = (int)ws.cap_list;
     SlotBuffers& B = T.b;
@@ -234,14 +248,13 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r) {
     T.dbg = r.dbg;
 }
 
-int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
-    if (n <= 0 || n > slots_) throw ArgError("batch of " + std::to_string(n) + " requests for " +
-                                             std::to_string(slots_) + " slots");
+BatchShape BatchCore::shape_of(const SlotRequest* reqs, int n, int variant) const {
+    const RasterVariant& rv = kRasterVariants[variant];
     BatchShape sh;
     sh.slots = n;
+    sh.variant = variant;
     for (int k = 0; k < n; ++k) {
         const SlotRequest& r = reqs[k];
-        ws_[k]->ensure(ctx_, r.scene, r.virt.width, r.virt.height);
         const int nv = (int)r.scene->cams.size();
         sh.max_views = std::max(sh.max_views, nv);
         for (const auto& c : r.scene->cams) {
@@ -249,35 +262,37 @@ int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
             sh.max_h = std::max(sh.max_h, c.height);
             sh.max_blocks = std::max(sh.max_blocks, nblocks_x(c.width) * nblocks_y(c.height));
         }
-        const int ntiles = ((r.virt.width + TILE - 1) / TILE) * ((r.virt.height + TILE - 1) / TILE);
+        const int ntiles = ((r.virt.width + rv.tw - 1) / rv.tw) * ((r.virt.height + rv.th - 1) / rv.th);
         sh.max_wo = std::max(sh.max_wo, r.virt.width);
         sh.max_ho = std::max(sh.max_ho, r.virt.height);
         sh.max_tiles = std::max(sh.max_tiles, ntiles);
         sh.max_bins = std::max(sh.max_bins, ntiles * nv);
     }
+    return sh;
+}
+
+int BatchCore::launch_variant(const SlotRequest* reqs, int n, int variant, cudaStream_t s) {
+    const BatchShape sh = shape_of(reqs, n, variant);
     if (n == 1 && !use_graphs_) {
         // A single synthesis: the table travels as a kernel parameter.
         TableParam tp;
-        fill(tp.t, 0, reqs[0]);
+        fill(tp.t, 0, reqs[0], variant);
         const int launches = launch_batch(tp, sh, s, profiling_ ? events_ : nullptr);
         if (launches < 0) check(cudaGetLastError(), "kernel launch");
-        profiled_ = profiling_;
-        last_launches_ = launches;
         return launches;
     }
     // The staging buffer is reused every other call: its previous copy must
     // have been consumed.
     check(cudaEventSynchronize(copied_[cur_]), "wait for table staging");
-    for (int k = 0; k < n; ++k) fill(staging_[cur_][k], k, reqs[k]);
+    for (int k = 0; k < n; ++k) fill(staging_[cur_][k], k, reqs[k], variant);
     check(cudaMemcpyAsync(tables_.ptr, staging_[cur_], sizeof(SlotTable) * (size_t)n, cudaMemcpyHostToDevice, s),
           "upload slot tables");
     check(cudaEventRecord(copied_[cur_], s), "record table upload");
     cur_ ^= 1;
     const TablePtr tabs{tables_.as<SlotTable>()};
-    int launches;
     if (use_graphs_ && !profiling_) {
-        const std::vector<int> key = {sh.slots, sh.max_views, sh.max_w, sh.max_h, sh.max_blocks,
-                                      sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins};
+        const std::vector<int> key = {sh.slots,  sh.variant, sh.max_views, sh.max_w,    sh.max_h,
+                                      sh.max_blocks, sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins};
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {
             cudaGraph_t g = nullptr;
@@ -293,13 +308,64 @@ int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
             it = graphs_.emplace(key, Graph{exec, nl}).first;
         }
         check(cudaGraphLaunch(it->second.exec, s), "graph launch");
-        launches = it->second.launches;
-    } else {
-        launches = launch_batch(tabs, sh, s, profiling_ ? events_ : nullptr);
-        if (launches < 0) check(cudaGetLastError(), "kernel launch");
+        return it->second.launches;
     }
+    const int launches = launch_batch(tabs, sh, s, profiling_ ? events_ : nullptr);
+    if (launches < 0) check(cudaGetLastError(), "kernel launch");
+    return launches;
+}
+
+int BatchCore::tune(const SlotRequest* reqs, int n, cudaStream_t s) {
+    const bool graphs = use_graphs_, prof = profiling_;
+    use_graphs_ = false;
+    profiling_ = false;
+    int best = 0;
+    float best_ms = 0.f;
+    for (int v = 0; v < NUM_RASTER_VARIANTS; ++v) {
+        launch_variant(reqs, n, v, s);  // warm-up (first use of the variant's module)
+        check(cudaEventRecord(tune_ev_[0], s), "record");
+        launch_variant(reqs, n, v, s);
+        check(cudaEventRecord(tune_ev_[1], s), "record");
+        check(cudaEventSynchronize(tune_ev_[1]), "synchronize");
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, tune_ev_[0], tune_ev_[1]), "elapsed");
+        if (v == 0 || ms < best_ms) {
+            best = v;
+            best_ms = ms;
+        }
+    }
+    use_graphs_ = graphs;
+    profiling_ = prof;
+    return best;
+}
+
+int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
+    if (n <= 0 || n > slots_) throw ArgError("batch of " + std::to_string(n) + " requests for " +
+                                             std::to_string(slots_) + " slots");
+    for (int k = 0; k < n; ++k) ws_[k]->ensure(ctx_, reqs[k].scene, reqs[k].virt.width, reqs[k].virt.height);
+    int variant = 0;
+    if (forced_variant_ >= 0) {
+        variant = forced_variant_;
+    } else if (autotune_) {
+        // The shape the tuner keys on: the batch size bucket and, over the
+        // batch, the largest input set and output and the projections.
+        const BatchShape sh = shape_of(reqs, n, 0);
+        int proj_in = 0, proj_out = 0;
+        for (int k = 0; k < n; ++k) {
+            proj_in |= 1 << reqs[k].scene->cams[0].projection;
+            proj_out |= 1 << reqs[k].virt.projection;
+        }
+        const int bucket = n == 1 ? 1 : n <= 4 ? 4 : n <= 16 ? 16 : 64;
+        const std::vector<int> sig = {bucket, sh.max_views, sh.max_w, sh.max_h, sh.max_wo, sh.max_ho,
+                                      proj_in, proj_out};
+        auto it = tuned_.find(sig);
+        if (it == tuned_.end()) it = tuned_.emplace(sig, tune(reqs, n, s)).first;
+        variant = it->second;
+    }
+    const int launches = launch_variant(reqs, n, variant, s);
     profiled_ = profiling_;
     last_launches_ = launches;
+    last_variant_ = variant;
     return launches;
 }
 

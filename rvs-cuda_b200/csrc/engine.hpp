@@ -107,13 +107,23 @@ public:
     int run(const SlotRequest* reqs, int n, cudaStream_t stream);
 
     void set_graphs(bool on) { use_graphs_ = on; }
+    // Time every raster variant on the first batch of each new shape and
+    // keep the fastest (all variants give identical results).
+    void set_autotune(bool on) { autotune_ = on; }
+    // Use raster variant v for every run (-1: default or tuned).
+    void force_variant(int v) { forced_variant_ = v; }
+    // Variant used by the last run, and the tuner's choices so far.
+    int last_variant() const { return last_variant_; }
     void set_profiling(bool on);
     // Milliseconds per stage of the last profiled run (stream complete).
     int stage_times(float* ms, int max_stages) const;
     int last_launches() const { return last_launches_; }
 
 private:
-    void fill(SlotTable& t, int k, const SlotRequest& r);
+    void fill(SlotTable& t, int k, const SlotRequest& r, int variant);
+    BatchShape shape_of(const SlotRequest* reqs, int n, int variant) const;
+    int launch_variant(const SlotRequest* reqs, int n, int variant, cudaStream_t s);
+    int tune(const SlotRequest* reqs, int n, cudaStream_t s);
 
     rvsb_context* ctx_;
     int slots_;
@@ -133,6 +143,11 @@ private:
     bool profiled_ = false;
     cudaEvent_t events_[2 * NUM_STAGES] = {};
     int last_launches_ = 0;
+    bool autotune_ = false;
+    int forced_variant_ = -1;
+    int last_variant_ = 0;
+    std::map<std::vector<int>, int> tuned_;
+    cudaEvent_t tune_ev_[2] = {nullptr, nullptr};
 };
 
 }  // namespace rvsb

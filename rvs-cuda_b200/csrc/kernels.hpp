@@ -11,6 +11,7 @@ namespace rvsb {
 // Grid extents of one batch launch: maxima over its slots.
 struct BatchShape {
     int slots = 0;
+    int variant = 0;         // raster variant (kRasterVariants)
     int max_views = 0;       // largest n_views
     int max_w = 0, max_h = 0;  // largest input view
     int max_blocks = 0;      // largest nbx * nby of an input view
@@ -44,6 +45,19 @@ struct TablePtr {
 constexpr int NUM_STAGES = 5;
 template <class Tabs>
 int launch_batch(const Tabs& tabs, const BatchShape& shape, cudaStream_t stream, cudaEvent_t* events = nullptr);
+
+// Raster variants the autotuner chooses from: tile width and height, views
+// per shared z-buffer group, the candidate count above which a triangle is
+// rasterised warp-cooperatively, and the bin entries staged per round.
+// Every variant gives identical results.
+struct RasterVariant {
+    int tw, th, vg, small, ent;
+};
+constexpr int NUM_RASTER_VARIANTS = 6;
+constexpr RasterVariant kRasterVariants[NUM_RASTER_VARIANTS] = {
+    {32, 32, 4, 4, 1024}, {64, 32, 2, 4, 1024}, {32, 32, 4, 2, 1024},
+    {32, 32, 4, 8, 1024}, {32, 32, 2, 4, 512},  {32, 16, 4, 4, 512},
+};
 
 // One-time kernel attributes of the current device (the raster kernel's
 // dynamic shared memory); call before launching or capturing a batch.

@@ -31,7 +31,11 @@ EXPORTED = [
     "rvsb_synthesize_batch", "rvsb_batch_last_launch_count", "rvsb_batch_set_profiling", "rvsb_batch_stage_times",
     "rvsb_server_create", "rvsb_server_add_scene", "rvsb_server_reserve", "rvsb_server_submit", "rvsb_server_poll",
     "rvsb_server_drain", "rvsb_server_clock", "rvsb_server_destroy",
+    "rvsb_batch_set_autotune", "rvsb_batch_set_raster_variant", "rvsb_batch_last_raster_variant",
+    "rvsb_scene_set_autotune",
 ]
+
+RASTER_VARIANTS = 6
 
 STAGES = ["warp", "bin", "raster", "inpaint", "total"]
 
@@ -103,6 +107,10 @@ def load():
     L.rvsb_batch_last_launch_count.argtypes = [c_p]
     L.rvsb_batch_set_profiling.argtypes = [c_p, ctypes.c_int]
     L.rvsb_batch_stage_times.argtypes = [c_p, P(ctypes.c_float), ctypes.c_int]
+    L.rvsb_batch_set_autotune.argtypes = [c_p, ctypes.c_int]
+    L.rvsb_batch_set_raster_variant.argtypes = [c_p, ctypes.c_int]
+    L.rvsb_batch_last_raster_variant.argtypes = [c_p]
+    L.rvsb_scene_set_autotune.argtypes = [c_p, ctypes.c_int]
     L.rvsb_server_create.argtypes = [c_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t, P(c_p)]
     L.rvsb_server_add_scene.argtypes = [c_p, c_p, P(ctypes.c_int)]
     L.rvsb_server_reserve.argtypes = [c_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -227,6 +235,9 @@ class Scene:
     def set_profiling(self, on=True):
         return self.ctx.check(self.ctx.lib.rvsb_scene_set_profiling(self.h, 1 if on else 0))
 
+    def set_autotune(self, on=True):
+        return self.ctx.check(self.ctx.lib.rvsb_scene_set_autotune(self.h, 1 if on else 0))
+
     def stage_times(self):
         """{stage: ms} of the last profiled synthesis (stream must be complete)."""
         buf = (ctypes.c_float * len(STAGES))()
@@ -268,6 +279,15 @@ class Batch:
 
     def set_profiling(self, on=True):
         return self.ctx.check(self.ctx.lib.rvsb_batch_set_profiling(self.h, 1 if on else 0))
+
+    def set_autotune(self, on=True):
+        return self.ctx.check(self.ctx.lib.rvsb_batch_set_autotune(self.h, 1 if on else 0))
+
+    def set_raster_variant(self, v):
+        return self.ctx.check(self.ctx.lib.rvsb_batch_set_raster_variant(self.h, int(v)))
+
+    def last_raster_variant(self):
+        return self.ctx.lib.rvsb_batch_last_raster_variant(self.h)
 
     def stage_times(self):
         buf = (ctypes.c_float * len(STAGES))()

@@ -100,3 +100,36 @@ def test_batch_1080p_matches_single(ctx):
     for c, o, e in zip(wl.targets, outs, expected):
         for x, y in zip(_yuv(o, c), e):
             np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("erp", [False, True], ids=["persp", "erp"])
+def test_every_raster_variant_identical(ctx, erp):
+    """Every raster variant the autotuner chooses from (tile sizes, view
+    groups, stretched-triangle threshold, staging depth) gives the same
+    bytes as the default path, for perspective and wrapped 360 outputs."""
+    import torch
+    wl = scenes.random_pose_small(n_views=3, w=128, h=64, seed=71, erp_in=erp, erp_out=erp)
+    sc = _upload(ctx, wl)
+    p = rvsb.params(5.0)
+    cams = _targets_small(wl)[:4]
+    expected = [_single(sc, c, p) for c in cams]
+    b = rvsb.Batch(sc, 4)
+    for v in range(rvsb.RASTER_VARIANTS):
+        b.set_raster_variant(v)
+        outs = [yuv_planes_torch(c.width, c.height) for c in cams]
+        b.synthesize(cams, p, outs)
+        torch.cuda.synchronize()
+        assert b.last_raster_variant() == v
+        for c, o, e in zip(cams, outs, expected):
+            for x, y in zip(_yuv(o, c), e):
+                np.testing.assert_array_equal(x, y)
+    b.set_raster_variant(-1)
+    b.set_autotune(True)
+    outs = [yuv_planes_torch(c.width, c.height) for c in cams]
+    b.synthesize(cams, p, outs)
+    torch.cuda.synchronize()
+    assert 0 <= b.last_raster_variant() < rvsb.RASTER_VARIANTS
+    for c, o, e in zip(cams, outs, expected):
+        for x, y in zip(_yuv(o, c), e):
+            np.testing.assert_array_equal(x, y)
+    b.close()
