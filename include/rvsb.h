@@ -178,6 +178,19 @@ const char* rvsb_config_output_path(const rvsb_config* cfg, int i);
 void rvsb_config_frames(const rvsb_config* cfg, int* start_frame, int* number_of_frames,
                         int* number_of_output_frames);
 void rvsb_config_synth_params(const rvsb_config* cfg, rvsb_synth_params* out);
+/* Output file i of one kind (NULL when the configuration has none):
+ * OutputFiles, MaskedOutputFiles, OutputMasks, DepthOutputFiles,
+ * MaskedDepthOutputFiles (Config.cpp:88-98). */
+typedef enum rvsb_output_kind {
+    RVSB_OUT_COLOR = 0,
+    RVSB_OUT_MASKED_COLOR = 1,
+    RVSB_OUT_MASK = 2,
+    RVSB_OUT_DEPTH = 3,
+    RVSB_OUT_MASKED_DEPTH = 4
+} rvsb_output_kind;
+const char* rvsb_config_output_file(const rvsb_config* cfg, int kind, int i);
+/* "ValidityThreshold" (default 5000, Config.hpp:157). */
+float rvsb_config_validity_threshold(const rvsb_config* cfg);
 /* Virtual camera i for output frame `frame` after applying the pose trace
  * the way Pipeline::computeView does (rvs/src/Pipeline.cpp:173-181:
  * position += trace position, rotation = trace rotation). */
@@ -271,6 +284,35 @@ typedef struct rvsb_debug_out {
 rvsb_status rvsb_synthesize_debug(rvsb_scene* scene, const rvsb_camera* virt,
                                   const rvsb_synth_params* params, const rvsb_yuv420* out,
                                   const rvsb_debug_out* dbg, void* stream);
+
+/* Auxiliary outputs of one synthesis: the extra files the reference writes
+ * in CPU mode (Pipeline.cpp:303-336; its CUDA mode skips them).  Device
+ * pointers; any may be NULL.
+ *   mask:          width*height bytes, 255 where the blended validity (the
+ *                  maximum over the views of the winning triangle's quality)
+ *                  is not above validity_threshold, else 0
+ *                  (View::get_validity_mask, View.cpp:206-211; OutputMasks)
+ *   masked:        YUV420 of the inpainted colour with masked pixels set to
+ *                  0.5 (MaskedOutputFiles)
+ *   depth:         width*height samples of the blended depth (the first
+ *                  view's depth, replaced by a later view's where its quality
+ *                  is larger, BlendedView.cpp:205-208) encoded as normalised
+ *                  disparity with the virtual camera's Depth_range and
+ *                  BitDepthDepth (write_depth, image_writing.cpp:232-268;
+ *                  DepthOutputFiles)
+ *   masked_depth:  the same, 0 where masked (MaskedDepthOutputFiles) */
+typedef struct rvsb_aux_out {
+    uint8_t* mask;
+    rvsb_yuv420 masked;
+    uint16_t* depth;
+    uint16_t* masked_depth;
+    float validity_threshold;  /* "ValidityThreshold" (default 5000) */
+    int32_t reserved;
+} rvsb_aux_out;
+
+/* rvsb_synthesize plus the auxiliary outputs. */
+rvsb_status rvsb_synthesize_aux(rvsb_scene* scene, const rvsb_camera* virt, const rvsb_synth_params* params,
+                                const rvsb_yuv420* out, const rvsb_aux_out* aux, void* stream);
 
 /* Kernel launches issued by the most recent synthesis call of the scene
  * (for launch accounting). */

@@ -54,6 +54,9 @@ def lib():
         L.orc_write_yuv420.argtypes = [_F, ctypes.c_int, ctypes.c_int, ctypes.c_int, _U16]
         L.orc_synthesize.argtypes = [ctypes.c_int, P, ctypes.POINTER(abi.ViewPlanes), P, ctypes.c_float,
                                      _U16, _F, _F]
+        L.orc_synthesize_aux.argtypes = [ctypes.c_int, P, ctypes.POINTER(abi.ViewPlanes), P, ctypes.c_float,
+                                         _U16, _F, _F, ctypes.c_float, ctypes.POINTER(ctypes.c_uint8), _U16,
+                                         _U16, _U16]
         L.orc_image_pos.argtypes = [P, _F]
         L.orc_unproject.argtypes = [P, _F, _F, _F]
         L.orc_project.argtypes = [P, _F, _F, _F, ctypes.POINTER(ctypes.c_int)]
@@ -203,6 +206,31 @@ def synthesize(inputs, planes, virt, exponent, want_intermediate=False):
     if want_intermediate:
         return yuv, q, c
     return yuv
+
+
+def synthesize_aux(inputs, planes, virt, exponent, threshold=5000.0):
+    """Synthesis with the auxiliary outputs of Pipeline.cpp:303-336.  Returns
+    a dict: yuv, mask (uint8), masked_yuv, depth and masked_depth (uint16)."""
+    n = len(inputs)
+    cams = (abi.Camera * n)(*inputs)
+    keep = []
+    vp = (abi.ViewPlanes * n)()
+    for i, (y, u, v, d) in enumerate(planes):
+        arrs = [np.ascontiguousarray(a, np.uint16) for a in (y, u, v, d)]
+        keep.append(arrs)
+        vp[i].y, vp[i].u, vp[i].v, vp[i].depth = (a.ctypes.data for a in arrs)
+    wo, ho = virt.width, virt.height
+    out = np.empty(wo * ho * 3 // 2, np.uint16)
+    masked = np.empty(wo * ho * 3 // 2, np.uint16)
+    mask = np.empty((ho, wo), np.uint8)
+    depth = np.empty((ho, wo), np.uint16)
+    mdepth = np.empty((ho, wo), np.uint16)
+    rc = lib().orc_synthesize_aux(n, cams, vp, ctypes.byref(virt), float(exponent), _p(out, _U16), None, None,
+                                  float(threshold), mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                  _p(masked, _U16), _p(depth, _U16), _p(mdepth, _U16))
+    assert rc == 0, rc
+    return {"yuv": split_yuv420(out, wo, ho), "mask": mask, "masked_yuv": split_yuv420(masked, wo, ho),
+            "depth": depth, "masked_depth": mdepth}
 
 
 def image_pos(cam):

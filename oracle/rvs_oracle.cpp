@@ -537,6 +537,68 @@ int orc_raster(const float* color, const float* vdepth, const float* uv, int w, 
  * the first is assigned as is, every later one is blended into the
  * accumulator.  color_i: Ho*Wo*3, quality_i = validity_i / depth_i and
  * depth_i: Ho*Wo.  Outputs the blended colour and quality. */
+}  // extern "C"
+
+/* One step of the incremental blend: view v (colour, quality, depth) into
+ * the accumulator (colour, quality, depth-prolongation mask). */
+static void blend_step(int v, const float* vcol, const float* vq, const float* vd, size_t no, float exponent,
+                       float* out_color, float* out_quality, uint8_t* acc_mask) {
+    if (v == 0) {
+        std::memcpy(out_color, vcol, no * 3 * sizeof(float));
+        std::memcpy(out_quality, vq, no * sizeof(float));
+        for (size_t p = 0; p < no; ++p) acc_mask[p] = vd[p] > 0.f;
+        return;
+    }
+    const float empty[3] = {0.f, 1.f, 0.f};
+    for (size_t p = 0; p < no; ++p) {
+        const float* cols[2] = {out_color + p * 3, vcol + p * 3};
+        float quals[2] = {out_quality[p], vq[p]};
+        bool prolong[2] = {acc_mask[p] != 0, vd[p] > 0.f};
+        float sumWeights = 0.0f;
+        float finalColor[3] = {0, 0, 0};
+        float inpaintedDepthColor[3] = {0, 0, 0};
+        float inpaintedDepthSumWeights = 0.0f;
+        for (int i = 0; i < 2; ++i) {
+            float quality = quals[i];
+            bool isValidDepth = quals[i] > 0 && !prolong[i];
+            if (quality > 0 && isValidDepth) {
+                quality = powf(quality, exponent);
+                sumWeights += quality;
+                for (int k = 0; k < 3; ++k) finalColor[k] += quality * cols[i][k];
+            } else if (quality > 0 && quals[i] > 0) {
+                quality = powf(quality, exponent);
+                inpaintedDepthSumWeights += quality;
+                for (int k = 0; k < 3; ++k) inpaintedDepthColor[k] += quality * cols[i][k];
+            }
+        }
+        float outc[3];
+        float outq;
+        bool outprol;
+        if (sumWeights == 0) {
+            if (inpaintedDepthSumWeights == 0.0) {
+                for (int k = 0; k < 3; ++k) outc[k] = empty[k];
+                outprol = true;
+                outq = 0.0f;
+            } else {
+                float inv = 1.f / inpaintedDepthSumWeights;
+                for (int k = 0; k < 3; ++k) outc[k] = inpaintedDepthColor[k] * inv;
+                outprol = true;
+                outq = powf(inpaintedDepthSumWeights, 1.0f / exponent);
+            }
+        } else {
+            float inv = 1.f / sumWeights;
+            for (int k = 0; k < 3; ++k) outc[k] = finalColor[k] * inv;
+            outprol = false;
+            outq = powf(sumWeights, 1.0f / exponent);
+        }
+        for (int k = 0; k < 3; ++k) out_color[p * 3 + k] = outc[k];
+        out_quality[p] = outq;
+        acc_mask[p] = outprol;
+    }
+}
+
+extern "C" {
+
 int orc_blend(int n, const float* const* colors, const float* const* qualities,
               const float* const* depths, int wo, int ho, float exponent, float* out_color,
               float* out_quality) {
@@ -544,57 +606,8 @@ int orc_blend(int n, const float* const* colors, const float* const* qualities,
     if (exponent < 0) return RVSB_E_UNSUPPORTED;  // blend_img_by_max
     const size_t no = (size_t)wo * ho;
     std::vector<uint8_t> acc_mask(no);  // m_depth_mask
-    std::memcpy(out_color, colors[0], no * 3 * sizeof(float));
-    std::memcpy(out_quality, qualities[0], no * sizeof(float));
-    for (size_t p = 0; p < no; ++p) acc_mask[p] = depths[0][p] > 0.f;
-    const float empty[3] = {0.f, 1.f, 0.f};
-    for (int v = 1; v < n; ++v) {
-        for (size_t p = 0; p < no; ++p) {
-            const float* cols[2] = {out_color + p * 3, colors[v] + p * 3};
-            float quals[2] = {out_quality[p], qualities[v][p]};
-            bool prolong[2] = {acc_mask[p] != 0, depths[v][p] > 0.f};
-            float sumWeights = 0.0f;
-            float finalColor[3] = {0, 0, 0};
-            float inpaintedDepthColor[3] = {0, 0, 0};
-            float inpaintedDepthSumWeights = 0.0f;
-            for (int i = 0; i < 2; ++i) {
-                float quality = quals[i];
-                bool isValidDepth = quals[i] > 0 && !prolong[i];
-                if (quality > 0 && isValidDepth) {
-                    quality = powf(quality, exponent);
-                    sumWeights += quality;
-                    for (int k = 0; k < 3; ++k) finalColor[k] += quality * cols[i][k];
-                } else if (quality > 0 && quals[i] > 0) {
-                    quality = powf(quality, exponent);
-                    inpaintedDepthSumWeights += quality;
-                    for (int k = 0; k < 3; ++k) inpaintedDepthColor[k] += quality * cols[i][k];
-                }
-            }
-            float outc[3];
-            float outq;
-            bool outprol;
-            if (sumWeights == 0) {
-                if (inpaintedDepthSumWeights == 0.0) {
-                    for (int k = 0; k < 3; ++k) outc[k] = empty[k];
-                    outprol = true;
-                    outq = 0.0f;
-                } else {
-                    float inv = 1.f / inpaintedDepthSumWeights;
-                    for (int k = 0; k < 3; ++k) outc[k] = inpaintedDepthColor[k] * inv;
-                    outprol = true;
-                    outq = powf(inpaintedDepthSumWeights, 1.0f / exponent);
-                }
-            } else {
-                float inv = 1.f / sumWeights;
-                for (int k = 0; k < 3; ++k) outc[k] = finalColor[k] * inv;
-                outprol = false;
-                outq = powf(sumWeights, 1.0f / exponent);
-            }
-            for (int k = 0; k < 3; ++k) out_color[p * 3 + k] = outc[k];
-            out_quality[p] = outq;
-            acc_mask[p] = outprol;
-        }
-    }
+    for (int v = 0; v < n; ++v)
+        blend_step(v, colors[v], qualities[v], depths[v], no, exponent, out_color, out_quality, acc_mask.data());
     return RVSB_OK;
 }
 
@@ -700,20 +713,63 @@ int orc_write_yuv420(const float* color, int w, int h, int bits, uint16_t* out) 
     return RVSB_OK;
 }
 
+/* Depth of the blended view (BlendedView.cpp:205-208): the first view's
+ * depth, then at every later view the view's depth where its quality is
+ * larger than the accumulator's quality before the blend; validity is the
+ * running maximum (cv::max).  acc_q_before: the accumulator's quality
+ * before view v (view 0: unused). */
+static void blend_depth_validity(int v, const float* acc_q_before, const float* vq, const float* vd,
+                                 const float* vv, size_t no, float* depth, float* validity) {
+    for (size_t p = 0; p < no; ++p) {
+        if (v == 0) {
+            depth[p] = vd[p];
+            validity[p] = vv[p];
+        } else {
+            if (vq[p] > acc_q_before[p]) depth[p] = vd[p];
+            validity[p] = std::max(validity[p], vv[p]);
+        }
+    }
+}
+
+/* write_maskedDepth (image_writing.cpp:237-268) for integer bit depths:
+ * normalised disparity near / depth (far >= 1000) or
+ * (far * near / depth - near) / (far - near), masked pixels set to 0, then
+ * convertTo(CV_16U, 2^bits - 1): rounded to nearest (ties to even) and
+ * saturated, NaN to 0. */
+static uint16_t encode_depth(float depth, const rvsb_camera* vt, bool masked) {
+    const float near_ = vt->depth_range[0], far_ = vt->depth_range[1];
+    float d;
+    if (far_ >= 1000.f)
+        d = near_ / depth;
+    else
+        d = ((far_ * near_) / depth - near_) / (far_ - near_);
+    if (masked) d = 0.f;
+    const float v = d * (float)max_level(vt->bit_depth_depth);
+    if (std::isnan(v)) return 0;
+    const float r = std::nearbyint(v);
+    return (uint16_t)std::min(65535.f, std::max(0.f, r));
+}
+
 /* One output frame of Pipeline::computeView in CPU mode
- * (Pipeline.cpp:169-285): for every input view in order, load, warp,
+ * (Pipeline.cpp:169-336): for every input view in order, load, warp,
  * raster (SynthetisedViewTriangle::transform, SynthesizedView.cpp:428-441:
  * quality = validity / depth) and blend; then inpaint and write.
  * planes: n entries of {y, u, v, depth} host pointers.  Optional outputs:
  * out_quality (blended quality, Ho*Wo), out_color (blended colour before
- * inpainting, Ho*Wo*3). */
-int orc_synthesize(int n, const rvsb_camera* cams, const rvsb_view_planes* planes,
-                   const rvsb_camera* vt, float exponent, uint16_t* out_yuv, float* out_quality,
-                   float* out_color) {
+ * inpainting, Ho*Wo*3).  orc_synthesize_aux adds the outputs of
+ * Pipeline.cpp:303-336 (all optional): the validity mask (Ho*Wo bytes, 255
+ * where the blended validity is not above `threshold`), the masked colour
+ * (YUV420 of the inpainted colour with masked pixels set to 0.5), the
+ * blended depth and the masked depth (Ho*Wo uint16 each, encoded with the
+ * virtual camera's depth range and bit depth). */
+int orc_synthesize_aux(int n, const rvsb_camera* cams, const rvsb_view_planes* planes,
+                       const rvsb_camera* vt, float exponent, uint16_t* out_yuv, float* out_quality,
+                       float* out_color, float threshold, uint8_t* out_mask, uint16_t* out_masked_yuv,
+                       uint16_t* out_depth, uint16_t* out_masked_depth) {
     if (n <= 0 || !cams || !planes || !vt || !out_yuv) return RVSB_E_ARG;
     const int wo = vt->width, ho = vt->height;
     const size_t no = (size_t)wo * ho;
-    std::vector<std::vector<float>> vcol(n), vq(n), vd(n);
+    std::vector<std::vector<float>> vcol(n), vq(n), vd(n), vv(n);
     for (int v = 0; v < n; ++v) {
         const rvsb_camera& c = cams[v];
         const size_t ni = (size_t)c.width * c.height;
@@ -729,25 +785,54 @@ int orc_synthesize(int n, const rvsb_camera* cams, const rvsb_view_planes* plane
         vcol[v].resize(no * 3);
         vd[v].resize(no);
         vq[v].resize(no);
-        std::vector<float> validity(no);
+        vv[v].resize(no);
         orc_raster(col.data(), vdep.data(), uv.data(), c.width, c.height, wo, ho, wrap,
-                   vcol[v].data(), vd[v].data(), validity.data());
-        for (size_t p = 0; p < no; ++p) vq[v][p] = validity[p] / vd[v][p];
+                   vcol[v].data(), vd[v].data(), vv[v].data());
+        for (size_t p = 0; p < no; ++p) vq[v][p] = vv[v][p] / vd[v][p];
     }
-    std::vector<const float*> pc(n), pq(n), pd(n);
+    // Blend view by view; the accumulator's quality before each view feeds
+    // the depth rule.
+    if (exponent < 0) return RVSB_E_UNSUPPORTED;  // blend_img_by_max
+    std::vector<float> bc(no * 3), bq(no), prev_q(no), depth(no), validity(no);
+    std::vector<uint8_t> acc_mask(no);
+    const bool want_aux = out_mask || out_masked_yuv || out_depth || out_masked_depth;
     for (int v = 0; v < n; ++v) {
-        pc[v] = vcol[v].data();
-        pq[v] = vq[v].data();
-        pd[v] = vd[v].data();
+        if (want_aux) prev_q = bq;
+        blend_step(v, vcol[v].data(), vq[v].data(), vd[v].data(), no, exponent, bc.data(), bq.data(),
+                   acc_mask.data());
+        if (want_aux)
+            blend_depth_validity(v, prev_q.data(), vq[v].data(), vd[v].data(), vv[v].data(), no, depth.data(),
+                                 validity.data());
     }
-    std::vector<float> bc(no * 3), bq(no);
-    int rc = orc_blend(n, pc.data(), pq.data(), pd.data(), wo, ho, exponent, bc.data(), bq.data());
-    if (rc) return rc;
     if (out_quality) std::memcpy(out_quality, bq.data(), no * sizeof(float));
     if (out_color) std::memcpy(out_color, bc.data(), no * 3 * sizeof(float));
     std::vector<float> filled(no * 3);
     orc_inpaint(bc.data(), bq.data(), wo, ho, filled.data(), nullptr, nullptr);
-    return orc_write_yuv420(filled.data(), wo, ho, vt->bit_depth_color, out_yuv);
+    int rc = orc_write_yuv420(filled.data(), wo, ho, vt->bit_depth_color, out_yuv);
+    if (rc) return rc;
+    std::vector<uint8_t> mask(no);
+    for (size_t p = 0; p < no; ++p) mask[p] = (validity[p] > threshold) ? 0 : 255;
+    if (out_mask) std::memcpy(out_mask, mask.data(), no);
+    if (out_masked_yuv) {
+        std::vector<float> masked = filled;
+        for (size_t p = 0; p < no; ++p)
+            if (mask[p])
+                for (int k = 0; k < 3; ++k) masked[p * 3 + k] = 0.5f;
+        rc = orc_write_yuv420(masked.data(), wo, ho, vt->bit_depth_color, out_masked_yuv);
+        if (rc) return rc;
+    }
+    if (out_depth)
+        for (size_t p = 0; p < no; ++p) out_depth[p] = encode_depth(depth[p], vt, false);
+    if (out_masked_depth)
+        for (size_t p = 0; p < no; ++p) out_masked_depth[p] = encode_depth(depth[p], vt, mask[p] != 0);
+    return RVSB_OK;
+}
+
+int orc_synthesize(int n, const rvsb_camera* cams, const rvsb_view_planes* planes,
+                   const rvsb_camera* vt, float exponent, uint16_t* out_yuv, float* out_quality,
+                   float* out_color) {
+    return orc_synthesize_aux(n, cams, planes, vt, exponent, out_yuv, out_quality, out_color, 0.f, nullptr,
+                              nullptr, nullptr, nullptr);
 }
 
 }  // extern "C"

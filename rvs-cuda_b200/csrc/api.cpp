@@ -84,7 +84,7 @@ BatchCore& single_core(rvsb_scene* sc) {
 // their colour is decoded into the scene and their depth read in place.
 rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_synth_params* params,
                             const rvsb_yuv420* out, const rvsb_debug_out* dbg_out, void* stream,
-                            const rvsb_view_planes* frame = nullptr) {
+                            const rvsb_view_planes* frame = nullptr, const rvsb_aux_out* aux = nullptr) {
     if (!sc) return RVSB_E_ARG;
     rvsb_context* ctx = sc->ctx;
     return guarded(ctx, [&]() -> rvsb_status {
@@ -115,6 +115,12 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
         r.params = *params;
         r.out = *out;
         r.frame = frame;
+        if (aux) {
+            if (aux->masked.y || aux->masked.u || aux->masked.v)
+                if (!aux->masked.y || !aux->masked.u || !aux->masked.v)
+                    throw ArgError("masked colour needs all three planes");
+            if (aux->mask || aux->masked.y || aux->depth || aux->masked_depth) r.aux = aux;
+        }
         if (dbg_out) {
             r.dbg.warped_uvz = dbg_out->warped_uvz;
             r.dbg.view_color = dbg_out->view_color;
@@ -274,6 +280,11 @@ rvsb_status rvsb_scene_upload(rvsb_scene* sc, int view, const rvsb_view_planes* 
 rvsb_status rvsb_synthesize(rvsb_scene* scene, const rvsb_camera* virt, const rvsb_synth_params* params,
                             const rvsb_yuv420* out, void* stream) {
     return synthesize_impl(scene, virt, params, out, nullptr, stream);
+}
+
+rvsb_status rvsb_synthesize_aux(rvsb_scene* scene, const rvsb_camera* virt, const rvsb_synth_params* params,
+                                const rvsb_yuv420* out, const rvsb_aux_out* aux, void* stream) {
+    return synthesize_impl(scene, virt, params, out, nullptr, stream, nullptr, aux);
 }
 
 rvsb_status rvsb_synthesize_debug(rvsb_scene* scene, const rvsb_camera* virt, const rvsb_synth_params* params,
@@ -546,6 +557,22 @@ void rvsb_config_frames(const rvsb_config* c, int* start, int* n, int* nout) {
     if (n) *n = c->cfg.number_of_frames;
     if (nout) *nout = c->cfg.number_of_output_frames;
 }
+
+const char* rvsb_config_output_file(const rvsb_config* c, int kind, int i) {
+    if (!c) return nullptr;
+    const std::vector<std::string>* v = nullptr;
+    switch (kind) {
+        case RVSB_OUT_COLOR: v = &c->cfg.outfilenames; break;
+        case RVSB_OUT_MASKED_COLOR: v = &c->cfg.outmaskedfilenames; break;
+        case RVSB_OUT_MASK: v = &c->cfg.outmaskfilenames; break;
+        case RVSB_OUT_DEPTH: v = &c->cfg.outdepthfilenames; break;
+        case RVSB_OUT_MASKED_DEPTH: v = &c->cfg.outmaskdepthfilenames; break;
+        default: return nullptr;
+    }
+    return (i >= 0 && i < (int)v->size()) ? (*v)[i].c_str() : nullptr;
+}
+
+float rvsb_config_validity_threshold(const rvsb_config* c) { return c ? c->cfg.validity_threshold : 5000.f; }
 
 void rvsb_config_synth_params(const rvsb_config* c, rvsb_synth_params* out) {
     if (!c || !out) return;

@@ -88,6 +88,25 @@ struct DebugPtrs {
     }
 };
 
+// Auxiliary outputs of a synthesis (Pipeline.cpp:303-336, CPU mode): any
+// pointer may be null.  acc_depth / acc_valid are the slot's per-pixel
+// blended depth and validity (workspace buffers, set when any output is on).
+struct AuxPtrs {
+    uint8_t* mask;            // 255 where the blended validity is not above threshold
+    uint16_t* masked_y;       // YUV420 colour with masked pixels set to 0.5
+    uint16_t* masked_u;
+    uint16_t* masked_v;
+    uint16_t* depth;          // encoded blended depth
+    uint16_t* masked_depth;   // the same, 0 where masked
+    float* acc_depth;
+    float* acc_valid;
+    float threshold;          // "ValidityThreshold"
+    int on;                   // any output requested
+    float depth_near, depth_far;  // virtual camera's depth range
+    unsigned depth_max;       // 2^BitDepthDepth - 1
+    int pad;
+};
+
 // Device buffers of one slot's workspace.
 struct SlotBuffers {
     DevStatus* status;   // 1 entry
@@ -113,6 +132,7 @@ struct SlotTable {
     uint16_t* out_u;
     uint16_t* out_v;
     DebugPtrs dbg;
+    AuxPtrs aux;
     DevView v[MAX_VIEWS];
 };
 

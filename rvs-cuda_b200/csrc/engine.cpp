@@ -103,6 +103,15 @@ void SlotWorkspace::ensure(rvsb_context* ctx, const rvsb_scene* sc, int wo, int 
     }
 }
 
+void SlotWorkspace::ensure_aux(rvsb_context* ctx, int wo, int ho) {
+    const size_t n = (size_t)wo * ho;
+    if (n > cap_aux) {
+        aux_depth.alloc(ctx, n * sizeof(float));
+        aux_valid.alloc(ctx, n * sizeof(float));
+        cap_aux = n;
+    }
+}
+
 BatchCore::BatchCore(rvsb_context* ctx, int slots) : ctx_(ctx), slots_(slots) {
     if (slots <= 0) throw ArgError("a batch needs at least one slot");
     prepare_kernels();
@@ -246,6 +255,22 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
     T.out_u = r.out.u;
     T.out_v = r.out.v;
     T.dbg = r.dbg;
+    if (r.aux) {
+        AuxPtrs& A = T.aux;
+        A.mask = r.aux->mask;
+        A.masked_y = r.aux->masked.y;
+        A.masked_u = r.aux->masked.u;
+        A.masked_v = r.aux->masked.v;
+        A.depth = r.aux->depth;
+        A.masked_depth = r.aux->masked_depth;
+        A.acc_depth = ws.aux_depth.as<float>();
+        A.acc_valid = ws.aux_valid.as<float>();
+        A.threshold = r.aux->validity_threshold;
+        A.on = 1;
+        A.depth_near = virt.depth_range[0];
+        A.depth_far = virt.depth_range[1];
+        A.depth_max = (1u << virt.bit_depth_depth) - 1u;
+    }
 }
 
 BatchShape BatchCore::shape_of(const SlotRequest* reqs, int n, int variant) const {
@@ -253,6 +278,8 @@ BatchShape BatchCore::shape_of(const SlotRequest* reqs, int n, int variant) cons
     BatchShape sh;
     sh.slots = n;
     sh.variant = variant;
+    for (int k = 0; k < n; ++k)
+        if (reqs[k].aux) sh.aux = 1;
     for (int k = 0; k < n; ++k) {
         const SlotRequest& r = reqs[k];
         const int nv = (int)r.scene->cams.size();
@@ -292,7 +319,7 @@ int BatchCore::launch_variant(const SlotRequest* reqs, int n, int variant, cudaS
     const TablePtr tabs{tables_.as<SlotTable>()};
     if (use_graphs_ && !profiling_) {
         const std::vector<int> key = {sh.slots,  sh.variant, sh.max_views, sh.max_w,    sh.max_h,
-                                      sh.max_blocks, sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins};
+                                      sh.max_blocks, sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins, sh.aux};
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {
             cudaGraph_t g = nullptr;
@@ -342,7 +369,10 @@ int BatchCore::tune(const SlotRequest* reqs, int n, cudaStream_t s) {
 int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
     if (n <= 0 || n > slots_) throw ArgError("batch of " + std::to_string(n) + " requests for " +
                                              std::to_string(slots_) + " slots");
-    for (int k = 0; k < n; ++k) ws_[k]->ensure(ctx_, reqs[k].scene, reqs[k].virt.width, reqs[k].virt.height);
+    for (int k = 0; k < n; ++k) {
+        ws_[k]->ensure(ctx_, reqs[k].scene, reqs[k].virt.width, reqs[k].virt.height);
+        if (reqs[k].aux) ws_[k]->ensure_aux(ctx_, reqs[k].virt.width, reqs[k].virt.height);
+    }
     int variant = 0;
     if (forced_variant_ >= 0) {
         variant = forced_variant_;

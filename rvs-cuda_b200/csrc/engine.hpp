@@ -68,7 +68,9 @@ struct DevMem {
 // and the output-sized codes, hole mask and inpainting scratch.
 struct SlotWorkspace {
     DevMem status, counts, offsets, cursor, list, codes, holes, scan[4], vert, bbox;
-    size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0;
+    DevMem aux_depth, aux_valid;  // blended depth / validity (auxiliary outputs only)
+    size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0, cap_aux = 0;
+    void ensure_aux(rvsb_context* ctx, int wo, int ho);
 
     // Bytes a slot needs for `scene` at output size wo x ho.
     static size_t bytes_for(const rvsb_scene* scene, int wo, int ho);
@@ -87,6 +89,7 @@ struct SlotRequest {
     rvsb_yuv420 out{};
     DebugPtrs dbg{};
     const rvsb_view_planes* frame = nullptr;  // optional raw device planes (depth read in place)
+    const rvsb_aux_out* aux = nullptr;        // optional auxiliary outputs
 };
 
 // Slot tables in device memory, their pinned host staging, and the launch

@@ -12,6 +12,7 @@ namespace rvsb {
 struct BatchShape {
     int slots = 0;
     int variant = 0;         // raster variant (kRasterVariants)
+    int aux = 0;             // some slot wants auxiliary outputs
     int max_views = 0;       // largest n_views
     int max_w = 0, max_h = 0;  // largest input view
     int max_blocks = 0;      // largest nbx * nby of an input view

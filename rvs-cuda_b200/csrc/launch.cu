@@ -15,6 +15,8 @@ template <class Tabs>
 void launch_raster(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 template <class Tabs>
 void launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
+template <class Tabs>
+void launch_aux(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 
 namespace {
 
@@ -59,10 +61,11 @@ int launch_batch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s, cudaEve
     mark(5);
     mark(6);
     launch_inpaint(tabs, sh, s);
+    if (sh.aux) launch_aux(tabs, sh, s);
     mark(7);
     mark(9);
     if (cudaPeekAtLastError() != cudaSuccess) return -1;
-    return 1 + 1 + 3 + 1 + 6;
+    return 1 + 1 + 3 + 1 + 6 + (sh.aux ? 1 : 0);
 }
 
 template int launch_batch<TableParam>(const TableParam&, const BatchShape&, cudaStream_t, cudaEvent_t*);

@@ -233,10 +233,30 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
         if (g0 > 0) {
             a.c0 = acc[0][p]; a.c1 = acc[1][p]; a.c2 = acc[2][p]; a.q = acc[3][p];
         }
+        const bool aux = tab.aux.on != 0;
+        const size_t po = (size_t)y * T.wo + x;
+        float adepth = 0.f, avalid = 0.f;
+        if (aux && g0 > 0) {
+            adepth = tab.aux.acc_depth[po];
+            avalid = tab.aux.acc_valid[po];
+        }
         for (int k = 0; k < gn; ++k) {
             const int v = g0 + k;
             const Fragment f = resolve_fragment(tab.v[v], zb[k][p], x, y);
             const float qv = __fdiv_rn(f.validity, f.depth);
+            if (aux) {
+                // BlendedView.cpp:205-208: the view's depth where its quality
+                // beats the accumulator's before this blend (view 0: its
+                // quality; later: (weight sum)^(1/exp)); validity = max.
+                if (v == 0) {
+                    adepth = f.depth;
+                    avalid = f.validity;
+                } else {
+                    const float qacc = v == 1 ? a.q : (a.q > 0.f ? powf(a.q, T.inv_blend_exp) : a.q);
+                    if (qv > qacc) adepth = f.depth;
+                    avalid = smax(avalid, f.validity);
+                }
+            }
             if (dbg.view_color || dbg.view_depth || dbg.view_validity) {
                 const size_t o = (size_t)y * T.wo + x;
                 if (dbg.view_color) {
@@ -249,6 +269,10 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
             blend_view(a, v, f, qv, T);
         }
         acc[0][p] = a.c0; acc[1][p] = a.c1; acc[2][p] = a.c2; acc[3][p] = a.q;
+        if (aux) {
+            tab.aux.acc_depth[po] = adepth;
+            tab.aux.acc_valid[po] = avalid;
+        }
     }
 }
 

@@ -6,10 +6,20 @@
 // 157-298): output frame f uses input frame start_frame + f, mapped into the
 // input files with the ping-pong rule of getExtendedIndex, the pose trace
 // entry of that input frame, and appends its YUV420 planes to each output
-// file (truncating on frame 0, image_writing.cpp:72-76).
+// file (truncating on frame 0, image_writing.cpp:72-76).  Like the
+// reference's asynchronous loader and writer (Pipeline.cpp:226-245), the
+// next frame's input files are read while the current frame is synthesised
+// and the previous frame's outputs are written meanwhile.  Besides
+// OutputFiles, the CPU-mode outputs MaskedOutputFiles, OutputMasks,
+// DepthOutputFiles and MaskedDepthOutputFiles are written when configured
+// (Pipeline.cpp:303-336).
+#include <cuda_runtime.h>
+
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <string>
 #include <vector>
 
@@ -44,6 +54,29 @@ bool read_at(const char* path, long offset_per_frame, int frame, std::vector<uin
     }
     std::fclose(f);
     return true;
+}
+
+// Host planes of one input frame (all views).
+struct InputFrame {
+    std::vector<std::vector<uint16_t>> bufs;  // 4 per view: y, u, v, depth
+};
+
+// Host copies of one frame's outputs and the files they go to.
+struct OutputFrame {
+    std::vector<uint16_t> yuv, masked, depth, masked_depth;
+    std::vector<uint8_t> mask;
+};
+
+bool append(const char* path, bool first, const void* data, size_t bytes, std::string& err) {
+    FILE* f = std::fopen(path, first ? "wb" : "ab");
+    if (!f) {
+        err = "Failed to open YUV output image";
+        return false;
+    }
+    const bool ok = std::fwrite(data, 1, bytes, f) == bytes;
+    std::fclose(f);
+    if (!ok) err = std::string("Failed to write \"") + path + "\"";
+    return ok;
 }
 
 }  // namespace
@@ -96,79 +129,169 @@ int main(int argc, char** argv) {
     params.chroma_rounding = chroma_rounding;
     std::vector<rvsb_camera> cams(n_in);
     for (int i = 0; i < n_in; ++i) rvsb_config_input_camera(cfg, i, &cams[i]);
+    const char* files[5];
+    for (int k = 0; k < 5; ++k) files[k] = rvsb_config_output_file(cfg, k, 0);
 
     rvsb_context* ctx = nullptr;
     if (rvsb_create(0, 0, &ctx) != RVSB_OK) {
         std::fprintf(stderr, "failed to create a CUDA context on device 0\n");
         return 1;
     }
-    std::vector<std::vector<uint16_t>> bufs(n_in * 4);
-    std::vector<rvsb_view_planes> planes(n_in);
+    rvsb_scene* scene = nullptr;
+    if ((st = rvsb_scene_create(ctx, cams.data(), n_in, &scene)) != RVSB_OK) {
+        std::fprintf(stderr, "%s\n", rvsb_last_error(ctx));
+        return 1;
+    }
+    rvsb_camera virt0;
+    rvsb_config_virtual_camera(cfg, 0, &virt0);
+    const size_t ny = (size_t)virt0.width * virt0.height, nc = (size_t)(virt0.width / 2) * (virt0.height / 2);
+    // Device outputs.
+    uint16_t *d_yuv = nullptr, *d_masked = nullptr, *d_depth = nullptr, *d_mdepth = nullptr;
+    uint8_t* d_mask = nullptr;
+    cudaMalloc(&d_yuv, (ny + 2 * nc) * 2);
+    if (files[RVSB_OUT_MASKED_COLOR]) cudaMalloc(&d_masked, (ny + 2 * nc) * 2);
+    if (files[RVSB_OUT_MASK]) cudaMalloc(&d_mask, ny);
+    if (files[RVSB_OUT_DEPTH]) cudaMalloc(&d_depth, ny * 2);
+    if (files[RVSB_OUT_MASKED_DEPTH]) cudaMalloc(&d_mdepth, ny * 2);
+    rvsb_yuv420 out{d_yuv, d_yuv + ny, d_yuv + ny + nc};
+    rvsb_aux_out aux{};
+    aux.mask = d_mask;
+    if (d_masked) aux.masked = rvsb_yuv420{d_masked, d_masked + ny, d_masked + ny + nc};
+    aux.depth = d_depth;
+    aux.masked_depth = d_mdepth;
+    aux.validity_threshold = rvsb_config_validity_threshold(cfg);
+
+    auto load = [&](int vf, InputFrame& fr, std::string& e) -> bool {
+        const int frame = extended_index(start + vf, n_frames);
+        fr.bufs.resize(n_in * 4);
+        for (int i = 0; i < n_in; ++i) {
+            const rvsb_camera& c = cams[i];
+            const size_t cy = (size_t)c.width * c.height, cc = (size_t)(c.width / 2) * (c.height / 2);
+            fr.bufs[i * 4 + 0].resize(cy);
+            fr.bufs[i * 4 + 1].resize(cc);
+            fr.bufs[i * 4 + 2].resize(cc);
+            fr.bufs[i * 4 + 3].resize(cy);
+            const long color_frame = (long)(cy * 2 * 3 / 2);
+            if (!read_at(rvsb_config_texture_path(cfg, i), color_frame, frame,
+                         {fr.bufs[i * 4].data(), fr.bufs[i * 4 + 1].data(), fr.bufs[i * 4 + 2].data()}, {cy, cc, cc},
+                         e))
+                return false;
+            const long depth_frame = c.depth_color_format == RVSB_FMT_YUV420 ? (long)(cy * 2 * 3 / 2) : (long)(cy * 2);
+            if (!read_at(rvsb_config_depth_path(cfg, i), depth_frame, frame, {fr.bufs[i * 4 + 3].data()}, {cy}, e))
+                return false;
+        }
+        return true;
+    };
+    // Depth and mask files carry constant chroma planes
+    // (write_depth_YUV / write_mask_YUV, image_writing.cpp:104-139).
+    const uint16_t neutral = (uint16_t)std::lround(0.5 * (1.0 + (double)((1u << virt0.bit_depth_depth) - 1u)));
+    const bool depth_chroma = virt0.depth_color_format == RVSB_FMT_YUV420;
+    auto write = [&](int vf, const OutputFrame& o, std::string& e) -> bool {
+        const bool first = vf == 0;
+        if (files[RVSB_OUT_COLOR] && !append(files[RVSB_OUT_COLOR], first, o.yuv.data(), o.yuv.size() * 2, e))
+            return false;
+        if (files[RVSB_OUT_MASKED_COLOR] &&
+            !append(files[RVSB_OUT_MASKED_COLOR], first, o.masked.data(), o.masked.size() * 2, e))
+            return false;
+        if (files[RVSB_OUT_MASK]) {
+            std::vector<uint8_t> m(ny + 2 * nc, 128);
+            std::memcpy(m.data(), o.mask.data(), ny);
+            if (!append(files[RVSB_OUT_MASK], first, m.data(), m.size(), e)) return false;
+        }
+        for (int k : {RVSB_OUT_DEPTH, RVSB_OUT_MASKED_DEPTH}) {
+            if (!files[k]) continue;
+            const std::vector<uint16_t>& d = k == RVSB_OUT_DEPTH ? o.depth : o.masked_depth;
+            std::vector<uint16_t> img(d);
+            if (depth_chroma) img.resize(ny + 2 * nc, neutral);
+            if (!append(files[k], first, img.data(), img.size() * 2, e)) return false;
+        }
+        return true;
+    };
+
+    InputFrame in[2];
+    OutputFrame outs[2];
+    std::string load_err, write_err;
+    std::future<bool> loading = std::async(std::launch::async, [&] { return load(0, in[0], load_err); });
+    std::future<bool> writing;
     const auto t0 = std::chrono::steady_clock::now();
     int rc = 0;
     for (int vf = 0; vf < n_out && rc == 0; ++vf) {
-        const int input_frame = start + vf;
-        const int frame = extended_index(input_frame, n_frames);
-        for (int i = 0; i < n_in && rc == 0; ++i) {
-            const rvsb_camera& c = cams[i];
-            const size_t ny = (size_t)c.width * c.height, nc = (size_t)(c.width / 2) * (c.height / 2);
-            bufs[i * 4 + 0].resize(ny);
-            bufs[i * 4 + 1].resize(nc);
-            bufs[i * 4 + 2].resize(nc);
-            bufs[i * 4 + 3].resize(ny);
-            std::string e;
-            const long color_frame = (long)(ny * 2 * 3 / 2);
-            if (!read_at(rvsb_config_texture_path(cfg, i), color_frame, frame,
-                         {bufs[i * 4].data(), bufs[i * 4 + 1].data(), bufs[i * 4 + 2].data()}, {ny, nc, nc}, e)) {
-                std::fprintf(stderr, "%s\n", e.c_str());
-                rc = 1;
-                break;
-            }
-            const long depth_frame = c.depth_color_format == RVSB_FMT_YUV420 ? (long)(ny * 2 * 3 / 2) : (long)(ny * 2);
-            if (!read_at(rvsb_config_depth_path(cfg, i), depth_frame, frame, {bufs[i * 4 + 3].data()}, {ny}, e)) {
-                std::fprintf(stderr, "%s\n", e.c_str());
-                rc = 1;
-                break;
-            }
-            planes[i].y = bufs[i * 4].data();
-            planes[i].u = bufs[i * 4 + 1].data();
-            planes[i].v = bufs[i * 4 + 2].data();
-            planes[i].depth = bufs[i * 4 + 3].data();
-        }
-        if (rc) break;
-        rvsb_camera virt;
-        if (rvsb_config_virtual_camera_at(cfg, 0, input_frame, &virt) != RVSB_OK) {
-            std::fprintf(stderr, "pose trace has no entry for frame %d\n", input_frame);
+        if (!loading.get()) {
+            std::fprintf(stderr, "%s\n", load_err.c_str());
             rc = 1;
             break;
         }
-        const size_t ny = (size_t)virt.width * virt.height, nc = (size_t)(virt.width / 2) * (virt.height / 2);
-        std::vector<uint16_t> oy(ny), ou(nc), ov(nc);
-        rvsb_yuv420 out{oy.data(), ou.data(), ov.data()};
-        st = rvsb_synthesize_host(ctx, cams.data(), n_in, planes.data(), &virt, &params, &out, nullptr);
+        InputFrame& cur = in[vf % 2];
+        if (vf + 1 < n_out)
+            loading = std::async(std::launch::async, [&, vf] { return load(vf + 1, in[(vf + 1) % 2], load_err); });
+        for (int i = 0; i < n_in && rc == 0; ++i) {
+            rvsb_view_planes p{cur.bufs[i * 4].data(), cur.bufs[i * 4 + 1].data(), cur.bufs[i * 4 + 2].data(),
+                               cur.bufs[i * 4 + 3].data()};
+            if ((st = rvsb_scene_upload(scene, i, &p, 0, nullptr)) != RVSB_OK) {
+                std::fprintf(stderr, "upload failed: %s\n", rvsb_last_error(ctx));
+                rc = 1;
+            }
+        }
+        if (rc) break;
+        rvsb_camera virt;
+        if (rvsb_config_virtual_camera_at(cfg, 0, start + vf, &virt) != RVSB_OK) {
+            std::fprintf(stderr, "pose trace has no entry for frame %d\n", start + vf);
+            rc = 1;
+            break;
+        }
+        st = rvsb_synthesize_aux(scene, &virt, &params, &out, &aux, nullptr);
         if (st != RVSB_OK) {
             std::fprintf(stderr, "synthesis failed: %s (%s)\n", rvsb_status_string(st), rvsb_last_error(ctx));
             rc = 1;
             break;
         }
-        const char* out_path = rvsb_config_output_path(cfg, 0);
-        if (out_path) {
-            FILE* f = std::fopen(out_path, vf ? "ab" : "wb");
-            if (!f) {
-                std::fprintf(stderr, "Failed to open YUV output image\n");
-                rc = 1;
-                break;
-            }
-            std::fwrite(oy.data(), 2, ny, f);
-            std::fwrite(ou.data(), 2, nc, f);
-            std::fwrite(ov.data(), 2, nc, f);
-            std::fclose(f);
+        // The previous frame's write must finish before its buffers are reused.
+        if (writing.valid() && !writing.get()) {
+            std::fprintf(stderr, "%s\n", write_err.c_str());
+            rc = 1;
+            break;
         }
+        OutputFrame& o = outs[vf % 2];
+        o.yuv.resize(ny + 2 * nc);
+        cudaMemcpy(o.yuv.data(), d_yuv, o.yuv.size() * 2, cudaMemcpyDeviceToHost);
+        if (d_masked) {
+            o.masked.resize(ny + 2 * nc);
+            cudaMemcpy(o.masked.data(), d_masked, o.masked.size() * 2, cudaMemcpyDeviceToHost);
+        }
+        if (d_mask) {
+            o.mask.resize(ny);
+            cudaMemcpy(o.mask.data(), d_mask, ny, cudaMemcpyDeviceToHost);
+        }
+        if (d_depth) {
+            o.depth.resize(ny);
+            cudaMemcpy(o.depth.data(), d_depth, ny * 2, cudaMemcpyDeviceToHost);
+        }
+        if (d_mdepth) {
+            o.masked_depth.resize(ny);
+            cudaMemcpy(o.masked_depth.data(), d_mdepth, ny * 2, cudaMemcpyDeviceToHost);
+        }
+        if (cudaGetLastError() != cudaSuccess) {
+            std::fprintf(stderr, "copying the outputs failed\n");
+            rc = 1;
+            break;
+        }
+        writing = std::async(std::launch::async, [&, vf] { return write(vf, outs[vf % 2], write_err); });
+    }
+    if (loading.valid()) loading.wait();
+    if (writing.valid() && !writing.get() && rc == 0) {
+        std::fprintf(stderr, "%s\n", write_err.c_str());
+        rc = 1;
     }
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (rc == 0)
         std::printf("Total time: %.3f sec.\nAv. speed: %.3f fps.\nAv. time per frame: %.3f sec.\n", secs,
                     n_out / secs, secs / n_out);
+    cudaFree(d_yuv);
+    cudaFree(d_masked);
+    cudaFree(d_mask);
+    cudaFree(d_depth);
+    cudaFree(d_mdepth);
+    rvsb_scene_destroy(scene);
     rvsb_destroy(ctx);
     rvsb_config_free(cfg);
     return rc;

@@ -10,7 +10,7 @@ streams as cudaStream_t handles (torch.cuda.Stream.cuda_stream).
 import ctypes
 import os
 
-from .abi import (Camera, DebugOut, SynthParams, ViewPlanes, Yuv420, make_camera, PERSPECTIVE,
+from .abi import (AuxOut, Camera, DebugOut, SynthParams, ViewPlanes, Yuv420, make_camera, PERSPECTIVE,
                   EQUIRECTANGULAR, YUV420, YUV400, RVSB_OK)
 from . import abi
 
@@ -32,8 +32,10 @@ EXPORTED = [
     "rvsb_server_create", "rvsb_server_add_scene", "rvsb_server_reserve", "rvsb_server_submit", "rvsb_server_poll",
     "rvsb_server_drain", "rvsb_server_clock", "rvsb_server_destroy",
     "rvsb_batch_set_autotune", "rvsb_batch_set_raster_variant", "rvsb_batch_last_raster_variant",
-    "rvsb_scene_set_autotune",
+    "rvsb_scene_set_autotune", "rvsb_synthesize_aux", "rvsb_config_output_file", "rvsb_config_validity_threshold",
 ]
+
+OUT_COLOR, OUT_MASKED_COLOR, OUT_MASK, OUT_DEPTH, OUT_MASKED_DEPTH = range(5)
 
 RASTER_VARIANTS = 6
 
@@ -107,6 +109,11 @@ def load():
     L.rvsb_batch_last_launch_count.argtypes = [c_p]
     L.rvsb_batch_set_profiling.argtypes = [c_p, ctypes.c_int]
     L.rvsb_batch_stage_times.argtypes = [c_p, P(ctypes.c_float), ctypes.c_int]
+    L.rvsb_synthesize_aux.argtypes = [c_p, P(Camera), P(SynthParams), P(Yuv420), P(AuxOut), c_p]
+    L.rvsb_config_output_file.argtypes = [c_p, ctypes.c_int, ctypes.c_int]
+    L.rvsb_config_output_file.restype = ctypes.c_char_p
+    L.rvsb_config_validity_threshold.argtypes = [c_p]
+    L.rvsb_config_validity_threshold.restype = ctypes.c_float
     L.rvsb_batch_set_autotune.argtypes = [c_p, ctypes.c_int]
     L.rvsb_batch_set_raster_variant.argtypes = [c_p, ctypes.c_int]
     L.rvsb_batch_last_raster_variant.argtypes = [c_p]
@@ -209,6 +216,21 @@ class Scene:
         out = Yuv420(*(_ptr(a) for a in out_planes))
         return self.ctx.check(self.ctx.lib.rvsb_synthesize(self.h, ctypes.byref(virt), ctypes.byref(p),
                                                            ctypes.byref(out), _stream(stream)))
+
+    def synthesize_aux(self, virt, p, out_planes, mask=None, masked=None, depth=None, masked_depth=None,
+                       validity_threshold=5000.0, stream=None):
+        """rvsb_synthesize_aux: the output planes plus the auxiliary outputs
+        (device buffers; any may be None)."""
+        out = Yuv420(*(_ptr(a) for a in out_planes))
+        aux = AuxOut()
+        aux.mask = _ptr(mask)
+        if masked is not None:
+            aux.masked = Yuv420(*(_ptr(a) for a in masked))
+        aux.depth = _ptr(depth)
+        aux.masked_depth = _ptr(masked_depth)
+        aux.validity_threshold = validity_threshold
+        return self.ctx.check(self.ctx.lib.rvsb_synthesize_aux(self.h, ctypes.byref(virt), ctypes.byref(p),
+                                                               ctypes.byref(out), ctypes.byref(aux), _stream(stream)))
 
     def synthesize_frame(self, device_planes, virt, p, out_planes, stream=None):
         """Per-frame call with raw planes in device memory (no copies)."""
@@ -469,6 +491,13 @@ class Config:
     def paths(self, i):
         f = lambda g: (g(self.h, i) or b"").decode()
         return f(self.lib.rvsb_config_texture_path), f(self.lib.rvsb_config_depth_path)
+
+    def output_file(self, kind, i=0):
+        r = self.lib.rvsb_config_output_file(self.h, int(kind), i)
+        return r.decode() if r else None
+
+    def validity_threshold(self):
+        return self.lib.rvsb_config_validity_threshold(self.h)
 
     def output_path(self, i=0):
         r = self.lib.rvsb_config_output_path(self.h, i)

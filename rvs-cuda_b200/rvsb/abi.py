@@ -124,3 +124,16 @@ def make_camera(projection=PERSPECTIVE, width=960, height=540, position=(0, 0, 0
     c.full_hor_range = 1 if (projection == EQUIRECTANGULAR and
                              float(hor_range[0]) == -180.0 and float(hor_range[1]) == 180.0) else 0
     return c
+
+
+class AuxOut(ctypes.Structure):
+    """rvsb_aux_out: device pointers of the auxiliary outputs (NULL = off)."""
+
+    _fields_ = [
+        ("mask", ctypes.c_void_p),
+        ("masked", Yuv420),
+        ("depth", ctypes.c_void_p),
+        ("masked_depth", ctypes.c_void_p),
+        ("validity_threshold", ctypes.c_float),
+        ("reserved", ctypes.c_int32),
+    ]

@@ -1,0 +1,108 @@
+"""The RVS drop-in CLI (rvs-cuda_b200/lib/rvsb) end to end: reference-format
+configuration, camera file, pose trace and raw YUV files in, the five output
+files out, every output frame checked against the oracle.  Three input
+frames and five output frames exercise the ping-pong frame index
+(Pipeline.cpp:157-167) and the pose trace (Pipeline.cpp:173-181)."""
+import copy
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from rvsb import abi, scenes
+from helpers import assert_parity
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "rvs-cuda_b200", "lib", "rvsb")
+
+
+def _cam_json(name, c):
+    d = {"Name": name, "Projection": "Equirectangular" if c.projection else "Perspective",
+         "Position": [float(x) for x in c.position], "Rotation": [float(x) for x in c.rotation],
+         "Depthmap": 1, "Background": 0, "Depth_range": [float(x) for x in c.depth_range],
+         "Resolution": [c.width, c.height], "BitDepthColor": c.bit_depth_color, "BitDepthDepth": c.bit_depth_depth,
+         "ColorSpace": "YUV420", "DepthColorSpace": "YUV420", "HasInvalidDepth": bool(c.has_invalid_depth)}
+    if c.projection:
+        d["Hor_range"] = [float(x) for x in c.hor_range]
+        d["Ver_range"] = [float(x) for x in c.ver_range]
+    else:
+        d["Focal"] = [float(x) for x in c.focal]
+        d["Principle_point"] = [float(x) for x in c.principle_point]
+    return d
+
+
+def _frame_planes(planes, k):
+    """Input frame k: luma shifted by 7 codes per frame so frames differ."""
+    y, u, v, d = planes
+    y2 = np.clip(y.astype(np.int32) + 7 * k, 0, 1023).astype(np.uint16)
+    return y2, u, v, d
+
+
+def extended_index(f, n):
+    g, r = divmod(f, n)
+    return n - r - 1 if g % 2 else r
+
+
+def test_cli_end_to_end(tmp_path):
+    wl = scenes.random_pose_small(n_views=2, w=96, h=54, seed=91)
+    n_frames, n_out = 3, 5
+    names = [f"v{i}" for i in range(len(wl.inputs))]
+    target = wl.targets[0]
+    cams = {"Version": "2.0", "cameras": [_cam_json(n, c) for n, c in zip(names, wl.inputs)] +
+            [_cam_json("viewport", target)]}
+    (tmp_path / "cams.json").write_text(json.dumps(cams))
+    for i, planes in enumerate(wl.planes):
+        with open(tmp_path / f"t{i}.yuv", "wb") as ft, open(tmp_path / f"d{i}.yuv", "wb") as fd:
+            for k in range(n_frames):
+                y, u, v, d = _frame_planes(planes, k)
+                ft.write(y.tobytes() + u.tobytes() + v.tobytes())
+                chroma = np.full((d.shape[0] // 2) * (d.shape[1] // 2), 32768, np.uint16)
+                fd.write(d.tobytes() + chroma.tobytes() + chroma.tobytes())
+    rng = np.random.default_rng(5)
+    trace = []
+    for f in range(n_out):
+        dp = rng.uniform(-0.01, 0.01, 3)
+        rot = [target.rotation[0] + rng.uniform(-1, 1), target.rotation[1], target.rotation[2]]
+        trace.append((dp, rot))
+    (tmp_path / "pose.csv").write_text("X,Y,Z,Yaw,Pitch,Roll\n" + "".join(
+        ",".join(repr(float(x)) for x in list(dp) + list(rot)) + "\n" for dp, rot in trace))
+    cfg = {"Version": "3.0", "InputCameraParameterFile": "cams.json", "VirtualCameraParameterFile": "cams.json",
+           "InputCameraNames": names, "VirtualCameraNames": ["viewport"],
+           "ViewImageNames": [f"t{i}.yuv" for i in range(len(names))],
+           "DepthMapNames": [f"d{i}.yuv" for i in range(len(names))],
+           "OutputFiles": ["out.yuv"], "MaskedOutputFiles": ["masked.yuv"], "OutputMasks": ["mask.yuv"],
+           "DepthOutputFiles": ["depth.yuv"], "MaskedDepthOutputFiles": ["mdepth.yuv"],
+           "NumberOfFrames": n_frames, "NumberOfOutputFrames": n_out, "StartFrame": 0,
+           "VirtualPoseTraceName": "pose.csv", "BlendingFactor": 5.0, "ValidityThreshold": 6000.0}
+    (tmp_path / "rvs.json").write_text(json.dumps(cfg))
+    r = subprocess.run([CLI, "rvs.json", "--cuda"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    wo, ho = target.width, target.height
+    ny, nc = wo * ho, (wo // 2) * (ho // 2)
+    out = np.fromfile(tmp_path / "out.yuv", np.uint16).reshape(n_out, ny + 2 * nc)
+    masked = np.fromfile(tmp_path / "masked.yuv", np.uint16).reshape(n_out, ny + 2 * nc)
+    mask = np.fromfile(tmp_path / "mask.yuv", np.uint8).reshape(n_out, ny + 2 * nc)
+    depth = np.fromfile(tmp_path / "depth.yuv", np.uint16).reshape(n_out, ny + 2 * nc)
+    mdepth = np.fromfile(tmp_path / "mdepth.yuv", np.uint16).reshape(n_out, ny + 2 * nc)
+    assert (mask[:, ny:] == 128).all() and (depth[:, ny:] == 32768).all()
+    for f in range(n_out):
+        k = extended_index(f, n_frames)
+        planes = [_frame_planes(p, k) for p in wl.planes]
+        virt = copy.deepcopy(target)
+        dp, rot = trace[f]
+        for a in range(3):
+            virt.position[a] = np.float32(np.float32(target.position[a]) + np.float32(dp[a]))
+            virt.rotation[a] = np.float32(rot[a])
+        ref = O.synthesize_aux(wl.inputs, planes, virt, 5.0, 6000.0)
+        got = O.split_yuv420(out[f], wo, ho)
+        assert_parity(got, ref["yuv"])
+        assert_parity(O.split_yuv420(masked[f], wo, ho), ref["masked_yuv"])
+        assert (mask[f, :ny].reshape(ho, wo) != ref["mask"]).mean() <= 1e-3
+        for g, rr in ((depth[f, :ny], ref["depth"]), (mdepth[f, :ny], ref["masked_depth"])):
+            diff = np.abs(g.reshape(ho, wo).astype(np.int64) - rr.astype(np.int64))
+            assert (diff > 1).mean() <= 5e-3
