@@ -115,7 +115,7 @@ typedef enum rvsb_chroma_rounding {
 
 /* Synthesis options (Config, rvs/src/Config.hpp:172-205). */
 typedef struct rvsb_synth_params {
-    float blending_factor;    /* "BlendingFactor" (default 5); must be > 0 */
+    float blending_factor;    /* "BlendingFactor" (default 5); < 0 blends by maximum quality */
     float precision;          /* "Precision"; only 1 is supported */
     int32_t chroma_rounding;  /* rvsb_chroma_rounding; 0 unless set */
     int32_t reserved;         /* must be 0 */

@@ -550,6 +550,30 @@ static void blend_step(int v, const float* vcol, const float* vq, const float* v
         return;
     }
     const float empty[3] = {0.f, 1.f, 0.f};
+    if (exponent < 0) {
+        // blend_img_by_max (blending.cpp:293-308) over {accumulator, view}:
+        // start from the empty colour and quality 0, then each image
+        // replaces the result where its quality is strictly larger.
+        for (size_t p = 0; p < no; ++p) {
+            float c[3] = {empty[0], empty[1], empty[2]};
+            float q = 0.f;
+            bool prol = false;
+            if (out_quality[p] > q) {
+                for (int k = 0; k < 3; ++k) c[k] = out_color[p * 3 + k];
+                q = out_quality[p];
+                prol = acc_mask[p] != 0;
+            }
+            if (vq[p] > q) {
+                for (int k = 0; k < 3; ++k) c[k] = vcol[p * 3 + k];
+                q = vq[p];
+                prol = vd[p] > 0.f;
+            }
+            for (int k = 0; k < 3; ++k) out_color[p * 3 + k] = c[k];
+            out_quality[p] = q;
+            acc_mask[p] = prol;
+        }
+        return;
+    }
     for (size_t p = 0; p < no; ++p) {
         const float* cols[2] = {out_color + p * 3, vcol + p * 3};
         float quals[2] = {out_quality[p], vq[p]};
@@ -603,7 +627,6 @@ int orc_blend(int n, const float* const* colors, const float* const* qualities,
               const float* const* depths, int wo, int ho, float exponent, float* out_color,
               float* out_quality) {
     if (n <= 0 || !colors || !qualities || !depths || !out_color || !out_quality) return RVSB_E_ARG;
-    if (exponent < 0) return RVSB_E_UNSUPPORTED;  // blend_img_by_max
     const size_t no = (size_t)wo * ho;
     std::vector<uint8_t> acc_mask(no);  // m_depth_mask
     for (int v = 0; v < n; ++v)
@@ -792,7 +815,6 @@ int orc_synthesize_aux(int n, const rvsb_camera* cams, const rvsb_view_planes* p
     }
     // Blend view by view; the accumulator's quality before each view feeds
     // the depth rule.
-    if (exponent < 0) return RVSB_E_UNSUPPORTED;  // blend_img_by_max
     std::vector<float> bc(no * 3), bq(no), prev_q(no), depth(no), validity(no);
     std::vector<uint8_t> acc_mask(no);
     const bool want_aux = out_mask || out_masked_yuv || out_depth || out_masked_depth;

@@ -59,8 +59,8 @@ size_t plane_bytes(const rvsb_camera& c, int k) {
 
 void validate_params(const rvsb_synth_params* p) {
     if (!p) throw ArgError("null synthesis parameters");
-    if (!(p->blending_factor > 0.f) || !std::isfinite(p->blending_factor))
-        throw Unsupported("BlendingFactor must be a positive finite number");
+    if (!std::isfinite(p->blending_factor) || p->blending_factor == 0.f)
+        throw Unsupported("BlendingFactor must be a finite nonzero number (negative: blend by maximum)");
     if (p->precision != 1.f) throw Unsupported("Precision other than 1 is not supported");
     if (p->chroma_rounding != RVSB_CHROMA_TIES_EVEN && p->chroma_rounding != RVSB_CHROMA_TIES_UP)
         throw ArgError("chroma_rounding must be RVSB_CHROMA_TIES_EVEN or RVSB_CHROMA_TIES_UP");

@@ -55,6 +55,7 @@ struct DevTarget {
     float inv_blend_exp;                  // 1.0f / BlendingFactor
     int blend_exp_int;                    // BlendingFactor when it is an integer in [2, 16], else 0
     int chroma_ties_up;                   // output chroma mean: 1 rounds ties up, 0 to even
+    int blend_max;                        // BlendingFactor < 0: blend by maximum quality
     int tile_wl, tile_hl;                 // log2 of the tile width and height
     int ntx, nty;                         // output tiles
     int n_views;

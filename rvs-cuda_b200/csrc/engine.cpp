@@ -234,6 +234,7 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
     if (p.blending_factor == std::floor(p.blending_factor) && p.blending_factor >= 2.f && p.blending_factor <= 16.f)
         D.blend_exp_int = (int)p.blending_factor;
     D.chroma_ties_up = p.chroma_rounding == RVSB_CHROMA_TIES_UP;
+    D.blend_max = p.blending_factor < 0.f ? 1 : 0;
     const RasterVariant& rv = kRasterVariants[variant];
     D.tile_wl = log2i(rv.tw);
     D.tile_hl = log2i(rv.th);

@@ -393,7 +393,6 @@ Config load_config(const std::string& path) {
     }
     if (c.blending_method != "Simple")
         throw ConfigError("Unknown view blending method \"" + c.blending_method + "\"");
-    if (c.blending_factor < 0) throw Unsupported("BlendingFactor < 0 (blend by maximum) is not supported");
     if (auto n = root.optional("StartFrame")) c.start_frame = n.asInt();
     if (auto n = root.optional("NumberOfFrames")) c.number_of_frames = n.asInt();
     if (auto n = root.optional("NumberOfOutputFrames"))

@@ -252,7 +252,8 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
                     adepth = f.depth;
                     avalid = f.validity;
                 } else {
-                    const float qacc = v == 1 ? a.q : (a.q > 0.f ? powf(a.q, T.inv_blend_exp) : a.q);
+                    const float qacc =
+                        (v == 1 || T.blend_max) ? a.q : (a.q > 0.f ? powf(a.q, T.inv_blend_exp) : a.q);
                     if (qv > qacc) adepth = f.depth;
                     avalid = smax(avalid, f.validity);
                 }
@@ -310,7 +311,8 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
                     dbg.blend_color[o * 3 + 2] = c2;
                 }
                 if (dbg.blend_quality)
-                    dbg.blend_quality[o] = (T.n_views == 1 || !(q > 0.f)) ? q : powf(q, T.inv_blend_exp);
+                    dbg.blend_quality[o] =
+                        (T.n_views == 1 || T.blend_max || !(q > 0.f)) ? q : powf(q, T.inv_blend_exp);
                 if (dbg.inpaint_source) {
                     dbg.inpaint_source[o * 2 + 0] = x;
                     dbg.inpaint_source[o * 2 + 1] = y;

@@ -76,6 +76,21 @@ __device__ __forceinline__ void blend_view(BlendAcc& a, int v, const Fragment& f
         a.q = qv;
         return;
     }
+    if (T.blend_max) {
+        // blend_img_by_max (blending.cpp:293-308): the empty colour and
+        // quality 0, replaced by the accumulator where its quality is
+        // positive, then by the view where its quality is larger still.
+        BlendAcc r = {0.f, 1.f, 0.f, 0.f};
+        if (a.q > r.q) r = a;
+        if (qv > r.q) {
+            r.c0 = f.col.x;
+            r.c1 = f.col.y;
+            r.c2 = f.col.z;
+            r.q = qv;
+        }
+        a = r;
+        return;
+    }
     float sum = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     if (a.q > 0.f) {
         const float w = v == 1 ? blend_pow(a.q, T.blend_exp, T.blend_exp_int) : a.q;

@@ -13,6 +13,7 @@
 // request records its submit, launch and completion times.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -245,7 +246,8 @@ rvsb_status rvsb_server_submit(rvsb_server* s, int scene_id, const rvsb_camera* 
         s->ctx->last_error = std::string("virtual camera: ") + why;
         return RVSB_E_ARG;
     }
-    if (!(params->blending_factor > 0.f) || params->precision != 1.f || params->reserved != 0 ||
+    if (!std::isfinite(params->blending_factor) || params->blending_factor == 0.f || params->precision != 1.f ||
+        params->reserved != 0 ||
         (params->chroma_rounding != RVSB_CHROMA_TIES_EVEN && params->chroma_rounding != RVSB_CHROMA_TIES_UP))
         return RVSB_E_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(s->mu);

@@ -20,8 +20,9 @@ CASES = [
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
-@pytest.mark.parametrize("threshold", [5000.0, 9000.0])
-def test_aux_outputs_match_oracle(ctx, case, threshold):
+@pytest.mark.parametrize("threshold,exponent", [(5000.0, 5.0), (9000.0, 5.0), (5000.0, -1.0)],
+                         ids=["t5000", "t9000", "t5000-by_max"])
+def test_aux_outputs_match_oracle(ctx, case, threshold, exponent):
     import torch
     wl = scenes.random_pose_small(**case)
     target = wl.targets[0]
@@ -35,10 +36,10 @@ def test_aux_outputs_match_oracle(ctx, case, threshold):
     mask = torch.zeros(wo * ho, dtype=torch.uint8, device="cuda")
     depth = torch.zeros(wo * ho, dtype=torch.int16, device="cuda")
     mdepth = torch.zeros(wo * ho, dtype=torch.int16, device="cuda")
-    sc.synthesize_aux(target, rvsb.params(5.0), out, mask=mask, masked=masked, depth=depth, masked_depth=mdepth,
-                      validity_threshold=threshold)
+    sc.synthesize_aux(target, rvsb.params(exponent), out, mask=mask, masked=masked, depth=depth,
+                      masked_depth=mdepth, validity_threshold=threshold)
     torch.cuda.synchronize()
-    ref = O.synthesize_aux(wl.inputs, wl.planes, target, 5.0, threshold)
+    ref = O.synthesize_aux(wl.inputs, wl.planes, target, exponent, threshold)
     yuv = (to_u16(out[0], (ho, wo)), to_u16(out[1], (ho // 2, wo // 2)), to_u16(out[2], (ho // 2, wo // 2)))
     assert_parity(yuv, ref["yuv"])
     gmask = mask.cpu().numpy().reshape(ho, wo)

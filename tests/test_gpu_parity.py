@@ -42,7 +42,7 @@ def _oracle_stages(wl, target, exponent):
 
 
 @pytest.mark.parametrize("case", SMALL_CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
-@pytest.mark.parametrize("exponent", [5.0, 1.0])
+@pytest.mark.parametrize("exponent", [5.0, 1.0, -1.0], ids=["exp5", "exp1", "by_max"])
 def test_stages_small(ctx, case, exponent):
     wl = scenes.random_pose_small(**case)
     target = wl.targets[0]
