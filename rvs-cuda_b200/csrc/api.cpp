@@ -101,12 +101,17 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
         BatchCore& core = single_core(sc);
         int decodes = 0;
         if (frame) {
+            DecodeJobs jobs{};
+            int max_w = 0, max_h = 0;
             for (size_t v = 0; v < sc->cams.size(); ++v) {
                 const rvsb_camera& c = sc->cams[v];
-                launch_decode_color(frame[v].y, frame[v].u, frame[v].v, c.width, c.height,
-                                    sc->color[v]->as<uint64_t>(), s);
-                ++decodes;
+                jobs.v[v] = DecodeJob{frame[v].y, frame[v].u, frame[v].v, sc->color[v]->as<uint64_t>(), c.width,
+                                      c.height};
+                max_w = std::max(max_w, c.width);
+                max_h = std::max(max_h, c.height);
             }
+            launch_decode_views(jobs, (int)sc->cams.size(), max_w, max_h, s);
+            decodes = 1;
             check(cudaPeekAtLastError(), "decode colour");
         }
         SlotRequest r;

@@ -24,7 +24,23 @@ __global__ void decode_color_kernel(const uint16_t* __restrict__ py, const uint1
              ((uint64_t)chroma4(pv, cw, ch, j, i) << 36);
 }
 
+// All views of a frame in one launch: grid (ceil(max_w / 256), max_h, views).
+__global__ void decode_views_kernel(const __grid_constant__ DecodeJobs jobs) {
+    const DecodeJob& J = jobs.v[blockIdx.z];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= J.w || i >= J.h) return;
+    const int cw = J.w / 2, ch = J.h / 2;
+    const size_t o = (size_t)i * J.w + j;
+    J.out[o] = (uint64_t)J.y[o] | ((uint64_t)chroma4(J.u, cw, ch, j, i) << 18) |
+               ((uint64_t)chroma4(J.v, cw, ch, j, i) << 36);
+}
+
 }  // namespace
+
+void launch_decode_views(const DecodeJobs& jobs, int n, int max_w, int max_h, cudaStream_t s) {
+    decode_views_kernel<<<dim3((max_w + 255) / 256, max_h, n), 256, 0, s>>>(jobs);
+}
 
 void launch_decode_color(const uint16_t* y, const uint16_t* u, const uint16_t* v, int w, int h, uint64_t* out,
                          cudaStream_t s) {

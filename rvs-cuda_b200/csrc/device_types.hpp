@@ -120,7 +120,11 @@ struct SlotBuffers {
     uint64_t* codes;     // Wo*Ho packed output codes + hole bit
     uint8_t* holes;      // Wo*Ho hole mask (1 = no view covers the pixel)
     uint64_t* scan[4];   // Wo*Ho inpainting scratch each
+    uint64_t* inpaint_seg;  // column-group minima of the inpainting passes
 };
+
+// Most row groups per column strip in the inpainting passes.
+constexpr int INPAINT_MAX_GROUPS = 8;
 
 // Everything one synthesis (one virtual view) needs on the device.  A batch
 // keeps one table per slot in device memory; every kernel of the batch reads

@@ -71,7 +71,8 @@ SlotNeeds needs_of(const rvsb_scene* sc, int wo, int ho) {
 size_t SlotWorkspace::bytes_for(const rvsb_scene* sc, int wo, int ho) {
     const SlotNeeds n = needs_of(sc, wo, ho);
     return sizeof(DevStatus) + n.vert * sizeof(float4) + n.bbox * sizeof(int4) + 3 * n.bins * sizeof(int) +
-           n.list * sizeof(int) + n.out * (sizeof(uint64_t) * 5 + 1);
+           n.list * sizeof(int) + n.out * (sizeof(uint64_t) * 5 + 1) +
+           (size_t)INPAINT_MAX_GROUPS * ((wo + 31) / 32) * 64 * sizeof(uint64_t);
 }
 
 void SlotWorkspace::ensure(rvsb_context* ctx, const rvsb_scene* sc, int wo, int ho) {
@@ -94,6 +95,11 @@ void SlotWorkspace::ensure(rvsb_context* ctx, const rvsb_scene* sc, int wo, int 
     if (n.list > cap_list) {
         list.alloc(ctx, n.list * sizeof(int));
         cap_list = n.list;
+    }
+    const size_t strips = (size_t)(wo + 31) / 32;
+    if (strips > cap_strips) {
+        inpaint_seg.alloc(ctx, (size_t)INPAINT_MAX_GROUPS * strips * 64 * sizeof(uint64_t));
+        cap_strips = strips;
     }
     if (n.out > cap_out) {
         codes.alloc(ctx, n.out * sizeof(uint64_t));
@@ -252,6 +258,7 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
     B.codes = ws.codes.as<uint64_t>();
     B.holes = ws.holes.as<uint8_t>();
     for (int s = 0; s < 4; ++s) B.scan[s] = ws.scan[s].as<uint64_t>();
+    B.inpaint_seg = ws.inpaint_seg.as<uint64_t>();
     T.out_y = r.out.y;
     T.out_u = r.out.u;
     T.out_v = r.out.v;

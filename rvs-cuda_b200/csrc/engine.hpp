@@ -69,7 +69,8 @@ struct DevMem {
 struct SlotWorkspace {
     DevMem status, counts, offsets, cursor, list, codes, holes, scan[4], vert, bbox;
     DevMem aux_depth, aux_valid;  // blended depth / validity (auxiliary outputs only)
-    size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0, cap_aux = 0;
+    DevMem inpaint_seg;           // column-group minima of the inpainting passes
+    size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0, cap_aux = 0, cap_strips = 0;
     void ensure_aux(rvsb_context* ctx, int wo, int ho);
 
     // Bytes a slot needs for `scene` at output size wo x ho.

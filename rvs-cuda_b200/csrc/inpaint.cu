@@ -23,6 +23,8 @@
 // of a hole, so restricting the scans to the grown bounding box changes
 // nothing.  Loads are issued in batches (RB rows, CB chunks) so each thread
 // keeps several in flight.
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "kernels.hpp"
 
@@ -49,6 +51,7 @@ struct InpaintImage {
     uint64_t* codes;           // wo*ho packed codes (the fill copies them)
     uint64_t* scan[4];         // wo*ho words each
     int32_t* sources;          // optional: (x, y) source of every hole
+    uint64_t* seg;             // column-group minima (2 words per group, strip and lane), G > 1 only
     uint16_t* out_y;
     uint16_t* out_u;
     uint16_t* out_v;
@@ -70,6 +73,7 @@ struct FromTables {
 #pragma unroll
         for (int k = 0; k < 4; ++k) im.scan[k] = t.b.scan[k];
         im.sources = t.dbg.inpaint_source;
+        im.seg = t.b.inpaint_seg;
         im.out_y = t.out_y;
         im.out_u = t.out_u;
         im.out_v = t.out_v;
@@ -122,27 +126,38 @@ __device__ __forceinline__ unsigned long long warp_incl_min_rev(unsigned long lo
 
 // Sweep 0, rows (forward): R(p) = lexmin over q.x <= p.x of
 // (C(q).d + p.x - q.x, C(q).src).  One warp per row of the region.
+// Rows are scanned by one CTA each: 8 warps take 128-pixel segments in
+// rounds of 8, exchange their segment minima through shared memory and scan
+// with the minimum of every segment before them.  The keys carry the column
+// bias, so a segment's minimum does not depend on where it is applied.
+constexpr int ROW_WARPS = 8;
+constexpr int SEG = 32 * CB;
+
 template <class Src>
-__global__ void inpaint_row0_kernel(const __grid_constant__ Src src) {
+__global__ void __launch_bounds__(32 * ROW_WARPS) inpaint_row0_kernel(const __grid_constant__ Src src) {
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
     const uint8_t* __restrict__ holes = im.holes;
     uint64_t* __restrict__ R = im.scan[0];
+    __shared__ unsigned long long s_min[ROW_WARPS];
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
-    const int lane = threadIdx.x & 31;
-    const int y = rg.y0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int y = rg.y0 + (int)blockIdx.x;
     if (y > rg.y1) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint8_t* hr = holes + (size_t)y * wo;
     const uint8_t* hd = y + 1 < ho ? hr + wo : nullptr;
-    unsigned long long carry = kEmptyKey;
-    for (int base = rg.x0; base <= rg.x1; base += 32 * CB) {
-        unsigned long long key[CB];
+    const int nseg = (rg.x1 - rg.x0 + SEG) / SEG;
+    unsigned long long round_carry = kEmptyKey;
+    for (int seg0 = 0; seg0 < nseg; seg0 += ROW_WARPS) {
+        const int base = rg.x0 + (seg0 + warp) * SEG;
+        unsigned long long incl[CB];
+        unsigned long long local = kEmptyKey;
 #pragma unroll
         for (int c = 0; c < CB; ++c) {
             const int x = base + 32 * c + lane;
-            key[c] = kEmptyKey;
+            unsigned long long key = kEmptyKey;
             if (x <= rg.x1) {
                 uint32_t d = kInfD;
                 int sx = x, sy = y;
@@ -153,22 +168,28 @@ __global__ void inpaint_row0_kernel(const __grid_constant__ Src src) {
                 } else if (x + 1 < wo && !hr[x + 1]) {
                     d = 1; sx = x + 1;
                 }
-                if (d != kInfD) key[c] = pack_dxy((uint32_t)((int)d - x + kScanBias), sx, sy);
+                if (d != kInfD) key = pack_dxy((uint32_t)((int)d - x + kScanBias), sx, sy);
             }
+            incl[c] = umin64(warp_incl_min(key, lane), local);
+            local = __shfl_sync(0xffffffffu, incl[c], 31);
         }
+        if (lane == 0) s_min[warp] = local;
+        __syncthreads();
+        unsigned long long carry = round_carry;
+        for (int w2 = 0; w2 < warp; ++w2) carry = umin64(carry, s_min[w2]);
 #pragma unroll
         for (int c = 0; c < CB; ++c) {
             const int x = base + 32 * c + lane;
-            unsigned long long k = umin64(warp_incl_min(key[c], lane), carry);
-            if (x <= rg.x1) {
-                uint64_t out = ~0ull;
-                if (k != kEmptyKey)
-                    out = pack_dxy((uint32_t)((int)(k >> 32) - kScanBias + x), (int)((k >> 16) & 0xffff),
-                                   (int)(k & 0xffff));
-                R[(size_t)y * wo + x] = out;
-            }
-            carry = __shfl_sync(0xffffffffu, k, 31);
+            if (x > rg.x1) continue;
+            const unsigned long long k = umin64(incl[c], carry);
+            uint64_t out = ~0ull;
+            if (k != kEmptyKey)
+                out = pack_dxy((uint32_t)((int)(k >> 32) - kScanBias + x), (int)((k >> 16) & 0xffff),
+                               (int)(k & 0xffff));
+            R[(size_t)y * wo + x] = out;
         }
+        for (int w2 = 0; w2 < ROW_WARPS; ++w2) round_carry = umin64(round_carry, s_min[w2]);
+        __syncthreads();
     }
 }
 
@@ -184,8 +205,27 @@ __device__ __forceinline__ unsigned long long col0_key(uint64_t r, int y) {
 
 // Sweep 0, columns (forward): D0, S0 (p) = lexmin over q.y <= p.y of
 // (R(q).d + p.y - q.y, src).  Output packed (D0, S0) per pixel.
-template <class Src>
-__global__ void __launch_bounds__(1024) inpaint_col0_kernel(const __grid_constant__ Src src) {
+// Rows [gy0, gy1] of column group blockIdx.y of G, and the rows of warp w
+// within them.
+struct GroupRows {
+    int yb, ye;
+};
+__device__ __forceinline__ GroupRows group_rows(const Region& rg, int G, int w) {
+    const int nrows = rg.y1 - rg.y0 + 1;
+    const int RG = (nrows + G - 1) / G;
+    const int gy0 = rg.y0 + (int)blockIdx.y * RG, gy1 = min(rg.y1, gy0 + RG - 1);
+    const int L = (max(0, gy1 - gy0 + 1) + 31) / 32;
+    GroupRows r;
+    r.yb = gy0 + w * L;
+    r.ye = min(gy1, r.yb + L - 1);
+    return r;
+}
+
+// Grid (strips of 32 columns, G row groups, images).  With PRE the CTA only
+// stores its group's column minima; otherwise it scans its group starting
+// from the minima of the groups above it.
+template <class Src, bool PRE>
+__global__ void __launch_bounds__(1024) inpaint_col0_kernel(const __grid_constant__ Src src, int G) {
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
@@ -198,9 +238,9 @@ __global__ void __launch_bounds__(1024) inpaint_col0_kernel(const __grid_constan
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int x = rg.x0 + (int)blockIdx.x * 32 + lane;
     if (rg.x0 + (int)blockIdx.x * 32 > rg.x1) return;
-    const int nrows = rg.y1 - rg.y0 + 1;
-    const int L = (nrows + 31) / 32;
-    const int yb = rg.y0 + w * L, ye = min(rg.y1, yb + L - 1);
+    const int nstrips = (rg.x1 - rg.x0 + 32) / 32;
+    const GroupRows gr = group_rows(rg, G, w);
+    const int yb = gr.yb, ye = gr.ye;
     const bool col_ok = x <= rg.x1;
     unsigned long long m = kEmptyKey;
     if (col_ok)
@@ -213,8 +253,18 @@ __global__ void __launch_bounds__(1024) inpaint_col0_kernel(const __grid_constan
         }
     seg[w][lane] = m;
     __syncthreads();
+    if (PRE) {
+        if (w == 0) {
+            unsigned long long t = kEmptyKey;
+            for (int s = 0; s < 32; ++s) t = umin64(t, seg[s][lane]);
+            im.seg[((size_t)blockIdx.y * nstrips + blockIdx.x) * 64 + lane] = t;
+        }
+        return;
+    }
     unsigned long long run = kEmptyKey;
     for (int s = 0; s < w; ++s) run = umin64(run, seg[s][lane]);
+    for (int g = 0; g < (int)blockIdx.y; ++g)
+        run = umin64(run, im.seg[((size_t)g * nstrips + blockIdx.x) * 64 + lane]);
     if (!col_ok) return;
     const uint32_t big = (uint32_t)(wo + ho);
     for (int y0 = yb; y0 <= ye; y0 += RB) {
@@ -294,48 +344,59 @@ __global__ void inpaint_seed1_kernel(const __grid_constant__ Src src) {
 // Sweep 1, rows (backward, exclusive): RR(x, y) = min over q.x > x of
 // (T(q).d + q.x, q.x).  One warp per row.
 template <class Src>
-__global__ void inpaint_row1_kernel(const __grid_constant__ Src src) {
+__global__ void __launch_bounds__(32 * ROW_WARPS) inpaint_row1_kernel(const __grid_constant__ Src src) {
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
     const uint64_t* __restrict__ Tq = im.scan[2];
     uint64_t* __restrict__ RR = im.scan[0];
+    __shared__ unsigned long long s_min[ROW_WARPS];
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
-    const int lane = threadIdx.x & 31;
-    const int y = rg.y0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int y = rg.y0 + (int)blockIdx.x;
     if (y > rg.y1) return;
-    unsigned long long carry = kEmptyKey;
-    const int n = rg.x1 - rg.x0 + 1;
-    for (int base = 0; base < n; base += 32 * CB) {
-        unsigned long long key[CB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nseg = (rg.x1 - rg.x0 + SEG) / SEG;
+    unsigned long long round_carry = kEmptyKey;
+    // Segments run from the right end; within a chunk lane 31 holds the
+    // rightmost pixel.
+    for (int seg0 = 0; seg0 < nseg; seg0 += ROW_WARPS) {
+        const int base = (seg0 + warp) * SEG;
+        unsigned long long excl[CB];
+        unsigned long long local = kEmptyKey;
 #pragma unroll
         for (int c = 0; c < CB; ++c) {
-            // x runs from the right end: lane 31 holds the rightmost pixel of chunk c.
             const int x = rg.x1 - (base + 32 * c + (31 - lane));
-            key[c] = kEmptyKey;
+            unsigned long long key = kEmptyKey;
             if (x >= rg.x0) {
                 const uint64_t t = Tq[(size_t)y * wo + x];
-                key[c] = ((unsigned long long)((t >> 32) + (uint64_t)x) << 16) | (unsigned long long)x;
+                key = ((unsigned long long)((t >> 32) + (uint64_t)x) << 16) | (unsigned long long)x;
             }
+            const unsigned long long incl = umin64(warp_incl_min_rev(key, lane), local);
+            unsigned long long e = __shfl_down_sync(0xffffffffu, incl, 1);
+            if (lane == 31) e = local;
+            excl[c] = e;
+            local = __shfl_sync(0xffffffffu, incl, 0);
         }
+        if (lane == 0) s_min[warp] = local;
+        __syncthreads();
+        unsigned long long carry = round_carry;
+        for (int w2 = 0; w2 < warp; ++w2) carry = umin64(carry, s_min[w2]);
 #pragma unroll
         for (int c = 0; c < CB; ++c) {
             const int x = rg.x1 - (base + 32 * c + (31 - lane));
-            const unsigned long long incl = umin64(warp_incl_min_rev(key[c], lane), carry);
-            unsigned long long excl = __shfl_down_sync(0xffffffffu, incl, 1);
-            if (lane == 31) excl = carry;
-            if (x >= rg.x0) RR[(size_t)y * wo + x] = excl;
-            carry = __shfl_sync(0xffffffffu, incl, 0);
+            if (x >= rg.x0) RR[(size_t)y * wo + x] = umin64(excl[c], carry);
         }
+        for (int w2 = 0; w2 < ROW_WARPS; ++w2) round_carry = umin64(round_carry, s_min[w2]);
+        __syncthreads();
     }
 }
 
 // Sweep 1, columns (backward): for each hole p choose its sweep-1 source
 // and copy that pixel's codes (the fill of inpaint_color,
 // inpainting.cpp:191-198).
-template <class Src>
-__global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constant__ Src src) {
+template <class Src, bool PRE>
+__global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constant__ Src src, int G) {
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
@@ -354,9 +415,9 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constan
     const int x = rg.x0 + (int)blockIdx.x * 32 + lane;
     if (rg.x0 + (int)blockIdx.x * 32 > rg.x1) return;
     const bool col_ok = x <= rg.x1;
-    const int nrows = rg.y1 - rg.y0 + 1;
-    const int L = (nrows + 31) / 32;
-    const int yb = rg.y0 + w * L, ye = min(rg.y1, yb + L - 1);
+    const int nstrips = (rg.x1 - rg.x0 + 32) / 32;
+    const GroupRows gr = group_rows(rg, G, w);
+    const int yb = gr.yb, ye = gr.ye;
     // Keys: column part (T.d + y) << 16 | y (minimum y on ties);
     //       off-column (RR.d - x + y) << 32 | (0xffff - y) << 16 | qx
     //       (largest y, then smallest x on ties).
@@ -388,10 +449,28 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constan
     seg_col[w][lane] = mc;
     seg_off[w][lane] = mo;
     __syncthreads();
+    if (PRE) {
+        if (w == 0) {
+            unsigned long long tc = kEmptyKey, to = kEmptyKey;
+            for (int s = 0; s < 32; ++s) {
+                tc = umin64(tc, seg_col[s][lane]);
+                to = umin64(to, seg_off[s][lane]);
+            }
+            uint64_t* dst = im.seg + ((size_t)blockIdx.y * nstrips + blockIdx.x) * 64;
+            dst[lane] = tc;
+            dst[32 + lane] = to;
+        }
+        return;
+    }
     unsigned long long run_c = kEmptyKey, run_o = kEmptyKey;
     for (int s = w + 1; s < 32; ++s) {
         run_c = umin64(run_c, seg_col[s][lane]);
         run_o = umin64(run_o, seg_off[s][lane]);
+    }
+    for (int g = (int)blockIdx.y + 1; g < G; ++g) {
+        const uint64_t* src_seg = im.seg + ((size_t)g * nstrips + blockIdx.x) * 64;
+        run_c = umin64(run_c, src_seg[lane]);
+        run_o = umin64(run_o, src_seg[32 + lane]);
     }
     if (!col_ok) return;
     // Bottom-up over the segment in batches of RB rows.
@@ -484,28 +563,44 @@ __global__ void inpaint_write_kernel(const __grid_constant__ Src src) {
     out_v[co] = quarter_round(sv, ties_up);
 }
 
-// The five scan passes of `src` (grid z = images), sized for max_w x max_h.
+// The scan passes of `src` (grid z = images), sized for max_w x max_h.
+// The column passes split each 32-column strip into G row groups (one CTA
+// each) when the strips alone would not fill the device; a pre-pass then
+// stores every group's column minima.
 template <class Src>
-void launch_scans(const Src& src, int max_w, int max_h, int images, cudaStream_t s) {
-    const int rows_per_cta = 8;  // 8 warps of 32
-    inpaint_row0_kernel<<<dim3((max_h + rows_per_cta - 1) / rows_per_cta, 1, images), 256, 0, s>>>(src);
-    inpaint_col0_kernel<<<dim3((max_w + 31) / 32, 1, images), 1024, 0, s>>>(src);
+int launch_scans(const Src& src, int max_w, int max_h, int images, int G, cudaStream_t s) {
+    const int strips = (max_w + 31) / 32;
+    int launches = 0;
+    inpaint_row0_kernel<<<dim3(max_h, 1, images), 32 * ROW_WARPS, 0, s>>>(src);
+    if (G > 1) inpaint_col0_kernel<Src, true><<<dim3(strips, G, images), 1024, 0, s>>>(src, G);
+    inpaint_col0_kernel<Src, false><<<dim3(strips, G, images), 1024, 0, s>>>(src, G);
     inpaint_seed1_kernel<<<dim3((max_w + 255) / 256, max_h, images), 256, 0, s>>>(src);
-    inpaint_row1_kernel<<<dim3((max_h + rows_per_cta - 1) / rows_per_cta, 1, images), 256, 0, s>>>(src);
-    inpaint_col1_kernel<<<dim3((max_w + 31) / 32, 1, images), 1024, 0, s>>>(src);
+    inpaint_row1_kernel<<<dim3(max_h, 1, images), 32 * ROW_WARPS, 0, s>>>(src);
+    if (G > 1) inpaint_col1_kernel<Src, true><<<dim3(strips, G, images), 1024, 0, s>>>(src, G);
+    inpaint_col1_kernel<Src, false><<<dim3(strips, G, images), 1024, 0, s>>>(src, G);
+    launches = 5 + (G > 1 ? 2 : 0);
+    return launches;
+}
+
+// Row groups per strip for the column passes: about two CTAs per SM.
+int column_groups(int max_w, int images) {
+    const int strips = (max_w + 31) / 32;
+    const int want = (2 * 148 + strips * images - 1) / (strips * images);
+    return std::max(1, std::min(INPAINT_MAX_GROUPS, want));
 }
 
 }  // namespace
 
 template <class Tabs>
-void launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
+int launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
     const FromTables<Tabs> src{tabs};
-    launch_scans(src, sh.max_wo, sh.max_ho, sh.slots, s);
+    const int n = launch_scans(src, sh.max_wo, sh.max_ho, sh.slots, column_groups(sh.max_wo, sh.slots), s);
     inpaint_write_kernel<<<dim3((sh.max_wo / 2 + 127) / 128, (sh.max_ho + 1) / 2, sh.slots), 128, 0, s>>>(src);
+    return n + 1;
 }
 
-template void launch_inpaint<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);
-template void launch_inpaint<TablePtr>(const TablePtr&, const BatchShape&, cudaStream_t);
+template int launch_inpaint<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);
+template int launch_inpaint<TablePtr>(const TablePtr&, const BatchShape&, cudaStream_t);
 
 void launch_inpaint_scans(DevStatus* st, const uint8_t* holes, uint64_t* codes, uint64_t* const scan[4], int w,
                           int h, int32_t* sources, cudaStream_t s) {
@@ -517,9 +612,10 @@ void launch_inpaint_scans(DevStatus* st, const uint8_t* holes, uint64_t* codes, 
     src.im.codes = codes;
     for (int k = 0; k < 4; ++k) src.im.scan[k] = scan[k];
     src.im.sources = sources;
+    src.im.seg = nullptr;
     src.im.out_y = src.im.out_u = src.im.out_v = nullptr;
     src.im.ties_up = 0;
-    launch_scans(src, w, h, 1, s);
+    launch_scans(src, w, h, 1, 1, s);
 }
 
 }  // namespace rvsb

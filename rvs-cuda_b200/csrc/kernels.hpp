@@ -64,6 +64,19 @@ constexpr RasterVariant kRasterVariants[NUM_RASTER_VARIANTS] = {
 // dynamic shared memory); call before launching or capturing a batch.
 void prepare_kernels();
 
+// Colour planes of up to MAX_VIEWS views decoded in one launch.
+struct DecodeJob {
+    const uint16_t* y;
+    const uint16_t* u;
+    const uint16_t* v;
+    uint64_t* out;
+    int w, h;
+};
+struct DecodeJobs {
+    DecodeJob v[MAX_VIEWS];
+};
+void launch_decode_views(const DecodeJobs& jobs, int n, int max_w, int max_h, cudaStream_t s);
+
 // Decodes the colour planes of one input view into packed per-pixel words.
 void launch_decode_color(const uint16_t* y, const uint16_t* u, const uint16_t* v, int w, int h, uint64_t* out,
                          cudaStream_t s);

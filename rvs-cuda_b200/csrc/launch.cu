@@ -14,7 +14,7 @@ void launch_bin(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 template <class Tabs>
 void launch_raster(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 template <class Tabs>
-void launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
+int launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 template <class Tabs>
 void launch_aux(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 
@@ -60,12 +60,12 @@ int launch_batch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s, cudaEve
     launch_raster(tabs, sh, s);
     mark(5);
     mark(6);
-    launch_inpaint(tabs, sh, s);
+    const int inpaint_launches = launch_inpaint(tabs, sh, s);
     if (sh.aux) launch_aux(tabs, sh, s);
     mark(7);
     mark(9);
     if (cudaPeekAtLastError() != cudaSuccess) return -1;
-    return 1 + 1 + 3 + 1 + 6 + (sh.aux ? 1 : 0);
+    return 1 + 1 + 3 + 1 + inpaint_launches + (sh.aux ? 1 : 0);
 }
 
 template int launch_batch<TableParam>(const TableParam&, const BatchShape&, cudaStream_t, cudaEvent_t*);
