@@ -113,12 +113,22 @@ typedef enum rvsb_chroma_rounding {
     RVSB_CHROMA_TIES_UP = 1    /* OpenCV built without IPP */
 } rvsb_chroma_rounding;
 
-/* Synthesis options (Config, rvs/src/Config.hpp:172-205). */
+/* "BlendingMethod" (Pipeline::createBlender, rvs/src/Pipeline.cpp:347-361). */
+typedef enum rvsb_blending_method {
+    RVSB_BLEND_SIMPLE = 0,        /* BlendedViewSimple: quality^BlendingFactor weights */
+    RVSB_BLEND_MULTISPECTRAL = 1  /* BlendedViewMultiSpec: low and high frequencies
+                                     blended with their own factors */
+} rvsb_blending_method;
+
+/* Synthesis options (Config, rvs/src/Config.hpp:157-205). */
 typedef struct rvsb_synth_params {
     float blending_factor;    /* "BlendingFactor" (default 5); < 0 blends by maximum quality */
     float precision;          /* "Precision"; only 1 is supported */
     int32_t chroma_rounding;  /* rvsb_chroma_rounding; 0 unless set */
-    int32_t reserved;         /* must be 0 */
+    int32_t blending_method;  /* rvsb_blending_method; 0 unless set */
+    float low_freq_factor;    /* "BlendingLowFreqFactor" (Multispectral) */
+    float high_freq_factor;   /* "BlendingHighFreqFactor" (Multispectral) */
+    int32_t reserved[2];      /* must be 0 */
 } rvsb_synth_params;
 
 /* ----------------------------------------------------------------------- */

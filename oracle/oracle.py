@@ -39,6 +39,7 @@ def lib():
         P = ctypes.POINTER(abi.Camera)
         L.orc_set_trig_mode.argtypes = [ctypes.c_int]
         L.orc_set_chroma_round.argtypes = [ctypes.c_int]
+        L.orc_set_multispectral.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float]
         L.orc_decode_color.argtypes = [_U16, _U16, _U16, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F]
         L.orc_decode_depth.argtypes = [_U16, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                        ctypes.c_float, ctypes.c_int, _F]
@@ -77,6 +78,11 @@ def set_trig_mode(mode):
 def set_chroma_round(mode):
     """0: ties to even (OpenCV built with IPP), 1: ties up (without)."""
     lib().orc_set_chroma_round(int(mode))
+
+
+def set_multispectral(on, low=0.0, high=0.0):
+    """BlendingMethod Multispectral with the two factors (off: Simple)."""
+    lib().orc_set_multispectral(1 if on else 0, float(low), float(high))
 
 
 def decode_color(y, u, v, bits=10):

@@ -47,6 +47,10 @@ namespace {
 
 int g_trig_mode = 0;  // 0: correctly rounded float trig, 1: host libm float trig
 int g_chroma_round = 0;  // 0: ties to even (OpenCV with IPP), 1: ties up (without)
+// BlendingMethod Multispectral (BlendedViewMultiSpec, BlendedView.cpp:63-88):
+// on, BlendingLowFreqFactor, BlendingHighFreqFactor.
+int g_ms_on = 0;
+float g_ms_low = 0.f, g_ms_high = 0.f;
 
 // Rounded quarter of a 2x2 sum of uint16 samples (cv::resize 0.5 x 0.5).
 inline uint16_t quarter_round(unsigned s) {
@@ -145,6 +149,11 @@ extern "C" {
 
 void orc_set_trig_mode(int mode) { g_trig_mode = mode; }
 void orc_set_chroma_round(int mode) { g_chroma_round = mode; }
+void orc_set_multispectral(int on, float low, float high) {
+    g_ms_on = on;
+    g_ms_low = low;
+    g_ms_high = high;
+}
 
 /* Colour loader: image_loading.cpp:74-145 read_color_YUV, chroma upsample
  * resizeUV (process_input_frame.cu:22-81, srcX = x * (inW/outW), no
@@ -736,6 +745,51 @@ int orc_write_yuv420(const float* color, int w, int h, int bits, uint16_t* out) 
     return RVSB_OK;
 }
 
+/* calcBlurring of one channel (blending.cpp:62-105): box mean of the
+ * masked, finite values over [x - rad, x + rad] x [y - rad, y + rad]
+ * clipped to the image, from an integral image in double
+ * (IntegralImage2D<float, 1>, IntegralImage2D.h:735-770: the recurrence
+ * I(y+1, x+1) = I(y, x+1) + I(y+1, x) - I(y, x) + v); the window sum is
+ * truncated to an integer before the division by the count; 0 outside the
+ * mask.  src: channel 0 of a 3-channel image. */
+static void blur_channel0(const float* src, const uint8_t* mask, int w, int h, int rad, float* out) {
+    const size_t W1 = (size_t)w + 1;
+    std::vector<double> I(W1 * (h + 1), 0.0);
+    std::vector<unsigned> C(W1 * (h + 1), 0u);
+    for (int y = 0; y < h; ++y) {
+        double* prev = &I[(size_t)y * W1];
+        double* cur = prev + W1;
+        unsigned* cprev = &C[(size_t)y * W1];
+        unsigned* ccur = cprev + W1;
+        cur[0] = 0.0;
+        ccur[0] = 0;
+        for (int x = 0; x < w; ++x) {
+            cur[x + 1] = prev[x + 1] + cur[x] - prev[x];
+            ccur[x + 1] = cprev[x + 1] + ccur[x] - cprev[x];
+            const float v = src[((size_t)y * w + x) * 3];
+            if (mask[(size_t)y * w + x] == 255 && v == v && std::isfinite(v)) {
+                cur[x + 1] += v;
+                ccur[x + 1] += 1;
+            }
+        }
+    }
+    for (int i = 0; i < h; ++i)
+        for (int j = 0; j < w; ++j) {
+            float& o = out[(size_t)i * w + j];
+            if (mask[(size_t)i * w + j] == 0) {
+                o = 0.f;
+                continue;
+            }
+            const int sx = std::max(0, j - rad), sy = std::max(0, i - rad);
+            const int ex = std::min(j - rad + 2 * rad + 1, w), ey = std::min(i - rad + 2 * rad + 1, h);
+            const size_t ul = (size_t)sy * W1 + sx, ur = (size_t)sy * W1 + ex;
+            const size_t ll = (size_t)ey * W1 + sx, lr = (size_t)ey * W1 + ex;
+            const unsigned cnt = C[lr] + C[ul] - C[ur] - C[ll];
+            const unsigned sum = (unsigned)(int)(I[lr] + I[ul] - I[ur] - I[ll]);
+            o = cnt > 0 ? float(float(sum) / float(cnt)) : 0.f;
+        }
+}
+
 /* Depth of the blended view (BlendedView.cpp:205-208): the first view's
  * depth, then at every later view the view's depth where its quality is
  * larger than the accumulator's quality before the blend; validity is the
@@ -818,14 +872,46 @@ int orc_synthesize_aux(int n, const rvsb_camera* cams, const rvsb_view_planes* p
     std::vector<float> bc(no * 3), bq(no), prev_q(no), depth(no), validity(no);
     std::vector<uint8_t> acc_mask(no);
     const bool want_aux = out_mask || out_masked_yuv || out_depth || out_masked_depth;
+    // Multispectral: a second (high-frequency) blender beside the first.
+    std::vector<float> hc, hq;
+    std::vector<uint8_t> hmask;
+    std::vector<float> low, high, blur;
+    if (g_ms_on) {
+        hc.resize(no * 3);
+        hq.resize(no);
+        hmask.resize(no);
+        low.resize(no * 3);
+        high.resize(no * 3);
+        blur.resize(no);
+    }
     for (int v = 0; v < n; ++v) {
         if (want_aux) prev_q = bq;
-        blend_step(v, vcol[v].data(), vq[v].data(), vd[v].data(), no, exponent, bc.data(), bq.data(),
-                   acc_mask.data());
+        if (g_ms_on) {
+            // split_frequencies (blending.cpp:371-395), YUV: blur Y only;
+            // low = (blur(Y), U, V), high = colour - low.
+            std::vector<uint8_t> m(no);
+            for (size_t p = 0; p < no; ++p) m[p] = vq[v][p] > 0.f ? 255 : 0;
+            blur_channel0(vcol[v].data(), m.data(), wo, ho, std::max(wo, ho) / 20, blur.data());
+            for (size_t p = 0; p < no; ++p) {
+                low[p * 3 + 0] = blur[p];
+                low[p * 3 + 1] = vcol[v][p * 3 + 1];
+                low[p * 3 + 2] = vcol[v][p * 3 + 2];
+                for (int k = 0; k < 3; ++k) high[p * 3 + k] = vcol[v][p * 3 + k] - low[p * 3 + k];
+            }
+            blend_step(v, low.data(), vq[v].data(), vd[v].data(), no, g_ms_low, bc.data(), bq.data(),
+                       acc_mask.data());
+            blend_step(v, high.data(), vq[v].data(), vd[v].data(), no, g_ms_high, hc.data(), hq.data(),
+                       hmask.data());
+        } else {
+            blend_step(v, vcol[v].data(), vq[v].data(), vd[v].data(), no, exponent, bc.data(), bq.data(),
+                       acc_mask.data());
+        }
         if (want_aux)
             blend_depth_validity(v, prev_q.data(), vq[v].data(), vd[v].data(), vv[v].data(), no, depth.data(),
                                  validity.data());
     }
+    if (g_ms_on)
+        for (size_t p = 0; p < no * 3; ++p) bc[p] = bc[p] + hc[p];
     if (out_quality) std::memcpy(out_quality, bq.data(), no * sizeof(float));
     if (out_color) std::memcpy(out_color, bc.data(), no * 3 * sizeof(float));
     std::vector<float> filled(no * 3);

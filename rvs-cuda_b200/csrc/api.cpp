@@ -64,7 +64,13 @@ void validate_params(const rvsb_synth_params* p) {
     if (p->precision != 1.f) throw Unsupported("Precision other than 1 is not supported");
     if (p->chroma_rounding != RVSB_CHROMA_TIES_EVEN && p->chroma_rounding != RVSB_CHROMA_TIES_UP)
         throw ArgError("chroma_rounding must be RVSB_CHROMA_TIES_EVEN or RVSB_CHROMA_TIES_UP");
-    if (p->reserved != 0) throw ArgError("reserved synthesis parameter must be 0");
+    if (p->reserved[0] != 0 || p->reserved[1] != 0) throw ArgError("reserved synthesis parameters must be 0");
+    if (p->blending_method != RVSB_BLEND_SIMPLE && p->blending_method != RVSB_BLEND_MULTISPECTRAL)
+        throw ArgError("blending_method must be RVSB_BLEND_SIMPLE or RVSB_BLEND_MULTISPECTRAL");
+    if (p->blending_method == RVSB_BLEND_MULTISPECTRAL &&
+        (!std::isfinite(p->low_freq_factor) || p->low_freq_factor == 0.f || !std::isfinite(p->high_freq_factor) ||
+         p->high_freq_factor == 0.f))
+        throw Unsupported("Multispectral blending factors must be finite and nonzero");
 }
 
 void validate_request(const rvsb_scene* sc, const rvsb_camera* virt, const rvsb_synth_params* params,
@@ -585,6 +591,11 @@ void rvsb_config_synth_params(const rvsb_config* c, rvsb_synth_params* out) {
     out->blending_factor = c->cfg.blending_factor;
     out->precision = c->cfg.precision;
     out->chroma_rounding = RVSB_CHROMA_TIES_EVEN;
+    if (c->cfg.blending_method == "Multispectral") {
+        out->blending_method = RVSB_BLEND_MULTISPECTRAL;
+        out->low_freq_factor = c->cfg.blending_low_freq_factor;
+        out->high_freq_factor = c->cfg.blending_high_freq_factor;
+    }
 }
 
 rvsb_status rvsb_config_virtual_camera_at(const rvsb_config* c, int i, int frame, rvsb_camera* out) {

@@ -108,6 +108,21 @@ struct AuxPtrs {
     int pad;
 };
 
+// Multispectral blending (BlendedViewMultiSpec, BlendedView.cpp:63-88): the
+// raster stores every view's resolved colour and quality, the blur kernels
+// the masked box mean of each view's luma, and the blend kernel the two
+// frequency bands' blends.  Per view, npix = Wo*Ho entries each.
+struct MsPtrs {
+    float4* view;       // (Y, U, V, quality) per view and pixel
+    double* hsum;       // row-window sums of masked luma
+    int* hcnt;          // row-window counts of masked pixels
+    float* blur;        // blurred luma (0 outside the mask)
+    int on;
+    int rad;            // window radius: max(Wo, Ho) / 20
+    float low_exp, high_exp;
+    int low_int, high_int;  // integer exponents in [2, 16] (0 otherwise)
+};
+
 // Device buffers of one slot's workspace.
 struct SlotBuffers {
     DevStatus* status;   // 1 entry
@@ -138,6 +153,7 @@ struct SlotTable {
     uint16_t* out_v;
     DebugPtrs dbg;
     AuxPtrs aux;
+    MsPtrs ms;
     DevView v[MAX_VIEWS];
 };
 

@@ -118,6 +118,17 @@ void SlotWorkspace::ensure_aux(rvsb_context* ctx, int wo, int ho) {
     }
 }
 
+void SlotWorkspace::ensure_ms(rvsb_context* ctx, int n_views, int wo, int ho) {
+    const size_t n = (size_t)n_views * wo * ho;
+    if (n > cap_ms) {
+        ms_view.alloc(ctx, n * sizeof(float4));
+        ms_hsum.alloc(ctx, n * sizeof(double));
+        ms_hcnt.alloc(ctx, n * sizeof(int));
+        ms_blur.alloc(ctx, n * sizeof(float));
+        cap_ms = n;
+    }
+}
+
 BatchCore::BatchCore(rvsb_context* ctx, int slots) : ctx_(ctx), slots_(slots) {
     if (slots <= 0) throw ArgError("a batch needs at least one slot");
     prepare_kernels();
@@ -241,6 +252,28 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
         D.blend_exp_int = (int)p.blending_factor;
     D.chroma_ties_up = p.chroma_rounding == RVSB_CHROMA_TIES_UP;
     D.blend_max = p.blending_factor < 0.f ? 1 : 0;
+    auto exp_int = [](float e) {
+        return (e == std::floor(e) && e >= 2.f && e <= 16.f) ? (int)e : 0;
+    };
+    if (p.blending_method == RVSB_BLEND_MULTISPECTRAL) {
+        // The raster's own blend follows the low band: its quality, holes,
+        // depth and validity are the multispectral blender's.
+        D.blend_exp = p.low_freq_factor;
+        D.inv_blend_exp = 1.0f / p.low_freq_factor;
+        D.blend_exp_int = exp_int(p.low_freq_factor);
+        D.blend_max = p.low_freq_factor < 0.f ? 1 : 0;
+        MsPtrs& M = T.ms;
+        M.view = ws.ms_view.as<float4>();
+        M.hsum = ws.ms_hsum.as<double>();
+        M.hcnt = ws.ms_hcnt.as<int>();
+        M.blur = ws.ms_blur.as<float>();
+        M.on = 1;
+        M.rad = std::max(virt.width, virt.height) / 20;
+        M.low_exp = p.low_freq_factor;
+        M.high_exp = p.high_freq_factor;
+        M.low_int = exp_int(p.low_freq_factor);
+        M.high_int = exp_int(p.high_freq_factor);
+    }
     const RasterVariant& rv = kRasterVariants[variant];
     D.tile_wl = log2i(rv.tw);
     D.tile_hl = log2i(rv.th);
@@ -286,8 +319,10 @@ BatchShape BatchCore::shape_of(const SlotRequest* reqs, int n, int variant) cons
     BatchShape sh;
     sh.slots = n;
     sh.variant = variant;
-    for (int k = 0; k < n; ++k)
+    for (int k = 0; k < n; ++k) {
         if (reqs[k].aux) sh.aux = 1;
+        if (reqs[k].params.blending_method == RVSB_BLEND_MULTISPECTRAL) sh.ms = 1;
+    }
     for (int k = 0; k < n; ++k) {
         const SlotRequest& r = reqs[k];
         const int nv = (int)r.scene->cams.size();
@@ -327,7 +362,7 @@ int BatchCore::launch_variant(const SlotRequest* reqs, int n, int variant, cudaS
     const TablePtr tabs{tables_.as<SlotTable>()};
     if (use_graphs_ && !profiling_) {
         const std::vector<int> key = {sh.slots,  sh.variant, sh.max_views, sh.max_w,    sh.max_h,
-                                      sh.max_blocks, sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins, sh.aux};
+                                      sh.max_blocks, sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins, sh.aux, sh.ms};
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {
             cudaGraph_t g = nullptr;
@@ -377,10 +412,17 @@ int BatchCore::tune(const SlotRequest* reqs, int n, cudaStream_t s) {
 int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
     if (n <= 0 || n > slots_) throw ArgError("batch of " + std::to_string(n) + " requests for " +
                                              std::to_string(slots_) + " slots");
+    int ms_wo = 0;
     for (int k = 0; k < n; ++k) {
-        ws_[k]->ensure(ctx_, reqs[k].scene, reqs[k].virt.width, reqs[k].virt.height);
-        if (reqs[k].aux) ws_[k]->ensure_aux(ctx_, reqs[k].virt.width, reqs[k].virt.height);
+        const SlotRequest& r = reqs[k];
+        ws_[k]->ensure(ctx_, r.scene, r.virt.width, r.virt.height);
+        if (r.aux) ws_[k]->ensure_aux(ctx_, r.virt.width, r.virt.height);
+        if (r.params.blending_method == RVSB_BLEND_MULTISPECTRAL) {
+            ws_[k]->ensure_ms(ctx_, (int)r.scene->cams.size(), r.virt.width, r.virt.height);
+            ms_wo = std::max(ms_wo, r.virt.width);
+        }
     }
+    if (ms_wo > 0) prepare_ms_kernels(ms_wo);
     int variant = 0;
     if (forced_variant_ >= 0) {
         variant = forced_variant_;

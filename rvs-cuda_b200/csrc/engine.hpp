@@ -70,6 +70,9 @@ struct SlotWorkspace {
     DevMem status, counts, offsets, cursor, list, codes, holes, scan[4], vert, bbox;
     DevMem aux_depth, aux_valid;  // blended depth / validity (auxiliary outputs only)
     DevMem inpaint_seg;           // column-group minima of the inpainting passes
+    DevMem ms_view, ms_hsum, ms_hcnt, ms_blur;  // multispectral blending only
+    size_t cap_ms = 0;            // view-pixels the multispectral buffers hold
+    void ensure_ms(rvsb_context* ctx, int n_views, int wo, int ho);
     size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0, cap_aux = 0, cap_strips = 0;
     void ensure_aux(rvsb_context* ctx, int wo, int ho);
 

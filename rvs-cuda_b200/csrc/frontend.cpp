@@ -387,9 +387,8 @@ Config load_config(const std::string& path) {
     if (auto n = root.optional("BlendingMethod")) c.blending_method = n.asString();
     if (auto n = root.optional("BlendingFactor")) c.blending_factor = (float)n.asDouble();
     if (c.blending_method == "Multispectral") {
-        root.require("BlendingLowFreqFactor").asDouble();
-        root.require("BlendingHighFreqFactor").asDouble();
-        throw Unsupported("BlendingMethod Multispectral is not supported");
+        c.blending_low_freq_factor = (float)root.require("BlendingLowFreqFactor").asDouble();
+        c.blending_high_freq_factor = (float)root.require("BlendingHighFreqFactor").asDouble();
     }
     if (c.blending_method != "Simple")
         throw ConfigError("Unknown view blending method \"" + c.blending_method + "\"");

@@ -88,6 +88,8 @@ struct Config {
     float validity_threshold = 5000.f;
     std::string vs_method = "Triangles";
     std::string blending_method = "Simple";
+    float blending_low_freq_factor = 0.f;
+    float blending_high_freq_factor = 0.f;
     float blending_factor = 5.f;
     int start_frame = 0;
     int number_of_frames = 1;

@@ -13,6 +13,7 @@ struct BatchShape {
     int slots = 0;
     int variant = 0;         // raster variant (kRasterVariants)
     int aux = 0;             // some slot wants auxiliary outputs
+    int ms = 0;              // some slot blends multispectrally
     int max_views = 0;       // largest n_views
     int max_w = 0, max_h = 0;  // largest input view
     int max_blocks = 0;      // largest nbx * nby of an input view
@@ -63,6 +64,8 @@ constexpr RasterVariant kRasterVariants[NUM_RASTER_VARIANTS] = {
 // One-time kernel attributes of the current device (the raster kernel's
 // dynamic shared memory); call before launching or capturing a batch.
 void prepare_kernels();
+// Shared memory of the multispectral row sums for outputs up to max_wo wide.
+void prepare_ms_kernels(int max_wo);
 
 // Colour planes of up to MAX_VIEWS views decoded in one launch.
 struct DecodeJob {

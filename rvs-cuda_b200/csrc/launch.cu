@@ -17,6 +17,8 @@ template <class Tabs>
 int launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 template <class Tabs>
 void launch_aux(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
+template <class Tabs>
+int launch_ms(const Tabs& tabs, const BatchShape& sh, cudaStream_t s);
 
 namespace {
 
@@ -58,6 +60,7 @@ int launch_batch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s, cudaEve
     mark(3);
     mark(4);
     launch_raster(tabs, sh, s);
+    const int ms_launches = sh.ms ? launch_ms(tabs, sh, s) : 0;
     mark(5);
     mark(6);
     const int inpaint_launches = launch_inpaint(tabs, sh, s);
@@ -65,7 +68,7 @@ int launch_batch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s, cudaEve
     mark(7);
     mark(9);
     if (cudaPeekAtLastError() != cudaSuccess) return -1;
-    return 1 + 1 + 3 + 1 + inpaint_launches + (sh.aux ? 1 : 0);
+    return 1 + 1 + 3 + 1 + ms_launches + inpaint_launches + (sh.aux ? 1 : 0);
 }
 
 template int launch_batch<TableParam>(const TableParam&, const BatchShape&, cudaStream_t, cudaEvent_t*);

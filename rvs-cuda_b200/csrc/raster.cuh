@@ -244,6 +244,7 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
             const int v = g0 + k;
             const Fragment f = resolve_fragment(tab.v[v], zb[k][p], x, y);
             const float qv = __fdiv_rn(f.validity, f.depth);
+            if (tab.ms.on) tab.ms.view[(size_t)v * npo + po] = make_float4(f.col.x, f.col.y, f.col.z, qv);
             if (aux) {
                 // BlendedView.cpp:205-208: the view's depth where its quality
                 // beats the accumulator's before this blend (view 0: its

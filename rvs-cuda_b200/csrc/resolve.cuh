@@ -68,24 +68,25 @@ struct BlendAcc {
 // weight sum itself: the reference re-powers its stored sum^(1/exp) by exp,
 // which returns the sum up to a few ulp, and quality > 0 exactly when the
 // sum is > 0.
-__device__ __forceinline__ void blend_view(BlendAcc& a, int v, const Fragment& f, float qv, const DevTarget& T) {
+__device__ __forceinline__ void blend_view(BlendAcc& a, int v, float3 col, float qv, float blend_exp, int exp_int,
+                                           bool by_max) {
     if (v == 0) {
-        a.c0 = f.col.x;
-        a.c1 = f.col.y;
-        a.c2 = f.col.z;
+        a.c0 = col.x;
+        a.c1 = col.y;
+        a.c2 = col.z;
         a.q = qv;
         return;
     }
-    if (T.blend_max) {
+    if (by_max) {
         // blend_img_by_max (blending.cpp:293-308): the empty colour and
         // quality 0, replaced by the accumulator where its quality is
         // positive, then by the view where its quality is larger still.
         BlendAcc r = {0.f, 1.f, 0.f, 0.f};
         if (a.q > r.q) r = a;
         if (qv > r.q) {
-            r.c0 = f.col.x;
-            r.c1 = f.col.y;
-            r.c2 = f.col.z;
+            r.c0 = col.x;
+            r.c1 = col.y;
+            r.c2 = col.z;
             r.q = qv;
         }
         a = r;
@@ -93,18 +94,18 @@ __device__ __forceinline__ void blend_view(BlendAcc& a, int v, const Fragment& f
     }
     float sum = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     if (a.q > 0.f) {
-        const float w = v == 1 ? blend_pow(a.q, T.blend_exp, T.blend_exp_int) : a.q;
+        const float w = v == 1 ? blend_pow(a.q, blend_exp, exp_int) : a.q;
         sum = __fadd_rn(sum, w);
         c0 = __fadd_rn(c0, __fmul_rn(w, a.c0));
         c1 = __fadd_rn(c1, __fmul_rn(w, a.c1));
         c2 = __fadd_rn(c2, __fmul_rn(w, a.c2));
     }
     if (qv > 0.f) {
-        const float w = blend_pow(qv, T.blend_exp, T.blend_exp_int);
+        const float w = blend_pow(qv, blend_exp, exp_int);
         sum = __fadd_rn(sum, w);
-        c0 = __fadd_rn(c0, __fmul_rn(w, f.col.x));
-        c1 = __fadd_rn(c1, __fmul_rn(w, f.col.y));
-        c2 = __fadd_rn(c2, __fmul_rn(w, f.col.z));
+        c0 = __fadd_rn(c0, __fmul_rn(w, col.x));
+        c1 = __fadd_rn(c1, __fmul_rn(w, col.y));
+        c2 = __fadd_rn(c2, __fmul_rn(w, col.z));
     }
     if (sum == 0.f) {
         a.c0 = 0.f; a.c1 = 1.f; a.c2 = 0.f;
@@ -116,6 +117,10 @@ __device__ __forceinline__ void blend_view(BlendAcc& a, int v, const Fragment& f
         a.c2 = __fmul_rn(c2, inv);
         a.q = sum;
     }
+}
+
+__device__ __forceinline__ void blend_view(BlendAcc& a, int v, const Fragment& f, float qv, const DevTarget& T) {
+    blend_view(a, v, f.col, qv, T.blend_exp, T.blend_exp_int, T.blend_max != 0);
 }
 
 }  // namespace dev

@@ -247,7 +247,8 @@ rvsb_status rvsb_server_submit(rvsb_server* s, int scene_id, const rvsb_camera* 
         return RVSB_E_ARG;
     }
     if (!std::isfinite(params->blending_factor) || params->blending_factor == 0.f || params->precision != 1.f ||
-        params->reserved != 0 ||
+        params->reserved[0] != 0 || params->reserved[1] != 0 ||
+        (params->blending_method != RVSB_BLEND_SIMPLE && params->blending_method != RVSB_BLEND_MULTISPECTRAL) ||
         (params->chroma_rounding != RVSB_CHROMA_TIES_EVEN && params->chroma_rounding != RVSB_CHROMA_TIES_UP))
         return RVSB_E_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(s->mu);

@@ -142,11 +142,19 @@ CHROMA_TIES_EVEN = 0  # output chroma rounding of OpenCV built with IPP
 CHROMA_TIES_UP = 1    # ... and without it
 
 
-def params(blending_factor=5.0, precision=1.0, chroma_rounding=CHROMA_TIES_EVEN):
+BLEND_SIMPLE, BLEND_MULTISPECTRAL = 0, 1
+
+
+def params(blending_factor=5.0, precision=1.0, chroma_rounding=CHROMA_TIES_EVEN, multispectral=None):
+    """Synthesis options; multispectral=(low, high) selects BlendingMethod
+    Multispectral with those factors."""
     p = SynthParams()
     p.blending_factor = blending_factor
     p.precision = precision
     p.chroma_rounding = chroma_rounding
+    if multispectral is not None:
+        p.blending_method = BLEND_MULTISPECTRAL
+        p.low_freq_factor, p.high_freq_factor = multispectral
     return p
 
 

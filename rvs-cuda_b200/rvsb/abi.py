@@ -82,7 +82,10 @@ class SynthParams(ctypes.Structure):
         ("blending_factor", ctypes.c_float),
         ("precision", ctypes.c_float),
         ("chroma_rounding", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("blending_method", ctypes.c_int32),
+        ("low_freq_factor", ctypes.c_float),
+        ("high_freq_factor", ctypes.c_float),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 

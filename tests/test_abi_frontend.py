@@ -36,7 +36,7 @@ def test_struct_sizes_match_header():
     assert ctypes.sizeof(abi.Camera) == 8 * 4 + 16 * 4
     assert ctypes.sizeof(abi.ViewPlanes) == 4 * ctypes.sizeof(ctypes.c_void_p)
     assert ctypes.sizeof(abi.Yuv420) == 3 * ctypes.sizeof(ctypes.c_void_p)
-    assert ctypes.sizeof(abi.SynthParams) == 16
+    assert ctypes.sizeof(abi.SynthParams) == 32
 
 
 def test_status_strings_and_stage_names():
@@ -224,7 +224,7 @@ def test_pose_trace_bad_header(tmp_path, monkeypatch):
 
 @pytest.mark.parametrize("over,status", [
     (dict(Precision=2.0), 7),
-    (dict(BlendingMethod="Multispectral", BlendingLowFreqFactor=1.0, BlendingHighFreqFactor=4.0), 7),
+    (dict(BlendingMethod="Multispectral", BlendingLowFreqFactor=1.0), 2),
     (dict(BlendingMethod="Median"), 2),
     (dict(ViewSynthesisMethod="Squares"), 2),
     (dict(Version="1.0"), 2),
