@@ -123,7 +123,9 @@ typedef enum rvsb_blending_method {
 /* Synthesis options (Config, rvs/src/Config.hpp:157-205). */
 typedef struct rvsb_synth_params {
     float blending_factor;    /* "BlendingFactor" (default 5); < 0 blends by maximum quality */
-    float precision;          /* "Precision"; only 1 is supported */
+    float precision;          /* "Precision" P > 0 (Config.cpp:389-399): rasterise at
+                                 int(0.5 + W*P) x int(0.5 + H*P), which must be even,
+                                 and resize to W x H when written; 1 unless set */
     int32_t chroma_rounding;  /* rvsb_chroma_rounding; 0 unless set */
     int32_t blending_method;  /* rvsb_blending_method; 0 unless set */
     float low_freq_factor;    /* "BlendingLowFreqFactor" (Multispectral) */
@@ -270,7 +272,8 @@ rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, i
 
 /* Intermediate results of one synthesis, for stage-by-stage checks against
  * the reference's CPU path.  Every pointer is a device pointer and may be
- * NULL; n = number of input views, W,H = input size, Wo,Ho = output size.
+ * NULL; n = number of input views, W,H = input size, Wo,Ho = raster size (the
+ * output size, or int(0.5 + Wout*P) x int(0.5 + Hout*P) for Precision P != 1).
  *   warped_uvz:    n*H*W*4 floats, (u, v, virtual depth, 0) per input pixel
  *                  (SynthesizedView::computeBasicMode, SynthesizedView.cpp:320-331)
  *   view_color:    n*Ho*Wo*3 floats, raster colour of each view
@@ -320,7 +323,8 @@ typedef struct rvsb_aux_out {
     int32_t reserved;
 } rvsb_aux_out;
 
-/* rvsb_synthesize plus the auxiliary outputs. */
+/* rvsb_synthesize plus the auxiliary outputs; Precision 1 only
+ * (RVSB_E_UNSUPPORTED otherwise). */
 rvsb_status rvsb_synthesize_aux(rvsb_scene* scene, const rvsb_camera* virt, const rvsb_synth_params* params,
                                 const rvsb_yuv420* out, const rvsb_aux_out* aux, void* stream);
 

@@ -40,6 +40,8 @@ def lib():
         L.orc_set_trig_mode.argtypes = [ctypes.c_int]
         L.orc_set_chroma_round.argtypes = [ctypes.c_int]
         L.orc_set_multispectral.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float]
+        L.orc_set_precision.argtypes = [ctypes.c_float]
+        L.orc_resize_linear3.argtypes = [_F, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, ctypes.c_int]
         L.orc_decode_color.argtypes = [_U16, _U16, _U16, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F]
         L.orc_decode_depth.argtypes = [_U16, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                        ctypes.c_float, ctypes.c_int, _F]
@@ -78,6 +80,32 @@ def set_trig_mode(mode):
 def set_chroma_round(mode):
     """0: ties to even (OpenCV built with IPP), 1: ties up (without)."""
     lib().orc_set_chroma_round(int(mode))
+
+
+_precision = np.float32(1.0)
+
+
+def set_precision(p):
+    """'Precision': rasterise at P times the output size, resize when written."""
+    global _precision
+    _precision = np.float32(p)
+    lib().orc_set_precision(float(p))
+
+
+def raster_size(w, h):
+    """(int(0.5 + W * P), int(0.5 + H * P)) in float, as SynthesizedView.cpp:327-329."""
+    if _precision == np.float32(1.0):
+        return w, h
+    return (int(np.float32(0.5) + np.float32(w) * _precision), int(np.float32(0.5) + np.float32(h) * _precision))
+
+
+def resize_linear3(img, w, h):
+    """cv::resize(img, (w, h)) with INTER_LINEAR of an HxWx3 float32 image
+    (the output resize of write_color, image_writing.cpp:188-190)."""
+    src = np.ascontiguousarray(img, np.float32)
+    dst = np.empty((h, w, 3), np.float32)
+    lib().orc_resize_linear3(_p(src, _F), src.shape[1], src.shape[0], _p(dst, _F), w, h)
+    return dst
 
 
 def set_multispectral(on, low=0.0, high=0.0):
@@ -202,8 +230,9 @@ def synthesize(inputs, planes, virt, exponent, want_intermediate=False):
         vp[i].y, vp[i].u, vp[i].v, vp[i].depth = (a.ctypes.data for a in arrs)
     wo, ho = virt.width, virt.height
     out = np.empty(wo * ho * 3 // 2, np.uint16)
-    q = np.empty((ho, wo), np.float32) if want_intermediate else None
-    c = np.empty((ho, wo, 3), np.float32) if want_intermediate else None
+    rw, rh = raster_size(wo, ho)
+    q = np.empty((rh, rw), np.float32) if want_intermediate else None
+    c = np.empty((rh, rw, 3), np.float32) if want_intermediate else None
     rc = lib().orc_synthesize(n, cams, vp, ctypes.byref(virt), float(exponent), _p(out, _U16),
                               _p(q, _F) if q is not None else None,
                               _p(c, _F) if c is not None else None)

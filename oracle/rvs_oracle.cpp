@@ -51,6 +51,8 @@ int g_chroma_round = 0;  // 0: ties to even (OpenCV with IPP), 1: ties up (witho
 // on, BlendingLowFreqFactor, BlendingHighFreqFactor.
 int g_ms_on = 0;
 float g_ms_low = 0.f, g_ms_high = 0.f;
+// "Precision" (detail::g_rescale, Config.cpp:389-399).
+float g_precision = 1.f;
 
 // Rounded quarter of a 2x2 sum of uint16 samples (cv::resize 0.5 x 0.5).
 inline uint16_t quarter_round(unsigned s) {
@@ -149,6 +151,7 @@ extern "C" {
 
 void orc_set_trig_mode(int mode) { g_trig_mode = mode; }
 void orc_set_chroma_round(int mode) { g_chroma_round = mode; }
+void orc_set_precision(float p) { g_precision = p; }
 void orc_set_multispectral(int on, float low, float high) {
     g_ms_on = on;
     g_ms_low = low;
@@ -455,7 +458,7 @@ void colorize_triangle(RasterState& st, int ax, int ay, int bx, int by, int cx, 
     const float* C = st.uv + ic * 2;
     float den = (B[1] - C[1]) * (A[0] - C[0]) + (C[0] - B[0]) * (A[1] - C[1]);
     if (den <= 0.f) return;
-    float triangle_validity = valid_tri(A, B, C, 1.f);
+    float triangle_validity = valid_tri(A, B, C, g_precision);
     if (triangle_validity == 0.f) return;
 
     int Xmin = imax(0, cvt_trunc_i32(std::floor(smin(smin(A[0], B[0]), C[0]))));
@@ -790,6 +793,72 @@ static void blur_channel0(const float* src, const uint8_t* mask, int w, int h, i
         }
 }
 
+/* cv::resize(src, dst, dsize) with INTER_LINEAR on a 3-channel float image
+ * (imgproc resize.cpp): an exact 2x reduction takes the area fast path,
+ * ((a + b) + c + d) * 0.25 over each 2x2 block; otherwise bilinear with
+ * source coordinate (d + 0.5) * scale - 0.5, weights (1 - f, f) in float,
+ * coordinates clamped to the first and last pixel (weight 0 beyond), a
+ * horizontal pass per source row and a vertical pass. */
+static void resize_linear3(const float* src, int ws, int hs, float* dst, int wd, int hd) {
+    const double scale_x = 1.0 / ((double)wd / ws), scale_y = 1.0 / ((double)hd / hs);
+    const int iscale_x = (int)std::lrint(scale_x), iscale_y = (int)std::lrint(scale_y);
+    const bool area_fast = std::fabs(scale_x - iscale_x) < 2.220446049250313e-16 &&
+                           std::fabs(scale_y - iscale_y) < 2.220446049250313e-16;
+    if (area_fast && iscale_x == 2 && iscale_y == 2) {
+        for (int y = 0; y < hd; ++y)
+            for (int x = 0; x < wd; ++x)
+                for (int k = 0; k < 3; ++k) {
+                    const float a = src[((size_t)(2 * y) * ws + 2 * x) * 3 + k];
+                    const float b = src[((size_t)(2 * y) * ws + 2 * x + 1) * 3 + k];
+                    const float c = src[((size_t)(2 * y + 1) * ws + 2 * x) * 3 + k];
+                    const float d = src[((size_t)(2 * y + 1) * ws + 2 * x + 1) * 3 + k];
+                    dst[((size_t)y * wd + x) * 3 + k] = (((a + b) + c) + d) * 0.25f;
+                }
+        return;
+    }
+    auto coord = [](int d, double scale, int n, int& s0, float& f) {
+        f = (float)((d + 0.5) * scale - 0.5);
+        int s = (int)std::floor(f);
+        f -= (float)s;
+        if (s < 0) {
+            f = 0.f;
+            s = 0;
+        }
+        if (s >= n - 1) {
+            f = 0.f;
+            s = n - 1;
+        }
+        s0 = s;
+    };
+    std::vector<float> rows((size_t)hs * wd * 3);
+    for (int x = 0; x < wd; ++x) {
+        int sx;
+        float fx;
+        coord(x, scale_x, ws, sx, fx);
+        const float a0 = 1.f - fx, a1 = fx;
+        const int sx1 = std::min(sx + 1, ws - 1);
+        for (int y = 0; y < hs; ++y)
+            for (int k = 0; k < 3; ++k)
+                rows[((size_t)y * wd + x) * 3 + k] =
+                    src[((size_t)y * ws + sx) * 3 + k] * a0 + src[((size_t)y * ws + sx1) * 3 + k] * a1;
+    }
+    for (int y = 0; y < hd; ++y) {
+        int sy;
+        float fy;
+        coord(y, scale_y, hs, sy, fy);
+        const float b0 = 1.f - fy, b1 = fy;
+        const int sy1 = std::min(sy + 1, hs - 1);
+        for (int x = 0; x < wd; ++x)
+            for (int k = 0; k < 3; ++k)
+                dst[((size_t)y * wd + x) * 3 + k] =
+                    rows[((size_t)sy * wd + x) * 3 + k] * b0 + rows[((size_t)sy1 * wd + x) * 3 + k] * b1;
+    }
+}
+
+extern "C" void orc_resize_linear3(const float* src, int ws, int hs, float* dst, int wd, int hd) {
+    resize_linear3(src, ws, hs, dst, wd, hd);
+}
+
 /* Depth of the blended view (BlendedView.cpp:205-208): the first view's
  * depth, then at every later view the view's depth where its quality is
  * larger than the accumulator's quality before the blend; validity is the
@@ -844,7 +913,15 @@ int orc_synthesize_aux(int n, const rvsb_camera* cams, const rvsb_view_planes* p
                        float* out_color, float threshold, uint8_t* out_mask, uint16_t* out_masked_yuv,
                        uint16_t* out_depth, uint16_t* out_masked_depth) {
     if (n <= 0 || !cams || !planes || !vt || !out_yuv) return RVSB_E_ARG;
-    const int wo = vt->width, ho = vt->height;
+    // Precision: rasterise at (int(0.5 + W * P), int(0.5 + H * P))
+    // (SynthesizedView.cpp:325-333); the colour is resized to W x H when
+    // written (image_writing.cpp:188-190).
+    const float P = g_precision;
+    const bool rescale = P != 1.f;
+    if (rescale && (out_mask || out_masked_yuv || out_depth || out_masked_depth)) return RVSB_E_UNSUPPORTED;
+    const int wo = rescale ? (int)(0.5f + vt->width * P) : vt->width;
+    const int ho = rescale ? (int)(0.5f + vt->height * P) : vt->height;
+    const float sxu = (float)wo / vt->width, syv = (float)ho / vt->height;
     const size_t no = (size_t)wo * ho;
     std::vector<std::vector<float>> vcol(n), vq(n), vd(n), vv(n);
     for (int v = 0; v < n; ++v) {
@@ -859,6 +936,12 @@ int orc_synthesize_aux(int n, const rvsb_camera* cams, const rvsb_view_planes* p
         if (rc) return rc;
         int wrap = 0;
         orc_warp(&c, vt, dep.data(), uv.data(), vdep.data(), &wrap);
+        if (rescale)  // cv::transform with Matx22f(sx, 0, 0, sy)
+            for (size_t p = 0; p < ni; ++p) {
+                const float u = uv[p * 2], w = uv[p * 2 + 1];
+                uv[p * 2] = sxu * u + 0.f * w;
+                uv[p * 2 + 1] = 0.f * u + syv * w;
+            }
         vcol[v].resize(no * 3);
         vd[v].resize(no);
         vq[v].resize(no);
@@ -916,6 +999,11 @@ int orc_synthesize_aux(int n, const rvsb_camera* cams, const rvsb_view_planes* p
     if (out_color) std::memcpy(out_color, bc.data(), no * 3 * sizeof(float));
     std::vector<float> filled(no * 3);
     orc_inpaint(bc.data(), bq.data(), wo, ho, filled.data(), nullptr, nullptr);
+    if (rescale) {
+        std::vector<float> small((size_t)vt->width * vt->height * 3);
+        resize_linear3(filled.data(), wo, ho, small.data(), vt->width, vt->height);
+        return orc_write_yuv420(small.data(), vt->width, vt->height, vt->bit_depth_color, out_yuv);
+    }
     int rc = orc_write_yuv420(filled.data(), wo, ho, vt->bit_depth_color, out_yuv);
     if (rc) return rc;
     std::vector<uint8_t> mask(no);

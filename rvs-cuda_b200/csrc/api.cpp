@@ -61,7 +61,7 @@ void validate_params(const rvsb_synth_params* p) {
     if (!p) throw ArgError("null synthesis parameters");
     if (!std::isfinite(p->blending_factor) || p->blending_factor == 0.f)
         throw Unsupported("BlendingFactor must be a finite nonzero number (negative: blend by maximum)");
-    if (p->precision != 1.f) throw Unsupported("Precision other than 1 is not supported");
+    if (!std::isfinite(p->precision) || !(p->precision > 0.f)) throw Unsupported("Precision must be positive");
     if (p->chroma_rounding != RVSB_CHROMA_TIES_EVEN && p->chroma_rounding != RVSB_CHROMA_TIES_UP)
         throw ArgError("chroma_rounding must be RVSB_CHROMA_TIES_EVEN or RVSB_CHROMA_TIES_UP");
     if (p->reserved[0] != 0 || p->reserved[1] != 0) throw ArgError("reserved synthesis parameters must be 0");
@@ -78,6 +78,7 @@ void validate_request(const rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
     if (!virt || !out || !out->y || !out->u || !out->v) throw ArgError("null camera or output planes");
     validate_params(params);
     if (const char* why = camera_problem(*virt, true)) throw ArgError(std::string("virtual camera: ") + why);
+    raster_dims(*virt, *params);
     (void)sc;
 }
 

@@ -98,6 +98,13 @@ __device__ __forceinline__ float4 warp_vertex(const DevView& V, const DevTarget&
             u = v = z = qnan();
         }
     }
+    if (T.rescale) {
+        // cv::transform with Matx22f(sx, 0, 0, sy) (SynthesizedView.cpp:330-331)
+        const float su = __fadd_rn(__fmul_rn(T.uv_sx, u), __fmul_rn(0.f, v));
+        const float sv = __fadd_rn(__fmul_rn(0.f, u), __fmul_rn(T.uv_sy, v));
+        u = su;
+        v = sv;
+    }
     return make_float4(u, v, z, 0.f);
 }
 
@@ -109,9 +116,11 @@ __device__ __forceinline__ double sq_len(float ax, float ay, float bx, float by)
     const double dx = (double)__fsub_rn(ax, bx), dy = (double)__fsub_rn(ay, by);
     return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
 }
-__device__ __forceinline__ float tri_quality(float ax, float ay, float bx, float by, float cx, float cy) {
+__device__ __forceinline__ float tri_quality(float ax, float ay, float bx, float by, float cx, float cy,
+                                            float precision = 1.f) {
     const double m = fmax(sq_len(bx, by, cx, cy), fmax(sq_len(ax, ay, bx, by), sq_len(ax, ay, cx, cy)));
-    const float stretch = (float)__dsqrt_rn(m);
+    float stretch = (float)__dsqrt_rn(m);
+    if (precision != 1.f) stretch = __fdiv_rn(stretch, precision);  // stretch /= g_rescale
     float q = __fsub_rn(10000.f, __fmul_rn(1000.f, stretch));
     q = smax(1.f, q);
     q = smin(10000.f, q);

@@ -56,6 +56,15 @@ struct DevTarget {
     int blend_exp_int;                    // BlendingFactor when it is an integer in [2, 16], else 0
     int chroma_ties_up;                   // output chroma mean: 1 rounds ties up, 0 to even
     int blend_max;                        // BlendingFactor < 0: blend by maximum quality
+    // Precision P != 1 (SynthesizedView.cpp:325-333): wo x ho is the raster
+    // size int(0.5 + W * P) x int(0.5 + H * P); the output W x H is resized
+    // from it (image_writing.cpp:188-190).
+    int rescale;
+    int out_w, out_h;
+    float uv_sx, uv_sy;                   // raster size / output size (float)
+    float precision;
+    int rs_area;                          // the resize is an exact 2x reduction (area mean)
+    double rs_scale_x, rs_scale_y;        // raster size / output size (double), bilinear
     int tile_wl, tile_hl;                 // log2 of the tile width and height
     int ntx, nty;                         // output tiles
     int n_views;
@@ -136,6 +145,8 @@ struct SlotBuffers {
     uint8_t* holes;      // Wo*Ho hole mask (1 = no view covers the pixel)
     uint64_t* scan[4];   // Wo*Ho inpainting scratch each
     uint64_t* inpaint_seg;  // column-group minima of the inpainting passes
+    float4* pcolor;      // Precision != 1: blended colour per raster pixel
+    int32_t* psrc;       // Precision != 1: inpainting source of every hole
 };
 
 // Most row groups per column strip in the inpainting passes.

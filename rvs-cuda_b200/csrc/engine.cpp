@@ -45,6 +45,18 @@ void DevMem::release() {
     bytes = 0;
 }
 
+RasterDims raster_dims(const rvsb_camera& virt, const rvsb_synth_params& p) {
+    if (!std::isfinite(p.precision) || !(p.precision > 0.f)) throw Unsupported("Precision must be positive");
+    if (p.precision == 1.f) return {virt.width, virt.height, false};
+    const int w = (int)(0.5f + (float)virt.width * p.precision);
+    const int h = (int)(0.5f + (float)virt.height * p.precision);
+    if (w < 2 || h < 2 || (w & 1) || (h & 1) || w > 32768 || h > 32768)
+        throw Unsupported("Precision " + std::to_string(p.precision) + " gives a raster size of " +
+                          std::to_string(w) + "x" + std::to_string(h) +
+                          "; only even sizes of at least 2 and at most 32768 are supported");
+    return {w, h, true};
+}
+
 int nblocks_x(int w) { return (w - 1 + BLOCK_W - 1) / BLOCK_W; }
 int nblocks_y(int h) { return (h - 1 + BLOCK_H - 1) / BLOCK_H; }
 
@@ -68,11 +80,21 @@ SlotNeeds needs_of(const rvsb_scene* sc, int wo, int ho) {
 
 }  // namespace
 
-size_t SlotWorkspace::bytes_for(const rvsb_scene* sc, int wo, int ho) {
+size_t SlotWorkspace::bytes_for(const rvsb_scene* sc, int wo, int ho, bool rescale) {
     const SlotNeeds n = needs_of(sc, wo, ho);
     return sizeof(DevStatus) + n.vert * sizeof(float4) + n.bbox * sizeof(int4) + 3 * n.bins * sizeof(int) +
            n.list * sizeof(int) + n.out * (sizeof(uint64_t) * 5 + 1) +
-           (size_t)INPAINT_MAX_GROUPS * ((wo + 31) / 32) * 64 * sizeof(uint64_t);
+           (size_t)INPAINT_MAX_GROUPS * ((wo + 31) / 32) * 64 * sizeof(uint64_t) +
+           (rescale ? n.out * (sizeof(float4) + 2 * sizeof(int32_t)) : 0);
+}
+
+void SlotWorkspace::ensure_rescale(rvsb_context* ctx, int wo, int ho) {
+    const size_t n = (size_t)wo * ho;
+    if (n > cap_rescale) {
+        pcolor.alloc(ctx, n * sizeof(float4));
+        psrc.alloc(ctx, n * 2 * sizeof(int32_t));
+        cap_rescale = n;
+    }
 }
 
 void SlotWorkspace::ensure(rvsb_context* ctx, const rvsb_scene* sc, int wo, int ho) {
@@ -234,8 +256,24 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
         boff += (size_t)V.nbx * V.nby;
     }
     DevTarget& D = T.t;
-    D.wo = virt.width;
-    D.ho = virt.height;
+    const RasterDims rd = raster_dims(virt, p);
+    D.wo = rd.w;
+    D.ho = rd.h;
+    D.out_w = virt.width;
+    D.out_h = virt.height;
+    D.precision = p.precision;
+    if (rd.rescale) {
+        D.rescale = 1;
+        D.uv_sx = (float)rd.w / (float)virt.width;
+        D.uv_sy = (float)rd.h / (float)virt.height;
+        // cv::resize from the raster size to W x H: an exact 2x reduction
+        // is an area mean, everything else bilinear.
+        D.rs_scale_x = 1.0 / ((double)virt.width / rd.w);
+        D.rs_scale_y = 1.0 / ((double)virt.height / rd.h);
+        const int ix = (int)std::lrint(D.rs_scale_x), iy = (int)std::lrint(D.rs_scale_y);
+        D.rs_area = std::fabs(D.rs_scale_x - ix) < 2.220446049250313e-16 &&
+                    std::fabs(D.rs_scale_y - iy) < 2.220446049250313e-16 && ix == 2 && iy == 2;
+    }
     D.proj = virt.projection;
     D.wrap = (virt.projection == RVSB_PROJ_EQUIRECTANGULAR && virt.full_hor_range) ? 1 : 0;
     D.f0 = virt.focal[0];
@@ -268,7 +306,7 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
         M.hcnt = ws.ms_hcnt.as<int>();
         M.blur = ws.ms_blur.as<float>();
         M.on = 1;
-        M.rad = std::max(virt.width, virt.height) / 20;
+        M.rad = std::max(rd.w, rd.h) / 20;
         M.low_exp = p.low_freq_factor;
         M.high_exp = p.high_freq_factor;
         M.low_int = exp_int(p.low_freq_factor);
@@ -277,8 +315,8 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
     const RasterVariant& rv = kRasterVariants[variant];
     D.tile_wl = log2i(rv.tw);
     D.tile_hl = log2i(rv.th);
-    D.ntx = (virt.width + rv.tw - 1) / rv.tw;
-    D.nty = (virt.height + rv.th - 1) / rv.th;
+    D.ntx = (rd.w + rv.tw - 1) / rv.tw;
+    D.nty = (rd.h + rv.th - 1) / rv.th;
     D.n_views = n;
     D.bin_capacity = (int)ws.cap_list;
     SlotBuffers& B = T.b;
@@ -292,6 +330,10 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
     B.holes = ws.holes.as<uint8_t>();
     for (int s = 0; s < 4; ++s) B.scan[s] = ws.scan[s].as<uint64_t>();
     B.inpaint_seg = ws.inpaint_seg.as<uint64_t>();
+    if (rd.rescale) {
+        B.pcolor = ws.pcolor.as<float4>();
+        B.psrc = r.dbg.inpaint_source ? r.dbg.inpaint_source : ws.psrc.as<int32_t>();
+    }
     T.out_y = r.out.y;
     T.out_u = r.out.u;
     T.out_v = r.out.v;
@@ -322,6 +364,7 @@ BatchShape BatchCore::shape_of(const SlotRequest* reqs, int n, int variant) cons
     for (int k = 0; k < n; ++k) {
         if (reqs[k].aux) sh.aux = 1;
         if (reqs[k].params.blending_method == RVSB_BLEND_MULTISPECTRAL) sh.ms = 1;
+        if (reqs[k].params.precision != 1.f) sh.rescale = 1;
     }
     for (int k = 0; k < n; ++k) {
         const SlotRequest& r = reqs[k];
@@ -332,9 +375,12 @@ BatchShape BatchCore::shape_of(const SlotRequest* reqs, int n, int variant) cons
             sh.max_h = std::max(sh.max_h, c.height);
             sh.max_blocks = std::max(sh.max_blocks, nblocks_x(c.width) * nblocks_y(c.height));
         }
-        const int ntiles = ((r.virt.width + rv.tw - 1) / rv.tw) * ((r.virt.height + rv.th - 1) / rv.th);
-        sh.max_wo = std::max(sh.max_wo, r.virt.width);
-        sh.max_ho = std::max(sh.max_ho, r.virt.height);
+        const RasterDims rd = raster_dims(r.virt, r.params);
+        const int ntiles = ((rd.w + rv.tw - 1) / rv.tw) * ((rd.h + rv.th - 1) / rv.th);
+        sh.max_wo = std::max(sh.max_wo, rd.w);
+        sh.max_ho = std::max(sh.max_ho, rd.h);
+        sh.max_out_w = std::max(sh.max_out_w, r.virt.width);
+        sh.max_out_h = std::max(sh.max_out_h, r.virt.height);
         sh.max_tiles = std::max(sh.max_tiles, ntiles);
         sh.max_bins = std::max(sh.max_bins, ntiles * nv);
     }
@@ -362,7 +408,8 @@ int BatchCore::launch_variant(const SlotRequest* reqs, int n, int variant, cudaS
     const TablePtr tabs{tables_.as<SlotTable>()};
     if (use_graphs_ && !profiling_) {
         const std::vector<int> key = {sh.slots,  sh.variant, sh.max_views, sh.max_w,    sh.max_h,
-                                      sh.max_blocks, sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins, sh.aux, sh.ms};
+                                      sh.max_blocks, sh.max_wo, sh.max_ho, sh.max_tiles, sh.max_bins, sh.aux, sh.ms,
+                                      sh.rescale, sh.max_out_w, sh.max_out_h};
         auto it = graphs_.find(key);
         if (it == graphs_.end()) {
             cudaGraph_t g = nullptr;
@@ -415,11 +462,14 @@ int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
     int ms_wo = 0;
     for (int k = 0; k < n; ++k) {
         const SlotRequest& r = reqs[k];
-        ws_[k]->ensure(ctx_, r.scene, r.virt.width, r.virt.height);
-        if (r.aux) ws_[k]->ensure_aux(ctx_, r.virt.width, r.virt.height);
+        const RasterDims rd = raster_dims(r.virt, r.params);
+        if (rd.rescale && r.aux) throw Unsupported("auxiliary outputs need Precision 1");
+        ws_[k]->ensure(ctx_, r.scene, rd.w, rd.h);
+        if (r.aux) ws_[k]->ensure_aux(ctx_, rd.w, rd.h);
+        if (rd.rescale) ws_[k]->ensure_rescale(ctx_, rd.w, rd.h);
         if (r.params.blending_method == RVSB_BLEND_MULTISPECTRAL) {
-            ws_[k]->ensure_ms(ctx_, (int)r.scene->cams.size(), r.virt.width, r.virt.height);
-            ms_wo = std::max(ms_wo, r.virt.width);
+            ws_[k]->ensure_ms(ctx_, (int)r.scene->cams.size(), rd.w, rd.h);
+            ms_wo = std::max(ms_wo, rd.w);
         }
     }
     if (ms_wo > 0) prepare_ms_kernels(ms_wo);
@@ -437,7 +487,7 @@ int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
         }
         const int bucket = n == 1 ? 1 : n <= 4 ? 4 : n <= 16 ? 16 : 64;
         const std::vector<int> sig = {bucket, sh.max_views, sh.max_w, sh.max_h, sh.max_wo, sh.max_ho,
-                                      proj_in, proj_out};
+                                      proj_in, proj_out, sh.max_out_w, sh.max_out_h};
         auto it = tuned_.find(sig);
         if (it == tuned_.end()) it = tuned_.emplace(sig, tune(reqs, n, s)).first;
         variant = it->second;

@@ -73,13 +73,29 @@ struct SlotWorkspace {
     DevMem ms_view, ms_hsum, ms_hcnt, ms_blur;  // multispectral blending only
     size_t cap_ms = 0;            // view-pixels the multispectral buffers hold
     void ensure_ms(rvsb_context* ctx, int n_views, int wo, int ho);
+    DevMem pcolor, psrc;          // Precision != 1: raster-size colour and inpainting sources
+    size_t cap_rescale = 0;
+    void ensure_rescale(rvsb_context* ctx, int wo, int ho);
     size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0, cap_aux = 0, cap_strips = 0;
     void ensure_aux(rvsb_context* ctx, int wo, int ho);
 
-    // Bytes a slot needs for `scene` at output size wo x ho.
-    static size_t bytes_for(const rvsb_scene* scene, int wo, int ho);
+    // Bytes a slot needs for `scene` at raster size wo x ho (rescale: plus
+    // the buffers of a Precision != 1 synthesis).
+    static size_t bytes_for(const rvsb_scene* scene, int wo, int ho, bool rescale = false);
     void ensure(rvsb_context* ctx, const rvsb_scene* scene, int wo, int ho);
 };
+
+// Raster size of a synthesis: the virtual camera's size, or for Precision
+// P != 1 int(0.5 + W * P) x int(0.5 + H * P) (SynthesizedView.cpp:326-329),
+// rasterised with uv scaled by raster size / W and H and resized to W x H
+// when written.  Throws Unsupported for a P that is not finite and positive
+// or for a raster size that is not even in both dimensions (the raster's
+// 4:2:0 tile writer and inpainting work on 2x2 blocks).
+struct RasterDims {
+    int w, h;
+    bool rescale;
+};
+RasterDims raster_dims(const rvsb_camera& virt, const rvsb_synth_params& p);
 
 // Number of binning blocks of a view (BLOCK_W x BLOCK_H quads).
 int nblocks_x(int w);

@@ -399,7 +399,7 @@ Config load_config(const std::string& path) {
     else
         c.number_of_output_frames = c.number_of_frames;
     if (auto n = root.optional("Precision")) c.precision = (float)n.asDouble();
-    if (c.precision != 1.f) throw Unsupported("Precision other than 1 is not supported");
+    if (!std::isfinite(c.precision) || !(c.precision > 0.f)) throw ConfigError("Precision must be positive");
     if (auto n = root.optional("ColorSpace")) {
         const std::string& cs = n.asString();
         if (cs != "YUV" && cs != "RGB") throw ConfigError("Unknown color space");

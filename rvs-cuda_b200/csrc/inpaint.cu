@@ -56,6 +56,7 @@ struct InpaintImage {
     uint16_t* out_u;
     uint16_t* out_v;
     int ties_up;               // output chroma rounding
+    int no_write;              // Precision != 1: the resize writes the output
 };
 
 // Image of slot blockIdx.z of a batch.
@@ -72,8 +73,9 @@ struct FromTables {
         im.codes = t.b.codes;
 #pragma unroll
         for (int k = 0; k < 4; ++k) im.scan[k] = t.b.scan[k];
-        im.sources = t.dbg.inpaint_source;
+        im.sources = t.t.rescale ? t.b.psrc : t.dbg.inpaint_source;
         im.seg = t.b.inpaint_seg;
+        im.no_write = t.t.rescale;
         im.out_y = t.out_y;
         im.out_u = t.out_u;
         im.out_v = t.out_v;
@@ -541,6 +543,7 @@ __global__ void inpaint_write_kernel(const __grid_constant__ Src src) {
     uint16_t* __restrict__ out_u = im.out_u;
     uint16_t* __restrict__ out_v = im.out_v;
     const int ties_up = im.ties_up;
+    if (im.no_write) return;
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
     const int bx0 = rg.x0 / 2, by0 = rg.y0 / 2;
@@ -615,6 +618,7 @@ void launch_inpaint_scans(DevStatus* st, const uint8_t* holes, uint64_t* codes, 
     src.im.seg = nullptr;
     src.im.out_y = src.im.out_u = src.im.out_v = nullptr;
     src.im.ties_up = 0;
+    src.im.no_write = 1;
     launch_scans(src, w, h, 1, 1, s);
 }
 

@@ -20,6 +20,8 @@ struct BatchShape {
     int max_wo = 0, max_ho = 0;
     int max_tiles = 0;       // largest ntx * nty
     int max_bins = 0;        // largest ntx * nty * n_views
+    int rescale = 0;         // some slot rasterises at Precision != 1
+    int max_out_w = 0, max_out_h = 0;  // largest output (virtual camera) size
 };
 
 // Where the kernels find the slot tables.  A single synthesis passes its
@@ -78,6 +80,11 @@ struct DecodeJob {
 struct DecodeJobs {
     DecodeJob v[MAX_VIEWS];
 };
+// Precision != 1: resize of the raster-size colour to the output and its
+// 4:2:0 write, one launch for all slots that rescale.
+template <class Tabs>
+void launch_resize(const Tabs& tabs, const BatchShape& shape, cudaStream_t stream);
+
 void launch_decode_views(const DecodeJobs& jobs, int n, int max_w, int max_h, cudaStream_t s);
 
 // Decodes the colour planes of one input view into packed per-pixel words.

@@ -65,10 +65,11 @@ int launch_batch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s, cudaEve
     mark(6);
     const int inpaint_launches = launch_inpaint(tabs, sh, s);
     if (sh.aux) launch_aux(tabs, sh, s);
+    if (sh.rescale) launch_resize(tabs, sh, s);
     mark(7);
     mark(9);
     if (cudaPeekAtLastError() != cudaSuccess) return -1;
-    return 1 + 1 + 3 + 1 + ms_launches + inpaint_launches + (sh.aux ? 1 : 0);
+    return 1 + 1 + 3 + 1 + ms_launches + inpaint_launches + (sh.aux ? 1 : 0) + (sh.rescale ? 1 : 0);
 }
 
 template int launch_batch<TableParam>(const TableParam&, const BatchShape&, cudaStream_t, cudaEvent_t*);

@@ -169,6 +169,7 @@ __global__ void ms_blend_kernel(const __grid_constant__ Tabs tabs) {
             blend_view(hi, v, highc, c.w, M.high_exp, M.high_int, M.high_exp < 0.f);
         }
         const float f0 = __fadd_rn(lo.c0, hi.c0), f1 = __fadd_rn(lo.c1, hi.c1), f2 = __fadd_rn(lo.c2, hi.c2);
+        if (T.rescale) tab.b.pcolor[o] = make_float4(f0, f1, f2, 0.f);
         const uint64_t hole = tab.b.codes[o] & kHoleBit;
         any_hole |= hole != 0;
         code[p] = (uint64_t)quantize(f0, T.max_val) | ((uint64_t)quantize(f1, T.max_val) << 16) |
@@ -180,7 +181,7 @@ __global__ void ms_blend_kernel(const __grid_constant__ Tabs tabs) {
             tab.dbg.blend_color[o * 3 + 2] = f2;
         }
     }
-    if (any_hole) return;  // written by the inpainting passes
+    if (any_hole || T.rescale) return;  // written by the inpainting passes or the resize
     const size_t o = (size_t)y0 * T.wo + x0;
     tab.out_y[o] = (uint16_t)(code[0] & 0xffff);
     tab.out_y[o + 1] = (uint16_t)(code[1] & 0xffff);

@@ -86,13 +86,15 @@ __device__ __forceinline__ bool test_pixel(const TriSetup& s, float cx, float cy
 // edge in float, a few ulp from the reference's double evaluation.  The
 // squared lengths of an edge shared by two triangles are identical, so
 // equal reference qualities stay equal here.
-__device__ __forceinline__ float key_invq(float4 A, float4 B, float4 C) {
+__device__ __forceinline__ float key_invq(float4 A, float4 B, float4 C, float precision) {
     auto sq = [](float ax, float ay, float bx, float by) {
         const float dx = __fsub_rn(ax, bx), dy = __fsub_rn(ay, by);
         return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
     };
     const float m = fmaxf(sq(B.x, B.y, C.x, C.y), fmaxf(sq(A.x, A.y, B.x, B.y), sq(A.x, A.y, C.x, C.y)));
-    const float q = fminf(10000.f, fmaxf(1.f, __fsub_rn(10000.f, __fmul_rn(1000.f, __fsqrt_rn(m)))));
+    float stretch = __fsqrt_rn(m);
+    if (precision != 1.f) stretch = __fdiv_rn(stretch, precision);
+    const float q = fminf(10000.f, fmaxf(1.f, __fsub_rn(10000.f, __fmul_rn(1000.f, stretch))));
     return rcp_approx(q);
 }
 
@@ -106,7 +108,7 @@ __device__ __forceinline__ unsigned long long frag_key(float d, float invq, uint
 // (one quad per lane) into the tile's z-buffer `zb`: transform.cpp:159-176.
 template <class C>
 __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, bool wrap, int bx, int by,
-                                             int tx0, int ty0, unsigned long long* zb, int lane) {
+                                             int tx0, int ty0, unsigned long long* zb, int lane, float precision) {
     const int i = by * BLOCK_H + lane / BLOCK_W, j = bx * BLOCK_W + lane % BLOCK_W;
     const bool quad_ok = i < V.h - 1 && j < V.w - 1;
     float4 v00, v01, v10, v11, w0, w1;
@@ -153,14 +155,14 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
                 for (int x = s.x0; x <= s.x1; ++x) {
                     float d;
                     if (!test_pixel(s, C.x, C.y, A.z, B.z, C.z, x, y, d)) continue;
-                    if (invq < 0.f) invq = key_invq(A, B, C);
+                    if (invq < 0.f) invq = key_invq(A, B, C, precision);
                     atomicMin(&zb[(y - ty0) * C::TW + (x - tx0)], frag_key(d, invq, tri));
                 }
         }
         unsigned mask = __ballot_sync(0xffffffffu, big);
         if (!mask) continue;
         float invq_own = 0.f;
-        if (big) invq_own = key_invq(A, B, C);
+        if (big) invq_own = key_invq(A, B, C, precision);
         while (mask) {
             const int src = __ffs(mask) - 1;
             mask &= mask - 1;
@@ -242,7 +244,7 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
         }
         for (int k = 0; k < gn; ++k) {
             const int v = g0 + k;
-            const Fragment f = resolve_fragment(tab.v[v], zb[k][p], x, y);
+            const Fragment f = resolve_fragment(tab.v[v], zb[k][p], x, y, T.precision);
             const float qv = __fdiv_rn(f.validity, f.depth);
             if (tab.ms.on) tab.ms.view[(size_t)v * npo + po] = make_float4(f.col.x, f.col.y, f.col.z, qv);
             if (aux) {
@@ -284,7 +286,7 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
 template <class C>
 __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0, const float (*acc)[C::NPIX],
                                           DevStatus* st, uint64_t* codes, uint8_t* holes, uint16_t* out_y,
-                                          uint16_t* out_u, uint16_t* out_v, const DebugPtrs& dbg) {
+                                          uint16_t* out_u, uint16_t* out_v, const DebugPtrs& dbg, float4* pcolor) {
     constexpr int BW = C::TW / 2, NB = (C::TW / 2) * (C::TH / 2);
     int hx0 = INT_MAX, hy0 = INT_MAX, hx1 = INT_MIN, hy1 = INT_MIN;
     bool warp_hole = false;
@@ -318,6 +320,7 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
                     dbg.inpaint_source[o * 2 + 0] = x;
                     dbg.inpaint_source[o * 2 + 1] = y;
                 }
+                if (T.rescale) pcolor[o] = make_float4(c0, c1, c2, 0.f);
             }
             const size_t o = (size_t)y0 * T.wo + x0;
             reinterpret_cast<ulonglong2*>(codes + o)[0] = make_ulonglong2(code[0], code[1]);
@@ -326,7 +329,7 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
             reinterpret_cast<uint16_t*>(holes + o)[0] = (uint16_t)(hole_of(code[0]) | (hole_of(code[1]) << 8));
             reinterpret_cast<uint16_t*>(holes + o + T.wo)[0] =
                 (uint16_t)(hole_of(code[2]) | (hole_of(code[3]) << 8));
-            if (!any_hole) {
+            if (!any_hole && !T.rescale) {
                 reinterpret_cast<uint32_t*>(out_y + o)[0] =
                     (uint32_t)(code[0] & 0xffff) | ((uint32_t)(code[1] & 0xffff) << 16);
                 reinterpret_cast<uint32_t*>(out_y + o + T.wo)[0] =
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_co
                 const int ent = s_ent[q];
                 if (ent < 0) continue;
                 const int k = ent >> 26, bx = ent & 2047, by = (ent >> 11) & 32767;
-                raster_block<C>(tab.v[g0 + k], T.wo, T.ho, wrap, bx, by, tx0, ty0, zb[k], lane);
+                raster_block<C>(tab.v[g0 + k], T.wo, T.ho, wrap, bx, by, tx0, ty0, zb[k], lane, T.precision);
             }
             __syncthreads();
         }
@@ -452,7 +455,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_co
         __syncthreads();
     }
     write_tile<C>(T, tx0, ty0, acc, tab.b.status, tab.b.codes, tab.b.holes, tab.out_y, tab.out_u, tab.out_v,
-                  tab.dbg);
+                  tab.dbg, tab.b.pcolor);
 }
 
 template <class C, class Tabs>

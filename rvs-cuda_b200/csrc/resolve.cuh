@@ -27,7 +27,8 @@ __device__ __forceinline__ float3 packed_color(const DevView& V, int x, int y) {
 
 // Re-evaluates the winning triangle at pixel (x, y) exactly as the CPU's
 // colorize_triangle does for the fragment it keeps (transform.cpp:109-135).
-__device__ __forceinline__ Fragment resolve_fragment(const DevView& V, unsigned long long key, int x, int y) {
+__device__ __forceinline__ Fragment resolve_fragment(const DevView& V, unsigned long long key, int x, int y,
+                                                     float precision = 1.f) {
     Fragment f;
     f.col = make_float3(0.f, 0.f, 0.f);
     f.depth = INFINITY;
@@ -51,7 +52,7 @@ __device__ __forceinline__ Fragment resolve_fragment(const DevView& V, unsigned 
     f.col.y = interp(ca.y, cb.y, cc.y, l1, l2, l3);
     f.col.z = interp(ca.z, cb.z, cc.z, l1, l2, l3);
     f.depth = interp(A.z, B.z, C.z, l1, l2, l3);
-    f.validity = tri_quality(A.x, A.y, B.x, B.y, C.x, C.y);
+    f.validity = tri_quality(A.x, A.y, B.x, B.y, C.x, C.y, precision);
     return f;
 }
 

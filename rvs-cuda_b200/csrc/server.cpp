@@ -246,11 +246,18 @@ rvsb_status rvsb_server_submit(rvsb_server* s, int scene_id, const rvsb_camera* 
         s->ctx->last_error = std::string("virtual camera: ") + why;
         return RVSB_E_ARG;
     }
-    if (!std::isfinite(params->blending_factor) || params->blending_factor == 0.f || params->precision != 1.f ||
+    if (!std::isfinite(params->blending_factor) || params->blending_factor == 0.f ||
         params->reserved[0] != 0 || params->reserved[1] != 0 ||
         (params->blending_method != RVSB_BLEND_SIMPLE && params->blending_method != RVSB_BLEND_MULTISPECTRAL) ||
         (params->chroma_rounding != RVSB_CHROMA_TIES_EVEN && params->chroma_rounding != RVSB_CHROMA_TIES_UP))
         return RVSB_E_UNSUPPORTED;
+    RasterDims rd;
+    try {
+        rd = raster_dims(*virt, *params);
+    } catch (const std::exception& e) {
+        s->ctx->last_error = e.what();
+        return RVSB_E_UNSUPPORTED;
+    }
     std::lock_guard<std::mutex> lock(s->mu);
     if (scene_id < 0 || scene_id >= (int)s->scenes.size()) return RVSB_E_NOT_FOUND;
     if (s->stop) return RVSB_E_BUSY;
@@ -261,7 +268,7 @@ rvsb_status rvsb_server_submit(rvsb_server* s, int scene_id, const rvsb_camera* 
     p.req.virt = *virt;
     p.req.params = *params;
     p.req.out = *out;
-    p.bytes = SlotWorkspace::bytes_for(p.req.scene, virt->width, virt->height);
+    p.bytes = SlotWorkspace::bytes_for(p.req.scene, rd.w, rd.h, rd.rescale);
     if (p.bytes > s->budget) {
         s->ctx->last_error = "request needs more than the server's HBM budget";
         return RVSB_E_OOM_BUDGET;

@@ -29,6 +29,12 @@ def gpu_synthesize(ctx, inputs, planes, target, exponent, debug=False, scene=Non
     p = params if params is not None else rvsb.params(exponent)
     dbg = None
     if debug:
+        # intermediates are at the raster size (Precision P: int(0.5 + W * P))
+        ow, oh = wo, ho
+        if p.precision != 1.0:
+            P = np.float32(p.precision)
+            wo = int(np.float32(0.5) + np.float32(wo) * P)
+            ho = int(np.float32(0.5) + np.float32(ho) * P)
         n = len(inputs)
         nin = sum(c.width * c.height for c in inputs)
         dev = lambda *s, dt=torch.float32: torch.full(s, float("nan") if dt == torch.float32 else -1,
@@ -43,6 +49,7 @@ def gpu_synthesize(ctx, inputs, planes, target, exponent, debug=False, scene=Non
             "inpaint_source": dev(ho, wo, 2, dt=torch.int32),
         }
         sc.synthesize_debug(target, p, out, dbg)
+        wo, ho = ow, oh
     else:
         sc.synthesize(target, p, out)
     torch.cuda.synchronize()

@@ -174,6 +174,13 @@ def test_config_load(tmp_path, monkeypatch):
     assert c.output_path(0) == "out.yuv"
 
 
+def test_config_precision(tmp_path, monkeypatch):
+    """'Precision' reaches the synthesis parameters (Config.cpp:389-399)."""
+    monkeypatch.chdir(tmp_path)
+    c = rvsb.Config(_write_setup(tmp_path, Precision=2.0))
+    assert c.synth_params().precision == 2.0
+
+
 def test_config_overrides(tmp_path, monkeypatch):
     """Test_JsonParser_overrides (unit_test.cpp:344-368): keys of the
     override object replace the file's; the others stay."""
@@ -223,7 +230,7 @@ def test_pose_trace_bad_header(tmp_path, monkeypatch):
 
 
 @pytest.mark.parametrize("over,status", [
-    (dict(Precision=2.0), 7),
+    (dict(Precision=-1.0), 2),
     (dict(BlendingMethod="Multispectral", BlendingLowFreqFactor=1.0), 2),
     (dict(BlendingMethod="Median"), 2),
     (dict(ViewSynthesisMethod="Squares"), 2),
