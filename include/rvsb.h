@@ -61,8 +61,9 @@ typedef enum rvsb_color_format {
 
 /* One camera of an RVS camera-parameter file.  Field meanings follow
  * Parameters::readFrom (rvs/src/Parameters.cpp:104-129) and the setters at
- * rvs/src/Parameters.cpp:316-463.  Crop_region is not supported (the crop
- * equals the full resolution). */
+ * rvs/src/Parameters.cpp:316-463.  width, height and principle_point are
+ * the values after a virtual camera's Crop_region
+ * (rvsb_config_virtual_crop). */
 typedef struct rvsb_camera {
     int32_t projection;          /* rvsb_projection ("Projection") */
     int32_t width;               /* "Resolution"[0] */
@@ -207,6 +208,19 @@ float rvsb_config_validity_threshold(const rvsb_config* cfg);
  * the way Pipeline::computeView does (rvs/src/Pipeline.cpp:173-181:
  * position += trace position, rotation = trace rotation). */
 rvsb_status rvsb_config_virtual_camera_at(const rvsb_config* cfg, int i, int frame, rvsb_camera* out);
+/* "Crop_region" of virtual camera i (Parameters::setCropRegionFrom,
+ * Parameters.cpp:424-434): region = x, y, width, height inside the padded
+ * "Resolution" padded_size = width, height.  The camera returned by
+ * rvsb_config_virtual_camera has the region's size and, for a perspective
+ * camera, its principal point moved by (-x, -y) (Parameters.cpp:187-190,
+ * 245-249).  Colour outputs have the region's size; depth and mask outputs
+ * are placed into a zero image of the padded size (write_maskedDepth /
+ * write_mask, image_writing.cpp:262-267, 285-290).  Without the key the
+ * region is the whole resolution.  Input cameras with a region other than
+ * the whole resolution are rejected (RVSB_E_UNSUPPORTED): the reference
+ * reads their colour at the region's size and their depth at the padded
+ * size. */
+rvsb_status rvsb_config_virtual_crop(const rvsb_config* cfg, int i, int32_t region[4], int32_t padded_size[2]);
 
 /* Relative pose of an input camera seen from the virtual camera:
  * R = R_virt^T * R_in, t = -R_virt^T * (t_virt - t_in), in float with the

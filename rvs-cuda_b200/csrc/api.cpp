@@ -553,6 +553,18 @@ rvsb_status rvsb_config_virtual_camera(const rvsb_config* c, int i, rvsb_camera*
     return RVSB_OK;
 }
 
+rvsb_status rvsb_config_virtual_crop(const rvsb_config* c, int i, int32_t region[4], int32_t padded_size[2]) {
+    if (!c || !region || !padded_size || i < 0 || i >= (int)c->cfg.crop_virtual.size()) return RVSB_E_ARG;
+    const CropRegion& r = c->cfg.crop_virtual[i];
+    region[0] = r.x;
+    region[1] = r.y;
+    region[2] = r.w;
+    region[3] = r.h;
+    padded_size[0] = r.padded_w;
+    padded_size[1] = r.padded_h;
+    return RVSB_OK;
+}
+
 const char* rvsb_config_texture_path(const rvsb_config* c, int i) {
     return (c && i >= 0 && i < (int)c->cfg.texture_names.size()) ? c->cfg.texture_names[i].c_str() : nullptr;
 }

@@ -202,7 +202,7 @@ void int_vec(const json::Node& n, int* out) {
 
 }  // namespace
 
-rvsb_camera parse_camera(const json::Node& root) {
+rvsb_camera parse_camera(const json::Node& root, CropRegion* crop) {
     rvsb_camera c{};
     const std::string& proj = root.require("Projection").asString();
     if (proj == "Perspective")
@@ -247,16 +247,34 @@ rvsb_camera parse_camera(const json::Node& root) {
         }
         float_vec<2>(root.require("Ver_range"), c.ver_range);
     }
+    CropRegion cr;
+    cr.w = cr.padded_w = c.width;
+    cr.h = cr.padded_h = c.height;
     if (auto n = root.optional("Crop_region")) {
-        int cr[4];
-        int_vec<4>(n, cr);
-        if (cr[0] != 0 || cr[1] != 0 || cr[2] != c.width || cr[3] != c.height)
-            throw Unsupported("Crop_region other than the full resolution is not supported");
+        int v[4];
+        int_vec<4>(n, v);
+        if (v[0] != 0 || v[1] != 0 || v[2] != c.width || v[3] != c.height) {
+            // An input camera's colour is read at the region's size and its
+            // depth at the padded size (image_loading.cpp:76, 149), which do
+            // not describe one image; only output cameras are cropped.
+            if (!crop) throw Unsupported("Crop_region is supported on virtual cameras only");
+            if (v[0] < 0 || v[1] < 0 || v[2] <= 0 || v[3] <= 0 || v[0] > c.width - v[2] || v[1] > c.height - v[3])
+                throw ConfigError("Crop_region must lie inside the resolution");
+            cr.x = v[0];
+            cr.y = v[1];
+            cr.w = v[2];
+            cr.h = v[3];
+        }
     }
+    c.width = cr.w;
+    c.height = cr.h;
     if (c.projection == RVSB_PROJ_PERSPECTIVE) {
         float_vec<2>(root.require("Focal"), c.focal);
         float_vec<2>(root.require("Principle_point"), c.principle_point);
+        c.principle_point[0] -= (float)cr.x;
+        c.principle_point[1] -= (float)cr.y;
     }
+    if (crop) *crop = cr;
     if (auto n = root.optional("DisplacementMethod")) {
         if (n.asString() == "Polynomial") throw Unsupported("Polynomial displacement is not supported");
     }
@@ -317,26 +335,32 @@ namespace {
 
 // Config::loadCamerasParametersFromFile (Config.cpp:122-175).
 std::vector<rvsb_camera> load_cameras(const std::string& path, const std::vector<std::string>& names,
-                                      const json::Node& overrides) {
+                                      const json::Node& overrides, std::vector<CropRegion>* crops = nullptr) {
     json::Node root = json::Node::parse(read_text_file(path, "camera parameters file"));
     std::string version = root.require("Version").asString();
     std::string v2 = version.substr(0, 2);
     if (v2 != "2." && v2 != "3." && v2 != "4.")
         throw ConfigError("Version of the camera parameters file is not compatible with this version of RVS");
-    std::map<std::string, rvsb_camera> index;
+    std::map<std::string, std::pair<rvsb_camera, CropRegion>> index;
     json::Node cams = root.require("cameras");
     for (size_t i = 0; i < cams.size(); ++i) {
         json::Node node = cams.at(i);
         std::string name = node.require("Name").asString();
         if (index.count(name)) throw ConfigError("Camera parameters file has duplicate camera '" + name + "'");
         if (overrides) node.setOverrides(overrides);
-        index.emplace(name, parse_camera(node));
+        CropRegion cr;
+        const rvsb_camera c = parse_camera(node, &cr);
+        index.emplace(name, std::make_pair(c, cr));
     }
     std::vector<rvsb_camera> out;
     for (const auto& n : names) {
         auto it = index.find(n);
         if (it == index.end()) throw ConfigError("Camera parameters file does not have camera '" + n + "'");
-        out.push_back(it->second);
+        const CropRegion& cr = it->second.second;
+        if (!crops && (cr.w != cr.padded_w || cr.h != cr.padded_h))
+            throw Unsupported("Crop_region is supported on virtual cameras only (camera '" + n + "')");
+        out.push_back(it->second.first);
+        if (crops) crops->push_back(cr);
     }
     return out;
 }
@@ -360,7 +384,7 @@ Config load_config(const std::string& path) {
     c.params_real = load_cameras(root.require("InputCameraParameterFile").asString(), c.input_names,
                                  root.optional("InputOverrides"));
     c.params_virtual = load_cameras(root.require("VirtualCameraParameterFile").asString(), c.virtual_names,
-                                    root.optional("VirtualOverrides"));
+                                    root.optional("VirtualOverrides"), &c.crop_virtual);
     auto inputs = [&](const char* key, std::vector<std::string>& dst) {
         json::Node n = root.require(key);
         if (n.size() != c.input_names.size())

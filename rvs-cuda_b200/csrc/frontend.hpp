@@ -67,8 +67,22 @@ private:
 
 }  // namespace json
 
-// Parameters::readFrom (Parameters.cpp:104-129).
-rvsb_camera parse_camera(const json::Node& node);
+// "Crop_region" of a camera (Parameters::setCropRegionFrom,
+// Parameters.cpp:424-434): the region x, y, w, h of the padded resolution
+// the camera's image covers.  Without the key it is the whole resolution.
+struct CropRegion {
+    int x = 0, y = 0, w = 0, h = 0;
+    int padded_w = 0, padded_h = 0;
+};
+
+// Parameters::readFrom (Parameters.cpp:104-129).  With `crop`, a
+// Crop_region is applied as the reference's getters do: the camera's size
+// is the region's (getSize, Parameters.cpp:187-190) and a perspective
+// principal point is moved by the region's top-left corner
+// (getPrinciplePoint, Parameters.cpp:245-249); ERP ranges already refer to
+// the region.  Without `crop`, a region other than the whole resolution is
+// rejected.
+rvsb_camera parse_camera(const json::Node& node, CropRegion* crop = nullptr);
 
 struct Pose {
     float position[3];
@@ -82,6 +96,7 @@ struct Config {
     std::string version;
     std::vector<std::string> input_names, virtual_names;
     std::vector<rvsb_camera> params_real, params_virtual;
+    std::vector<CropRegion> crop_virtual;
     std::vector<std::string> texture_names, depth_names;
     std::vector<std::string> outfilenames, outmaskedfilenames, outmaskfilenames, outdepthfilenames,
         outmaskdepthfilenames;

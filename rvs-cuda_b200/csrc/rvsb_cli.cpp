@@ -12,9 +12,12 @@
 // and the previous frame's outputs are written meanwhile.  Besides
 // OutputFiles, the CPU-mode outputs MaskedOutputFiles, OutputMasks,
 // DepthOutputFiles and MaskedDepthOutputFiles are written when configured
-// (Pipeline.cpp:303-336).
+// (Pipeline.cpp:303-336).  A virtual camera's Crop_region gives colour
+// outputs of the region's size and depth and mask outputs placed into a zero
+// image of the padded resolution (image_writing.cpp:262-267, 285-290).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -183,9 +186,19 @@ int main(int argc, char** argv) {
         return true;
     };
     // Depth and mask files carry constant chroma planes
-    // (write_depth_YUV / write_mask_YUV, image_writing.cpp:104-139).
+    // (write_depth_YUV / write_mask_YUV, image_writing.cpp:104-139) and the
+    // padded resolution of a cropped camera.
     const uint16_t neutral = (uint16_t)std::lround(0.5 * (1.0 + (double)((1u << virt0.bit_depth_depth) - 1u)));
     const bool depth_chroma = virt0.depth_color_format == RVSB_FMT_YUV420;
+    int32_t crop[4] = {0, 0, virt0.width, virt0.height}, padded[2] = {virt0.width, virt0.height};
+    rvsb_config_virtual_crop(cfg, 0, crop, padded);
+    const size_t py = (size_t)padded[0] * padded[1], pc = (size_t)(padded[0] / 2) * (padded[1] / 2);
+    // The region's rows placed into a zero luma plane of the padded size.
+    auto pad = [&](auto* dst, const auto* src) {
+        for (int r = 0; r < crop[3]; ++r)
+            std::memcpy(dst + (size_t)(crop[1] + r) * padded[0] + crop[0], src + (size_t)r * crop[2],
+                        (size_t)crop[2] * sizeof(*src));
+    };
     auto write = [&](int vf, const OutputFrame& o, std::string& e) -> bool {
         const bool first = vf == 0;
         if (files[RVSB_OUT_COLOR] && !append(files[RVSB_OUT_COLOR], first, o.yuv.data(), o.yuv.size() * 2, e))
@@ -194,15 +207,17 @@ int main(int argc, char** argv) {
             !append(files[RVSB_OUT_MASKED_COLOR], first, o.masked.data(), o.masked.size() * 2, e))
             return false;
         if (files[RVSB_OUT_MASK]) {
-            std::vector<uint8_t> m(ny + 2 * nc, 128);
-            std::memcpy(m.data(), o.mask.data(), ny);
+            std::vector<uint8_t> m(py + 2 * pc, 128);
+            std::fill(m.begin(), m.begin() + py, 0);
+            pad(m.data(), o.mask.data());
             if (!append(files[RVSB_OUT_MASK], first, m.data(), m.size(), e)) return false;
         }
         for (int k : {RVSB_OUT_DEPTH, RVSB_OUT_MASKED_DEPTH}) {
             if (!files[k]) continue;
             const std::vector<uint16_t>& d = k == RVSB_OUT_DEPTH ? o.depth : o.masked_depth;
-            std::vector<uint16_t> img(d);
-            if (depth_chroma) img.resize(ny + 2 * nc, neutral);
+            std::vector<uint16_t> img(depth_chroma ? py + 2 * pc : py, neutral);
+            std::fill(img.begin(), img.begin() + py, 0);
+            pad(img.data(), d.data());
             if (!append(files[k], first, img.data(), img.size() * 2, e)) return false;
         }
         return true;

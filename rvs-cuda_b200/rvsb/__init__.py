@@ -33,6 +33,7 @@ EXPORTED = [
     "rvsb_server_drain", "rvsb_server_clock", "rvsb_server_destroy",
     "rvsb_batch_set_autotune", "rvsb_batch_set_raster_variant", "rvsb_batch_last_raster_variant",
     "rvsb_scene_set_autotune", "rvsb_synthesize_aux", "rvsb_config_output_file", "rvsb_config_validity_threshold",
+    "rvsb_config_virtual_crop",
 ]
 
 OUT_COLOR, OUT_MASKED_COLOR, OUT_MASK, OUT_DEPTH, OUT_MASKED_DEPTH = range(5)
@@ -85,6 +86,7 @@ def load():
     L.rvsb_config_synth_params.argtypes = [c_p, P(SynthParams)]
     L.rvsb_config_synth_params.restype = None
     L.rvsb_config_virtual_camera_at.argtypes = [c_p, ctypes.c_int, ctypes.c_int, P(Camera)]
+    L.rvsb_config_virtual_crop.argtypes = [c_p, ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_int32)]
     L.rvsb_relative_pose.argtypes = [P(Camera), P(Camera), P(ctypes.c_float), P(ctypes.c_float)]
     L.rvsb_scene_create.argtypes = [c_p, P(Camera), ctypes.c_int, P(c_p)]
     L.rvsb_scene_destroy.argtypes = [c_p]
@@ -485,6 +487,15 @@ class Config:
         if st != RVSB_OK:
             raise RvsbError(st, "no such virtual camera / frame")
         return c
+
+    def virtual_crop(self, i=0):
+        """((x, y, width, height), (padded width, padded height)) of virtual camera i."""
+        r = (ctypes.c_int32 * 4)()
+        s = (ctypes.c_int32 * 2)()
+        st = self.lib.rvsb_config_virtual_crop(self.h, i, r, s)
+        if st != RVSB_OK:
+            raise RvsbError(st, "no such virtual camera")
+        return tuple(r), tuple(s)
 
     def frames(self):
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -131,9 +131,12 @@ def test_camera_from_json_missing_key():
     assert "Focal" in str(e.value)
 
 
-def test_camera_from_json_unsupported():
+@pytest.mark.parametrize("extra", [dict(DisplacementMethod="Polynomial"), dict(Crop_region=[0, 0, 960, 540])])
+def test_camera_from_json_unsupported(extra):
+    """A single camera outside a configuration: a crop region is only
+    supported on a configuration's virtual cameras."""
     with pytest.raises(rvsb.RvsbError) as e:
-        rvsb.camera_from_json(json.dumps(_persp(DisplacementMethod="Polynomial")))
+        rvsb.camera_from_json(json.dumps(_persp(**extra)))
     assert e.value.status == 7  # RVSB_E_UNSUPPORTED
 
 
@@ -141,10 +144,11 @@ def test_camera_from_json_unsupported():
 # Configuration files (Config.cpp, PoseTraces.cpp)
 # ---------------------------------------------------------------------------
 
-def _write_setup(tmp, pose_trace=None, **over):
-    cams = {"Version": "2.0", "cameras": [_persp(Name="v1"), _persp(Name="v2", Position=[0, 1, 0]),
-                                         _persp(Name="viewport", Resolution=[960, 540], Focal=[750, 750],
-                                                Principle_point=[480, 270])]}
+def _write_setup(tmp, pose_trace=None, viewport=None, input_extra=None, **over):
+    vp = dict(Name="viewport", Resolution=[960, 540], Focal=[750, 750], Principle_point=[480, 270])
+    vp.update(viewport or {})
+    cams = {"Version": "2.0", "cameras": [_persp(Name="v1", **(input_extra or {})),
+                                         _persp(Name="v2", Position=[0, 1, 0]), _persp(**vp)]}
     (tmp / "cams.json").write_text(json.dumps(cams))
     cfg = {"Version": "3.0", "InputCameraParameterFile": "cams.json", "VirtualCameraParameterFile": "cams.json",
            "InputCameraNames": ["v1", "v2"], "VirtualCameraNames": ["viewport"],
@@ -179,6 +183,40 @@ def test_config_precision(tmp_path, monkeypatch):
     monkeypatch.chdir(tmp_path)
     c = rvsb.Config(_write_setup(tmp_path, Precision=2.0))
     assert c.synth_params().precision == 2.0
+
+
+def test_config_virtual_crop(tmp_path, monkeypatch):
+    """Crop_region of the virtual camera: the camera takes the region's size
+    and its principal point moves by the region's corner (Parameters.cpp:
+    187-190, 245-249); the region and padded size are reported."""
+    monkeypatch.chdir(tmp_path)
+    c = rvsb.Config(_write_setup(tmp_path, viewport=dict(Crop_region=[100, 50, 640, 360])))
+    v = c.virtual(0)
+    assert (v.width, v.height) == (640, 360)
+    assert list(v.principle_point) == [380.0, 220.0]
+    assert c.virtual_crop(0) == ((100, 50, 640, 360), (960, 540))
+    full = rvsb.Config(_write_setup(tmp_path))
+    assert full.virtual_crop(0) == ((0, 0, 960, 540), (960, 540))
+
+
+@pytest.mark.parametrize("where,region,status", [
+    ("input", [0, 0, 800, 400], 7),      # input crops: colour and depth sizes disagree in the reference
+    ("viewport", [400, 0, 640, 360], 2),  # outside the resolution
+    ("viewport", [0, 0, 0, 360], 2),
+])
+def test_config_crop_rejected(tmp_path, monkeypatch, where, region, status):
+    monkeypatch.chdir(tmp_path)
+    kw = dict(viewport=dict(Crop_region=region)) if where == "viewport" else dict(input_extra=dict(Crop_region=region))
+    with pytest.raises(rvsb.RvsbError) as e:
+        rvsb.Config(_write_setup(tmp_path, **kw))
+    assert e.value.status == status
+
+
+def test_config_input_crop_full_resolution(tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    res = _persp()["Resolution"]
+    c = rvsb.Config(_write_setup(tmp_path, input_extra=dict(Crop_region=[0, 0, res[0], res[1]])))
+    assert (c.inputs()[0].width, c.inputs()[0].height) == tuple(res)
 
 
 def test_config_overrides(tmp_path, monkeypatch):

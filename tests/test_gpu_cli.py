@@ -106,3 +106,55 @@ def test_cli_end_to_end(tmp_path):
         for g, rr in ((depth[f, :ny], ref["depth"]), (mdepth[f, :ny], ref["masked_depth"])):
             diff = np.abs(g.reshape(ho, wo).astype(np.int64) - rr.astype(np.int64))
             assert (diff > 1).mean() <= 5e-3
+
+
+def test_cli_crop_region(tmp_path, monkeypatch):
+    """A virtual camera with Crop_region: the colour output has the region's
+    size and matches the oracle's synthesis of the cropped camera; the mask
+    and depth outputs are the region placed into a zero image of the padded
+    resolution (image_writing.cpp:262-267, 285-290)."""
+    wl = scenes.random_pose_small(n_views=2, w=96, h=54, seed=93)
+    names = [f"v{i}" for i in range(len(wl.inputs))]
+    target = wl.targets[0]
+    cx, cy, pw, ph = 16, 8, target.width + 32, target.height + 18
+    vp = _cam_json("viewport", target)
+    vp["Resolution"] = [pw, ph]
+    vp["Crop_region"] = [cx, cy, target.width, target.height]
+    vp["Principle_point"] = [float(target.principle_point[0]) + cx, float(target.principle_point[1]) + cy]
+    cams = {"Version": "2.0", "cameras": [_cam_json(n, c) for n, c in zip(names, wl.inputs)] + [vp]}
+    (tmp_path / "cams.json").write_text(json.dumps(cams))
+    for i, planes in enumerate(wl.planes):
+        y, u, v, d = planes
+        (tmp_path / f"t{i}.yuv").write_bytes(y.tobytes() + u.tobytes() + v.tobytes())
+        chroma = np.full((d.shape[0] // 2) * (d.shape[1] // 2), 32768, np.uint16)
+        (tmp_path / f"d{i}.yuv").write_bytes(d.tobytes() + chroma.tobytes() + chroma.tobytes())
+    cfg = {"Version": "3.0", "InputCameraParameterFile": "cams.json", "VirtualCameraParameterFile": "cams.json",
+           "InputCameraNames": names, "VirtualCameraNames": ["viewport"],
+           "ViewImageNames": [f"t{i}.yuv" for i in range(len(names))],
+           "DepthMapNames": [f"d{i}.yuv" for i in range(len(names))],
+           "OutputFiles": ["out.yuv"], "OutputMasks": ["mask.yuv"], "DepthOutputFiles": ["depth.yuv"],
+           "NumberOfFrames": 1, "BlendingFactor": 5.0, "ValidityThreshold": 6000.0}
+    (tmp_path / "rvs.json").write_text(json.dumps(cfg))
+    import rvsb
+    monkeypatch.chdir(tmp_path)  # camera files are resolved against the working directory
+    virt = rvsb.Config("rvs.json").virtual(0)
+    assert (virt.width, virt.height) == (target.width, target.height)
+    r = subprocess.run([CLI, "rvs.json"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    wo, ho = target.width, target.height
+    ref = O.synthesize_aux(wl.inputs, wl.planes, virt, 5.0, 6000.0)
+    out = np.fromfile(tmp_path / "out.yuv", np.uint16)
+    assert out.size == wo * ho * 3 // 2
+    assert_parity(O.split_yuv420(out, wo, ho), ref["yuv"])
+    npy = pw * ph
+    mask = np.fromfile(tmp_path / "mask.yuv", np.uint8)
+    depth = np.fromfile(tmp_path / "depth.yuv", np.uint16)
+    assert mask.size == npy * 3 // 2 and depth.size == npy * 3 // 2
+    assert (mask[npy:] == 128).all() and (depth[npy:] == 32768).all()
+    my, dy = mask[:npy].reshape(ph, pw), depth[:npy].reshape(ph, pw)
+    inside = np.zeros((ph, pw), bool)
+    inside[cy:cy + ho, cx:cx + wo] = True
+    assert (my[~inside] == 0).all() and (dy[~inside] == 0).all()
+    assert (my[inside].reshape(ho, wo) != ref["mask"]).mean() <= 1e-3
+    diff = np.abs(dy[inside].reshape(ho, wo).astype(np.int64) - ref["depth"].astype(np.int64))
+    assert (diff > 1).mean() <= 5e-3
