@@ -368,7 +368,12 @@ def main():
     ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=2)
     ap.add_argument("--no-batched-configs", action="store_true")
+    # only the per-view lines (value, e2e): for launch lists of the per-view path
+    ap.add_argument("--plain-only", action="store_true")
     args = ap.parse_args()
+    if args.plain_only:
+        args.no_batched_configs = True
+        args.serve_seconds = 0.0
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
@@ -453,7 +458,9 @@ def main():
     barrier(world)
     e2e_total = allreduce_max(sum(e2e_ms) / 1000.0, world)
     e2e_value = world * args.e2e_steps / e2e_total
-    batched = measure_batched(ctx, scene, wl, args.batch_slots, args.batch_steps, flush, stream, world)
+    batched = None
+    if not args.plain_only:
+        batched = measure_batched(ctx, scene, wl, args.batch_slots, args.batch_steps, flush, stream, world)
     batched_configs = None
     if not args.no_batched_configs:
         batched_configs = {
