@@ -284,6 +284,29 @@ rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, i
                                  const rvsb_synth_params* params, const rvsb_yuv420* out_host,
                                  void* stream);
 
+/* Frames with host buffers, pipelined: the reference's per-frame loop
+ * (Pipeline.cpp:76-94 with its asynchronous loader and writer,
+ * Pipeline.cpp:226-245) over one input camera set, with the upload of frame
+ * k+1 on its own stream while frame k synthesises and the download of frame
+ * k-1 on a third.  Up to two frames are in flight; a submit that would start
+ * a third first waits for the oldest.  Host buffers are best pinned (else
+ * the copies are synchronous) and must stay untouched until the frame's
+ * rvsb_host_stream_wait returns.  Each frame's uploads are ordered after
+ * the work queued on `stream` before the submit (NULL: the legacy default
+ * stream); rvsb_host_stream_join makes `stream` wait for every frame
+ * submitted so far without blocking the host.  Results are the same as
+ * rvsb_synthesize_host's. */
+typedef struct rvsb_host_stream rvsb_host_stream;
+rvsb_status rvsb_host_stream_create(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs,
+                                    rvsb_host_stream** out);
+void rvsb_host_stream_destroy(rvsb_host_stream* hs);
+rvsb_status rvsb_host_stream_submit(rvsb_host_stream* hs, const rvsb_view_planes* host_planes,
+                                    const rvsb_camera* virt, const rvsb_synth_params* params,
+                                    const rvsb_yuv420* out_host, void* stream, uint64_t* ticket);
+/* Blocks until frame `ticket` is in its host output buffers. */
+rvsb_status rvsb_host_stream_wait(rvsb_host_stream* hs, uint64_t ticket);
+rvsb_status rvsb_host_stream_join(rvsb_host_stream* hs, void* stream);
+
 /* Intermediate results of one synthesis, for stage-by-stage checks against
  * the reference's CPU path.  Every pointer is a device pointer and may be
  * NULL; n = number of input views, W,H = input size, Wo,Ho = raster size (the

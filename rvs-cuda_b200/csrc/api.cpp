@@ -22,6 +22,26 @@ struct rvsb_batch {
     std::unique_ptr<BatchCore> core;
 };
 
+// Pipelined host frames: two sets of raw device planes and output staging,
+// alternating between frames; uploads on `copy`, synthesis on `compute`,
+// downloads on `down`.
+struct rvsb_host_stream {
+    struct Set {
+        std::vector<std::unique_ptr<DevMem>> planes;  // 4 per view: y, u, v, depth
+        DevMem out;
+        cudaEvent_t uploaded = nullptr, computed = nullptr, downloaded = nullptr;
+        uint64_t ticket = 0;
+        bool busy = false;
+    };
+    rvsb_context* ctx = nullptr;
+    rvsb_scene* scene = nullptr;  // cameras, decoded colour, slot workspace
+    Set sets[2];
+    cudaStream_t copy = nullptr, compute = nullptr, down = nullptr;
+    cudaEvent_t ordered = nullptr;  // the caller's stream at submit time
+    uint64_t next = 0;
+    ~rvsb_host_stream();
+};
+
 namespace {
 
 rvsb_status fail(rvsb_context* ctx, rvsb_status s, const std::string& msg) {
@@ -484,6 +504,131 @@ rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, i
         check(cudaMemcpyAsync(out_host->u, dev.u, nc, cudaMemcpyDeviceToHost, s), "download U");
         check(cudaMemcpyAsync(out_host->v, dev.v, nc, cudaMemcpyDeviceToHost, s), "download V");
         check(cudaStreamSynchronize(s), "synchronize");
+        return RVSB_OK;
+    });
+}
+
+rvsb_host_stream::~rvsb_host_stream() {
+    cudaSetDevice(ctx->device);
+    for (Set& s : sets)
+        if (s.busy) cudaEventSynchronize(s.downloaded);
+    for (Set& s : sets)
+        for (cudaEvent_t e : {s.uploaded, s.computed, s.downloaded})
+            if (e) cudaEventDestroy(e);
+    for (cudaStream_t st : {copy, compute, down})
+        if (st) cudaStreamDestroy(st);
+    if (ordered) cudaEventDestroy(ordered);
+    if (scene) rvsb_scene_destroy(scene);
+}
+
+rvsb_status rvsb_host_stream_create(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs,
+                                    rvsb_host_stream** out) {
+    if (!ctx || !inputs || !out || n_inputs <= 0) return RVSB_E_ARG;
+    *out = nullptr;
+    auto hs = std::make_unique<rvsb_host_stream>();
+    hs->ctx = ctx;
+    rvsb_status st = rvsb_scene_create(ctx, inputs, n_inputs, &hs->scene);
+    if (st != RVSB_OK) return st;
+    return guarded(ctx, [&]() -> rvsb_status {
+        check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        for (auto& s : hs->sets) {
+            for (int v = 0; v < n_inputs; ++v)
+                for (int k = 0; k < 4; ++k) {
+                    auto m = std::make_unique<DevMem>();
+                    m->alloc(ctx, plane_bytes(inputs[v], k));
+                    s.planes.push_back(std::move(m));
+                }
+            for (cudaEvent_t* e : {&s.uploaded, &s.computed, &s.downloaded})
+                check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        for (cudaStream_t* sp : {&hs->copy, &hs->compute, &hs->down})
+            check(cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaEventCreateWithFlags(&hs->ordered, cudaEventDisableTiming), "cudaEventCreate");
+        *out = hs.release();
+        return RVSB_OK;
+    });
+}
+
+void rvsb_host_stream_destroy(rvsb_host_stream* hs) { delete hs; }
+
+rvsb_status rvsb_host_stream_submit(rvsb_host_stream* hs, const rvsb_view_planes* host_planes,
+                                    const rvsb_camera* virt, const rvsb_synth_params* params,
+                                    const rvsb_yuv420* out_host, void* stream, uint64_t* ticket) {
+    if (!hs || !host_planes || !virt || !out_host || !ticket) return RVSB_E_ARG;
+    rvsb_context* ctx = hs->ctx;
+    return guarded(ctx, [&]() -> rvsb_status {
+        if (!out_host->y || !out_host->u || !out_host->v) throw ArgError("null output planes");
+        rvsb_scene* sc = hs->scene;
+        const int n = (int)sc->cams.size();
+        for (int v = 0; v < n; ++v)
+            if (!host_planes[v].y || !host_planes[v].u || !host_planes[v].v || !host_planes[v].depth)
+                throw ArgError("null plane");
+        validate_request(sc, virt, params, out_host);
+        check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        rvsb_host_stream::Set& S = hs->sets[hs->next % 2];
+        // The set's previous frame (two submits ago) must be complete before
+        // its planes and staging are reused.
+        if (S.busy) {
+            check(cudaEventSynchronize(S.downloaded), "wait for an earlier frame");
+            S.busy = false;
+        }
+        const size_t ny = (size_t)virt->width * virt->height * 2;
+        const size_t nc = (size_t)(virt->width / 2) * (virt->height / 2) * 2;
+        if (S.out.bytes < ny + 2 * nc) S.out.alloc(ctx, ny + 2 * nc);
+        check(cudaEventRecord(hs->ordered, static_cast<cudaStream_t>(stream)), "record caller stream");
+        check(cudaStreamWaitEvent(hs->copy, hs->ordered, 0), "order after caller stream");
+        std::vector<rvsb_view_planes> dev(n);
+        for (int v = 0; v < n; ++v) {
+            const void* src[4] = {host_planes[v].y, host_planes[v].u, host_planes[v].v, host_planes[v].depth};
+            for (int k = 0; k < 4; ++k)
+                check(cudaMemcpyAsync(S.planes[v * 4 + k]->ptr, src[k], plane_bytes(sc->cams[v], k),
+                                      cudaMemcpyHostToDevice, hs->copy),
+                      "upload plane");
+            dev[v].y = S.planes[v * 4 + 0]->as<uint16_t>();
+            dev[v].u = S.planes[v * 4 + 1]->as<uint16_t>();
+            dev[v].v = S.planes[v * 4 + 2]->as<uint16_t>();
+            dev[v].depth = S.planes[v * 4 + 3]->as<uint16_t>();
+        }
+        check(cudaEventRecord(S.uploaded, hs->copy), "record upload");
+        check(cudaStreamWaitEvent(hs->compute, S.uploaded, 0), "wait for upload");
+        rvsb_yuv420 o;
+        char* base = static_cast<char*>(S.out.ptr);
+        o.y = reinterpret_cast<uint16_t*>(base);
+        o.u = reinterpret_cast<uint16_t*>(base + ny);
+        o.v = reinterpret_cast<uint16_t*>(base + ny + nc);
+        rvsb_status st = synthesize_impl(sc, virt, params, &o, nullptr, hs->compute, dev.data());
+        if (st != RVSB_OK) return st;
+        check(cudaEventRecord(S.computed, hs->compute), "record synthesis");
+        check(cudaStreamWaitEvent(hs->down, S.computed, 0), "wait for synthesis");
+        check(cudaMemcpyAsync(out_host->y, o.y, ny, cudaMemcpyDeviceToHost, hs->down), "download Y");
+        check(cudaMemcpyAsync(out_host->u, o.u, nc, cudaMemcpyDeviceToHost, hs->down), "download U");
+        check(cudaMemcpyAsync(out_host->v, o.v, nc, cudaMemcpyDeviceToHost, hs->down), "download V");
+        check(cudaEventRecord(S.downloaded, hs->down), "record download");
+        S.ticket = hs->next;
+        S.busy = true;
+        *ticket = hs->next++;
+        return RVSB_OK;
+    });
+}
+
+rvsb_status rvsb_host_stream_wait(rvsb_host_stream* hs, uint64_t ticket) {
+    if (!hs || ticket >= hs->next) return RVSB_E_ARG;
+    return guarded(hs->ctx, [&]() -> rvsb_status {
+        for (auto& s : hs->sets)
+            if (s.busy && s.ticket == ticket) {
+                check(cudaEventSynchronize(s.downloaded), "wait for frame");
+                s.busy = false;
+            }
+        return RVSB_OK;  // older frames completed before their set was reused
+    });
+}
+
+rvsb_status rvsb_host_stream_join(rvsb_host_stream* hs, void* stream) {
+    if (!hs) return RVSB_E_ARG;
+    return guarded(hs->ctx, [&]() -> rvsb_status {
+        for (auto& s : hs->sets)
+            if (s.busy)
+                check(cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), s.downloaded, 0), "join");
         return RVSB_OK;
     });
 }

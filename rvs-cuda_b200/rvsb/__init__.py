@@ -33,7 +33,8 @@ EXPORTED = [
     "rvsb_server_drain", "rvsb_server_clock", "rvsb_server_destroy",
     "rvsb_batch_set_autotune", "rvsb_batch_set_raster_variant", "rvsb_batch_last_raster_variant",
     "rvsb_scene_set_autotune", "rvsb_synthesize_aux", "rvsb_config_output_file", "rvsb_config_validity_threshold",
-    "rvsb_config_virtual_crop",
+    "rvsb_config_virtual_crop", "rvsb_host_stream_create", "rvsb_host_stream_destroy", "rvsb_host_stream_submit",
+    "rvsb_host_stream_wait", "rvsb_host_stream_join",
 ]
 
 OUT_COLOR, OUT_MASKED_COLOR, OUT_MASK, OUT_DEPTH, OUT_MASKED_DEPTH = range(5)
@@ -95,6 +96,13 @@ def load():
     L.rvsb_synthesize.argtypes = [c_p, P(Camera), P(SynthParams), P(Yuv420), c_p]
     L.rvsb_synthesize_host.argtypes = [c_p, P(Camera), ctypes.c_int, P(ViewPlanes), P(Camera),
                                        P(SynthParams), P(Yuv420), c_p]
+    L.rvsb_host_stream_create.argtypes = [c_p, P(Camera), ctypes.c_int, P(c_p)]
+    L.rvsb_host_stream_destroy.argtypes = [c_p]
+    L.rvsb_host_stream_destroy.restype = None
+    L.rvsb_host_stream_submit.argtypes = [c_p, P(ViewPlanes), P(Camera), P(SynthParams), P(Yuv420), c_p,
+                                          P(ctypes.c_uint64)]
+    L.rvsb_host_stream_wait.argtypes = [c_p, ctypes.c_uint64]
+    L.rvsb_host_stream_join.argtypes = [c_p, c_p]
     L.rvsb_synthesize_debug.argtypes = [c_p, P(Camera), P(SynthParams), P(Yuv420), P(DebugOut), c_p]
     L.rvsb_synthesize_frame.argtypes = [c_p, P(ViewPlanes), P(Camera), P(SynthParams), P(Yuv420), c_p]
     L.rvsb_scene_last_launch_count.argtypes = [c_p]
@@ -204,6 +212,49 @@ class Context:
         return self.check(self.lib.rvsb_synthesize_host(self.h, arr, n, vp, ctypes.byref(virt),
                                                         ctypes.byref(p), ctypes.byref(out),
                                                         _stream(stream)))
+
+
+class HostStream:
+    """rvsb_host_stream: frames with host buffers, uploads, synthesis and
+    downloads of consecutive frames overlapped (two frames in flight)."""
+
+    def __init__(self, ctx, cams):
+        self.ctx = ctx
+        self.cams = list(cams)
+        n = len(self.cams)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.rvsb_host_stream_create(ctx.h, (Camera * n)(*self.cams), n, ctypes.byref(h)))
+        self.h = h
+
+    def submit(self, host_planes, virt, p, out_planes, stream=None):
+        """Enqueues one frame; returns its ticket.  The buffers must stay
+        untouched until wait(ticket)."""
+        n = len(self.cams)
+        vp = (ViewPlanes * n)()
+        for i, planes in enumerate(host_planes):
+            vp[i].y, vp[i].u, vp[i].v, vp[i].depth = (_ptr(a) for a in planes)
+        out = Yuv420(*(_ptr(a) for a in out_planes))
+        t = ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.rvsb_host_stream_submit(self.h, vp, ctypes.byref(virt), ctypes.byref(p),
+                                                            ctypes.byref(out), _stream(stream), ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket):
+        return self.ctx.check(self.ctx.lib.rvsb_host_stream_wait(self.h, ctypes.c_uint64(ticket)))
+
+    def join(self, stream=None):
+        return self.ctx.check(self.ctx.lib.rvsb_host_stream_join(self.h, _stream(stream)))
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.rvsb_host_stream_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Scene:
