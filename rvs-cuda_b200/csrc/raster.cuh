@@ -46,13 +46,15 @@ struct Cfg {
 // whatever the scheduling order.
 //
 // The coordinates come from rinv, an approximate reciprocal of den (at most
-// 1 ulp off).  Then l1 and l2 are within 4 ulp of the CPU's n / den and l3
-// within u * (4.1|l1| + 2.1|1 - l1| + 4.1|l2| + 2|l3|) of the CPU's
-// (1 - l1) - l2 (u = 2^-24: one rounding per product and subtraction).  A
-// test is decided when its value is farther than the (rounded up) bound
-// from -1e-6; otherwise the coordinates are recomputed with the
-// reference's divisions.  The depth in the key uses the fast coordinates;
-// the resolve recomputes the winning fragment exactly.
+// 1 ulp off).  Then l1 and l2 are within 4u|l| of the CPU's n / den
+// (u = 2^-24: 2u from the reciprocal, one rounding here and one in the
+// CPU's division), and l3 = (1 - l1) - l2 within
+// u * (4|l1| + 2|1 - l1| + 4|l2| + 2|l3|) of the CPU's, which is below
+// 21u * M with M = max(|l1|, |l2|, |l3|, 1).  One bound, 24u * M, therefore
+// covers every coordinate: the test is decided when the smallest coordinate
+// is farther than the bound from -1e-6; otherwise the coordinates are
+// recomputed with the reference's divisions.  The depth in the key uses the
+// fast coordinates; the resolve recomputes the winning fragment exactly.
 __device__ __forceinline__ bool test_pixel(const TriSetup& s, float cx, float cy, float za, float zb_, float zc,
                                            int x, int y, float& d) {
     const float u = 5.9604645e-8f, eps = 1e-6f;
@@ -61,18 +63,12 @@ __device__ __forceinline__ bool test_pixel(const TriSetup& s, float cx, float cy
     const float n1 = __fadd_rn(__fmul_rn(s.b1c1, tx), __fmul_rn(s.c0b0, ty));
     const float n2 = __fadd_rn(__fmul_rn(s.c1a1, tx), __fmul_rn(s.a0c0, ty));
     float l1 = __fmul_rn(n1, s.rinv), l2 = __fmul_rn(n2, s.rinv);
-    const float b1 = 5.f * u * fabsf(l1), b2 = 5.f * u * fabsf(l2);
-    if (l1 + b1 < -eps || l2 + b2 < -eps) return false;
-    bool decided = l1 - b1 >= -eps && l2 - b2 >= -eps;
-    float l3 = 0.f;
-    if (decided) {
-        const float a = __fsub_rn(1.f, l1);
-        l3 = __fsub_rn(a, l2);
-        const float b3 = u * (6.f * fabsf(l1) + 3.f * fabsf(a) + 6.f * fabsf(l2) + 3.f * fabsf(l3));
-        if (l3 + b3 < -eps) return false;
-        decided = l3 - b3 >= -eps;
-    }
-    if (!decided) {
+    float l3 = __fsub_rn(__fsub_rn(1.f, l1), l2);
+    const float mn = fminf(fminf(l1, l2), l3);
+    const float M = fmaxf(fmaxf(fabsf(l1), fabsf(l2)), fmaxf(fabsf(l3), 1.f));
+    const float bound = __fmul_rn(24.f * u, M);
+    if (__fadd_rn(mn, bound) < -eps) return false;
+    if (!(__fsub_rn(mn, bound) >= -eps)) {
         l1 = __fdiv_rn(n1, s.den);
         l2 = __fdiv_rn(n2, s.den);
         l3 = __fsub_rn(__fsub_rn(1.f, l1), l2);
@@ -150,14 +146,19 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
         const uint32_t tri = quad * 4u + (uint32_t)slot;
         const bool big = count > C::SMALL;
         if (count > 0 && !big) {
-            float invq = -1.f;
-            for (int y = s.y0; y <= s.y1; ++y)
-                for (int x = s.x0; x <= s.x1; ++x) {
-                    float d;
-                    if (!test_pixel(s, C.x, C.y, A.z, B.z, C.z, x, y, d)) continue;
-                    if (invq < 0.f) invq = key_invq(A, B, C, precision);
+            // One flat loop over the candidate box (at most SMALL pixels),
+            // with the quality key computed once up front.
+            const float invq = key_invq(A, B, C, precision);
+            int x = s.x0, y = s.y0;
+            for (int k = 0; k < count; ++k) {
+                float d;
+                if (test_pixel(s, C.x, C.y, A.z, B.z, C.z, x, y, d))
                     atomicMin(&zb[(y - ty0) * C::TW + (x - tx0)], frag_key(d, invq, tri));
+                if (++x > s.x1) {
+                    x = s.x0;
+                    ++y;
                 }
+            }
         }
         unsigned mask = __ballot_sync(0xffffffffu, big);
         if (!mask) continue;
