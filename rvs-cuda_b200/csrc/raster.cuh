@@ -110,17 +110,17 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
     float4 v00, v01, v10, v11, w0, w1;
     bool cond0 = false;
     if (quad_ok) {
+        // All four corners at once (one memory round trip), then the
+        // emission test of transform.cpp:161.
         const size_t r0 = (size_t)i * V.w, r1 = r0 + V.w;
-        v01 = V.vert[r0 + j + 1];
-        v10 = V.vert[r1 + j];
+        v00 = __ldg(V.vert + r0 + j);
+        v01 = __ldg(V.vert + r0 + j + 1);
+        v10 = __ldg(V.vert + r1 + j);
+        v11 = __ldg(V.vert + r1 + j + 1);
         cond0 = v01.z > 0.f && v10.z > 0.f && v01.x > 0.f && v10.x > 0.f;
-        if (cond0) {
-            v00 = V.vert[r0 + j];
-            v11 = V.vert[r1 + j + 1];
-            if (wrap && j == 0) {
-                w0 = V.vert[r0 + V.w - 1];
-                w1 = V.vert[r1 + V.w - 1];
-            }
+        if (cond0 && wrap && j == 0) {
+            w0 = __ldg(V.vert + r0 + V.w - 1);
+            w1 = __ldg(V.vert + r1 + V.w - 1);
         }
     }
     // Scan order of transform.cpp:159-176: row i, column j, then triangle
