@@ -1,32 +1,11 @@
-// Binning of input blocks into output tiles: count per (tile, view),
-// exclusive scan, fill.  Bin order does not affect the result (the raster's
+// Binning of input blocks into output tiles: count per (tile, view) (done
+// by the warp kernel as it writes each block's box), exclusive scan, fill.  Bin order does not affect the result (the raster's
 // 64-bit atomicMin keys are order independent).
 #include "device_common.cuh"
 #include "kernels.hpp"
 
 namespace rvsb {
 namespace {
-
-// Grid (ceil(max_blocks / 256), max_views, slots): one thread per binning
-// block of view blockIdx.y of slot blockIdx.z.
-template <class Tabs>
-__global__ void bin_count_kernel(const __grid_constant__ Tabs tabs) {
-    const SlotTable& tab = tabs.at(blockIdx.z);
-    const int v = blockIdx.y;
-    if (v >= tab.t.n_views) return;
-    const DevView& V = tab.v[v];
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= V.nbx * V.nby) return;
-    const int4 bb = V.bbox[b];
-    if (bb.x > bb.z || bb.y > bb.w) return;
-    const int ntx = tab.t.ntx, n = tab.t.n_views;
-    const int wl = tab.t.tile_wl, hl = tab.t.tile_hl;
-    const int tx0 = bb.x >> wl, tx1 = bb.z >> wl, ty0 = bb.y >> hl, ty1 = bb.w >> hl;
-    int* counts = tab.b.counts;
-    for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx) atomicAdd(&counts[(ty * ntx + tx) * n + v], 1);
-    atomicAdd(&tab.b.status->bin_total, (tx1 - tx0 + 1) * (ty1 - ty0 + 1));
-}
 
 // Exclusive scan of one slot's bin counts (one CTA of 1024 threads per slot).
 template <class Tabs>
@@ -70,6 +49,8 @@ __global__ void __launch_bounds__(1024) bin_scan_kernel(const __grid_constant__ 
     if (tid == 0 && tab.b.status->bin_total > tab.b.capacity) tab.b.status->bin_overflow = 1;
 }
 
+// Grid (ceil(max_blocks / 256), max_views, slots): one thread per binning
+// block of view blockIdx.y of slot blockIdx.z.
 template <class Tabs>
 __global__ void bin_fill_kernel(const __grid_constant__ Tabs tabs) {
     const SlotTable& tab = tabs.at(blockIdx.z);
@@ -97,7 +78,6 @@ __global__ void bin_fill_kernel(const __grid_constant__ Tabs tabs) {
 template <class Tabs>
 void launch_bin(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
     dim3 grid((sh.max_blocks + 255) / 256, sh.max_views, sh.slots);
-    bin_count_kernel<<<grid, 256, 0, s>>>(tabs);
     bin_scan_kernel<<<sh.slots, 1024, 0, s>>>(tabs);
     bin_fill_kernel<<<grid, 256, 0, s>>>(tabs);
 }

@@ -1,6 +1,6 @@
 // Orchestration of one batch of syntheses on a stream.  Every kernel covers
 // all slots of the batch in one launch (the slot is a grid dimension), so a
-// batch costs the same 12 launches as a single view and the sequence can be
+// batch costs the same 11 launches as a single view and the sequence can be
 // captured in a CUDA graph.
 #include "device_common.cuh"
 #include "kernels.hpp"
@@ -69,7 +69,7 @@ int launch_batch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s, cudaEve
     mark(7);
     mark(9);
     if (cudaPeekAtLastError() != cudaSuccess) return -1;
-    return 1 + 1 + 3 + 1 + ms_launches + inpaint_launches + (sh.aux ? 1 : 0) + (sh.rescale ? 1 : 0);
+    return 1 + 1 + 2 + 1 + ms_launches + inpaint_launches + (sh.aux ? 1 : 0) + (sh.rescale ? 1 : 0);
 }
 
 template int launch_batch<TableParam>(const TableParam&, const BatchShape&, cudaStream_t, cudaEvent_t*);

@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
     for (int o = 4; o > 0; o >>= 1) blk.add(blk.shfl_xor(o));
     const int b = lane >> 3;
     const int bx = blockIdx.x * 4 + b, by = blockIdx.y * 8 + warp;
+    int entries = 0;
     if ((lane & 7) == 0 && bx < V.nbx && by < V.nby) {
         Box out = blk;
         out.add(right);
@@ -153,8 +154,20 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
 #pragma unroll
             for (int r = 0; r <= ROWS; ++r) out.add(s_seam[warp * ROWS + r]);
         }
-        V.bbox[by * V.nbx + bx] = to_pixel_box(out.x0, out.y0, out.x1, out.y1, T.wo, T.ho);
+        const int4 bb = to_pixel_box(out.x0, out.y0, out.x1, out.y1, T.wo, T.ho);
+        V.bbox[by * V.nbx + bx] = bb;
+        // Binning, first pass: one entry per output tile the box touches,
+        // counted per (tile, view).
+        if (bb.x <= bb.z && bb.y <= bb.w) {
+            const int wl = T.tile_wl, hl = T.tile_hl, n = T.n_views, ntx = T.ntx;
+            const int tx0 = bb.x >> wl, tx1 = bb.z >> wl, ty0 = bb.y >> hl, ty1 = bb.w >> hl;
+            for (int ty = ty0; ty <= ty1; ++ty)
+                for (int tx = tx0; tx <= tx1; ++tx) atomicAdd(&tab.b.counts[(ty * ntx + tx) * n + view], 1);
+            entries = (tx1 - tx0 + 1) * (ty1 - ty0 + 1);
+        }
     }
+    entries = __reduce_add_sync(0xffffffffu, entries);
+    if (lane == 0 && entries > 0) atomicAdd(&tab.b.status->bin_total, entries);
 }
 
 }  // namespace
