@@ -47,6 +47,52 @@ __global__ void __launch_bounds__(1024) bin_scan_kernel(const __grid_constant__ 
         run += counts[k];
     }
     if (tid == 0 && tab.b.status->bin_total > tab.b.capacity) tab.b.status->bin_overflow = 1;
+
+    // Raster launch order: the tiles with clearly more bin entries than the
+    // average (over all views; mostly tiles crossed by stretched triangles)
+    // first, then the others, each part in raster order so that
+    // neighbouring tiles, which share input blocks, still run together.
+    // Tiles are independent, so the order changes only the schedule.
+    __syncthreads();
+    const int nv = tab.t.n_views, ntiles = tab.t.ntx * tab.t.nty;
+    const long long total = tab.b.status->bin_total;
+    const int tper = (ntiles + 1023) / 1024;
+    const int tb = min(ntiles, tid * tper), te = min(ntiles, tb + tper);
+    auto heavy = [&](int t) {
+        long long e = 0;
+        for (int v = 0; v < nv; ++v) e += counts[t * nv + v];
+        return 2 * e * ntiles > 3 * total;  // more than 1.5x the mean
+    };
+    int nh = 0;
+    for (int t = tb; t < te; ++t) nh += heavy(t) ? 1 : 0;
+    int hx = nh;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y2 = __shfl_up_sync(0xffffffffu, hx, o);
+        if (lane >= o) hx += y2;
+    }
+    __syncthreads();
+    if (lane == 31) warp_sums[warp] = hx;
+    __syncthreads();
+    if (warp == 0) {
+        int s2 = warp_sums[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y2 = __shfl_up_sync(0xffffffffu, s2, o);
+            if (lane >= o) s2 += y2;
+        }
+        warp_sums[lane] = s2;
+    }
+    __syncthreads();
+    const int hbefore = hx - nh + (warp > 0 ? warp_sums[warp - 1] : 0);
+    const int nheavy = warp_sums[31];
+    int ph = hbefore, pl = nheavy + (tb - hbefore);
+    for (int t = tb; t < te; ++t) {
+        if (heavy(t))
+            tab.b.tile_order[ph++] = t;
+        else
+            tab.b.tile_order[pl++] = t;
+    }
 }
 
 // Grid (ceil(max_blocks / 256), max_views, slots): one thread per binning

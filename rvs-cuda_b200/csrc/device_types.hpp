@@ -145,6 +145,7 @@ struct SlotBuffers {
     uint8_t* holes;      // Wo*Ho hole mask (1 = no view covers the pixel)
     uint64_t* scan[4];   // Wo*Ho inpainting scratch each
     uint64_t* inpaint_seg;  // column-group minima of the inpainting passes
+    int* tile_order;        // output tiles, most bin entries first (raster launch order)
     float4* pcolor;      // Precision != 1: blended colour per raster pixel
     int32_t* psrc;       // Precision != 1: inpainting source of every hole
 };

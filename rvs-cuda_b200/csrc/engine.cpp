@@ -85,6 +85,7 @@ size_t SlotWorkspace::bytes_for(const rvsb_scene* sc, int wo, int ho, bool resca
     return sizeof(DevStatus) + n.vert * sizeof(float4) + n.bbox * sizeof(int4) + 3 * n.bins * sizeof(int) +
            n.list * sizeof(int) + n.out * (sizeof(uint64_t) * 5 + 1) +
            (size_t)INPAINT_MAX_GROUPS * ((wo + 31) / 32) * 64 * sizeof(uint64_t) +
+           n.bins / std::max<size_t>(1, sc->cams.size()) * sizeof(int) +
            (rescale ? n.out * (sizeof(float4) + 2 * sizeof(int32_t)) : 0);
 }
 
@@ -117,6 +118,11 @@ void SlotWorkspace::ensure(rvsb_context* ctx, const rvsb_scene* sc, int wo, int 
     if (n.list > cap_list) {
         list.alloc(ctx, n.list * sizeof(int));
         cap_list = n.list;
+    }
+    const size_t tiles = (size_t)((wo + MIN_TILE_W - 1) / MIN_TILE_W) * ((ho + MIN_TILE_H - 1) / MIN_TILE_H);
+    if (tiles > cap_tiles) {
+        tile_order.alloc(ctx, tiles * sizeof(int));
+        cap_tiles = tiles;
     }
     const size_t strips = (size_t)(wo + 31) / 32;
     if (strips > cap_strips) {
@@ -330,6 +336,7 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
     B.holes = ws.holes.as<uint8_t>();
     for (int s = 0; s < 4; ++s) B.scan[s] = ws.scan[s].as<uint64_t>();
     B.inpaint_seg = ws.inpaint_seg.as<uint64_t>();
+    B.tile_order = ws.tile_order.as<int>();
     if (rd.rescale) {
         B.pcolor = ws.pcolor.as<float4>();
         B.psrc = r.dbg.inpaint_source ? r.dbg.inpaint_source : ws.psrc.as<int32_t>();

@@ -70,6 +70,8 @@ struct SlotWorkspace {
     DevMem status, counts, offsets, cursor, list, codes, holes, scan[4], vert, bbox;
     DevMem aux_depth, aux_valid;  // blended depth / validity (auxiliary outputs only)
     DevMem inpaint_seg;           // column-group minima of the inpainting passes
+    DevMem tile_order;            // raster launch order of the output tiles
+    size_t cap_tiles = 0;
     DevMem ms_view, ms_hsum, ms_hcnt, ms_blur;  // multispectral blending only
     size_t cap_ms = 0;            // view-pixels the multispectral buffers hold
     void ensure_ms(rvsb_context* ctx, int n_views, int wo, int ho);

@@ -396,8 +396,8 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_co
     __shared__ int s_off[C::VG];
     const SlotTable& tab = tabs.at(blockIdx.y);
     const DevTarget& T = tab.t;
-    const int tile = blockIdx.x;
-    if (tile >= T.ntx * T.nty) return;
+    if ((int)blockIdx.x >= T.ntx * T.nty) return;
+    const int tile = tab.b.tile_order[blockIdx.x];
     const int* __restrict__ counts = tab.b.counts;
     const int* __restrict__ offsets = tab.b.offsets;
     const int* __restrict__ list = tab.b.list;
