@@ -585,11 +585,23 @@ int launch_scans(const Src& src, int max_w, int max_h, int images, int G, cudaSt
     return launches;
 }
 
-// Row groups per strip for the column passes: about two CTAs per SM.
+// Row groups per strip for the column passes.
+// The column kernels hold one 1024-thread CTA per SM (their registers), so
+// the groups are sized for one wave: a second, partial wave would cost as
+// much as the first.
+int sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 148;
+    }
+    return n;
+}
+
 int column_groups(int max_w, int images) {
+    static const int sms = sm_count();
     const int strips = (max_w + 31) / 32;
-    const int want = (2 * 148 + strips * images - 1) / (strips * images);
-    return std::max(1, std::min(INPAINT_MAX_GROUPS, want));
+    return std::max(1, std::min(INPAINT_MAX_GROUPS, sms / (strips * images)));
 }
 
 }  // namespace
