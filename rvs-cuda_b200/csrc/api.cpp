@@ -271,7 +271,17 @@ rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int 
             auto col = std::make_unique<DevMem>();
             col->alloc(ctx, (size_t)inputs[v].width * inputs[v].height * sizeof(uint64_t));
             sc->color.push_back(std::move(col));
+            auto lut = std::make_unique<DevMem>();
+            lut->alloc(ctx, 65536 * sizeof(float));
+            const rvsb_camera& cam = inputs[v];
+            launch_depth_lut(cam.depth_range[0], cam.depth_range[1],
+                             1.0f / (float)((1u << cam.bit_depth_depth) - 1u), cam.has_invalid_depth,
+                             lut->as<float>(), nullptr);
+            check(cudaPeekAtLastError(), "depth table");
+            sc->depth_lut.push_back(std::move(lut));
         }
+        // The depth tables must be complete before any stream uses them.
+        check(cudaStreamSynchronize(nullptr), "depth tables");
         sc->uploaded.assign(n_inputs, false);
         *out = sc.release();
         return RVSB_OK;

@@ -34,14 +34,17 @@ __device__ __forceinline__ float smax(float a, float b) { return (a < b) ? b : a
 
 // Depth decode of process_input_frame.cu:346-385 (normalize kernel, built by
 // nvcc with fused multiply-add: near + d*(far-near) is one fma).
-__device__ __forceinline__ float decode_depth(const DevView& V, size_t idx) {
-    const float dd = __fmul_rn((float)V.pd[idx], V.depth_scale);
+// A depth sample takes one of 65536 values, so the warp reads the decoded
+// depth from a per-view table built with this function (depth_lut_kernel).
+__device__ __forceinline__ float decode_depth_raw(float near_, float far_, float depth_scale, int has_invalid,
+                                                 uint32_t raw) {
+    const float dd = __fmul_rn((float)raw, depth_scale);
     float z;
-    if (V.far_ >= 1000.f)
-        z = __fdiv_rn(V.near_, dd);
+    if (far_ >= 1000.f)
+        z = __fdiv_rn(near_, dd);
     else
-        z = __fdiv_rn(__fmul_rn(V.far_, V.near_), __fmaf_rn(dd, __fsub_rn(V.far_, V.near_), V.near_));
-    if (V.has_invalid && z == 0.f) z = qnan();
+        z = __fdiv_rn(__fmul_rn(far_, near_), __fmaf_rn(dd, __fsub_rn(far_, near_), near_));
+    if (has_invalid && z == 0.f) z = qnan();
     return z;
 }
 
@@ -49,9 +52,12 @@ __device__ __forceinline__ float decode_depth(const DevView& V, size_t idx) {
 // PerspectiveUnprojector.cpp:59-86 / EquirectangularUnprojector.cpp:55-98,
 // SynthesizedView.cpp:68-79 and PerspectiveProjector.cpp:59-87 /
 // EquirectangularProjector.cpp:60-99.
-__device__ __forceinline__ float4 warp_vertex(const DevView& V, const DevTarget& T, int i, int j) {
+// View: DevView, or a copy of the fields used here (the warp kernel keeps
+// them in registers).
+template <class View>
+__device__ __forceinline__ float4 warp_vertex(const View& V, const DevTarget& T, int i, int j) {
     const size_t idx = (size_t)i * V.w + j;
-    const float d = decode_depth(V, idx);
+    const float d = __ldg(V.depth_lut + __ldg(V.pd + idx));
     float x0, x1, x2;
     if (V.proj == 1) {
         const float ct = V.erp_row[2 * i], st = V.erp_row[2 * i + 1];

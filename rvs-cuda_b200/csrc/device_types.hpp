@@ -32,6 +32,7 @@ struct DevView {
     const uint16_t* pu;
     const uint16_t* pv;
     const uint16_t* pd;
+    const float* depth_lut;               // 65536 decoded depths, indexed by the raw sample
     const float* erp_row;                 // ERP: per row (cos theta, sin theta), 2*h floats
     const float* erp_col;                 // ERP: per column (cos phi, sin phi), 2*w floats
     const uint64_t* color;                // h*w decoded colour: Y | 4U << 18 | 4V << 36

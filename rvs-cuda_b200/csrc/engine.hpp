@@ -183,6 +183,7 @@ struct rvsb_scene {
     std::vector<std::unique_ptr<rvsb::DevMem>> planes;  // 4 per view: y, u, v, depth
     std::vector<std::unique_ptr<rvsb::DevMem>> erp;     // 2 per view: rows, cols (ERP inputs)
     std::vector<std::unique_ptr<rvsb::DevMem>> color;   // 1 per view: decoded colour words
+    std::vector<std::unique_ptr<rvsb::DevMem>> depth_lut;  // 1 per view: 65536 decoded depths
     std::vector<bool> uploaded;
     std::unique_ptr<rvsb::BatchCore> single;            // the per-view calls: a batch of one
     int last_launches = 0;

@@ -87,6 +87,11 @@ void launch_resize(const Tabs& tabs, const BatchShape& shape, cudaStream_t strea
 
 void launch_decode_views(const DecodeJobs& jobs, int n, int max_w, int max_h, cudaStream_t s);
 
+// The depth table of one input view: the decoded depth (normalised
+// disparity with near / far, rvs_cuda_lib/src/process_input_frame.cu:346-385)
+// of every 16-bit sample, 65536 floats.
+void launch_depth_lut(float near_, float far_, float depth_scale, int has_invalid, float* out, cudaStream_t s);
+
 // Decodes the colour planes of one input view into packed per-pixel words.
 void launch_decode_color(const uint16_t* y, const uint16_t* u, const uint16_t* v, int w, int h, uint64_t* out,
                          cudaStream_t s);

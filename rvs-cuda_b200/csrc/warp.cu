@@ -82,7 +82,30 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
     const int view = blockIdx.z % max_views;
     const DevTarget& T = tab.t;
     if (view >= T.n_views) return;
-    const DevView& V = tab.v[view];
+    // The view's fields used per vertex, in registers: tab.v[view] is
+    // indexed by the grid, so each use would otherwise be a load.
+    struct RegView {
+        int w, h, proj, nbx, nby;
+        float f0, f1, p0, p1;
+        float R[9], t[3];
+        const uint16_t* pd;
+        const float* depth_lut;
+        const float* erp_row;
+        const float* erp_col;
+        float4* vert;
+        int4* bbox;
+    } V;
+    {
+        const DevView& G = tab.v[view];
+        V.w = G.w; V.h = G.h; V.proj = G.proj; V.nbx = G.nbx; V.nby = G.nby;
+        V.f0 = G.f0; V.f1 = G.f1; V.p0 = G.p0; V.p1 = G.p1;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) V.R[k] = G.R[k];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) V.t[k] = G.t[k];
+        V.pd = G.pd; V.depth_lut = G.depth_lut; V.erp_row = G.erp_row; V.erp_col = G.erp_col;
+        V.vert = G.vert; V.bbox = G.bbox;
+    }
     const int j0 = blockIdx.x * VT, i0 = blockIdx.y * VT;
     if (j0 >= V.w || i0 >= V.h) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -170,7 +193,17 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
     if (lane == 0 && entries > 0) atomicAdd(&tab.b.status->bin_total, entries);
 }
 
+// Decoded depth of every possible 16-bit sample of one view.
+__global__ void depth_lut_kernel(float near_, float far_, float depth_scale, int has_invalid, float* out) {
+    const uint32_t raw = blockIdx.x * blockDim.x + threadIdx.x;
+    if (raw < 65536u) out[raw] = decode_depth_raw(near_, far_, depth_scale, has_invalid, raw);
+}
+
 }  // namespace
+
+void launch_depth_lut(float near_, float far_, float depth_scale, int has_invalid, float* out, cudaStream_t s) {
+    depth_lut_kernel<<<256, 256, 0, s>>>(near_, far_, depth_scale, has_invalid, out);
+}
 
 template <class Tabs>
 void launch_warp(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
