@@ -288,8 +288,8 @@ rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, i
  * (Pipeline.cpp:76-94 with its asynchronous loader and writer,
  * Pipeline.cpp:226-245) over one input camera set, with the upload of frame
  * k+1 on its own stream while frame k synthesises and the download of frame
- * k-1 on a third.  Up to two frames are in flight; a submit that would start
- * a third first waits for the oldest.  Host buffers are best pinned (else
+ * k-1 on a third.  Up to three frames are in flight; a submit that would
+ * start a fourth first waits for the oldest.  Host buffers are best pinned (else
  * the copies are synchronous) and must stay untouched until the frame's
  * rvsb_host_stream_wait returns.  Each frame's uploads are ordered after
  * the work queued on `stream` before the submit (NULL: the legacy default

@@ -22,9 +22,11 @@ struct rvsb_batch {
     std::unique_ptr<BatchCore> core;
 };
 
-// Pipelined host frames: two sets of raw device planes and output staging,
-// alternating between frames; uploads on `copy`, synthesis on `compute`,
-// downloads on `down`.
+// Pipelined host frames: three sets of raw device planes and output staging
+// used in turn; uploads on `copy`, synthesis on `compute`, downloads on
+// `down` (a second upload stream gains nothing: the uploads are bound by
+// the host link).  With three sets the upload of frame k waits only for frame k-3,
+// long finished, so the copy engine and the synthesis both stay busy.
 struct rvsb_host_stream {
     struct Set {
         std::vector<std::unique_ptr<DevMem>> planes;  // 4 per view: y, u, v, depth
@@ -35,7 +37,8 @@ struct rvsb_host_stream {
     };
     rvsb_context* ctx = nullptr;
     rvsb_scene* scene = nullptr;  // cameras, decoded colour, slot workspace
-    Set sets[2];
+    static constexpr int kDepth = 3;
+    Set sets[kDepth];
     cudaStream_t copy = nullptr, compute = nullptr, down = nullptr;
     cudaEvent_t ordered = nullptr;  // the caller's stream at submit time
     uint64_t next = 0;
@@ -575,9 +578,9 @@ rvsb_status rvsb_host_stream_submit(rvsb_host_stream* hs, const rvsb_view_planes
                 throw ArgError("null plane");
         validate_request(sc, virt, params, out_host);
         check(cudaSetDevice(ctx->device), "cudaSetDevice");
-        rvsb_host_stream::Set& S = hs->sets[hs->next % 2];
-        // The set's previous frame (two submits ago) must be complete before
-        // its planes and staging are reused.
+        rvsb_host_stream::Set& S = hs->sets[hs->next % rvsb_host_stream::kDepth];
+        // The set's previous frame (three submits ago) must be complete
+        // before its planes and staging are reused.
         if (S.busy) {
             check(cudaEventSynchronize(S.downloaded), "wait for an earlier frame");
             S.busy = false;

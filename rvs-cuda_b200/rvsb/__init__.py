@@ -216,7 +216,7 @@ class Context:
 
 class HostStream:
     """rvsb_host_stream: frames with host buffers, uploads, synthesis and
-    downloads of consecutive frames overlapped (two frames in flight)."""
+    downloads of consecutive frames overlapped (three frames in flight)."""
 
     def __init__(self, ctx, cams):
         self.ctx = ctx
