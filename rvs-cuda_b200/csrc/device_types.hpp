@@ -11,7 +11,7 @@ namespace rvsb {
 // z-buffers in shared memory and is processed by TILE_THREADS threads.
 constexpr int BLOCK_W = 8;
 constexpr int BLOCK_H = 4;
-constexpr int TILE_THREADS = 256;
+constexpr int TILE_THREADS = 512;
 // Smallest tile of any raster variant (sizes the bin arrays).
 constexpr int MIN_TILE_W = 32;
 constexpr int MIN_TILE_H = 16;

@@ -385,7 +385,7 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
 // the tile's accumulators.  After the last group the tile is quantised and
 // written.
 template <class C, class Tabs>
-__global__ void __launch_bounds__(TILE_THREADS, 4) raster_kernel(const __grid_constant__ Tabs tabs) {
+__global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_constant__ Tabs tabs) {
     // Dynamic shared memory: the group's z-buffers, the staged bin entries
     // and the tile's blend accumulators.
     extern __shared__ __align__(16) unsigned char s_raw[];
