@@ -30,6 +30,7 @@ __device__ __forceinline__ uint16_t encode_depth(float depth, const AuxPtrs& A, 
 
 template <class Tabs>
 __global__ void aux_kernel(const __grid_constant__ Tabs tabs) {
+    grid_dep_wait();
     const SlotTable& tab = tabs.at(blockIdx.z);
     const AuxPtrs& A = tab.aux;
     if (!A.on) return;
@@ -69,7 +70,7 @@ __global__ void aux_kernel(const __grid_constant__ Tabs tabs) {
 
 template <class Tabs>
 void launch_aux(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
-    aux_kernel<<<dim3((sh.max_wo / 2 + 127) / 128, sh.max_ho / 2, sh.slots), 128, 0, s>>>(tabs);
+    launch_dependent(aux_kernel<Tabs>, dim3((sh.max_wo / 2 + 127) / 128, sh.max_ho / 2, sh.slots), dim3(128), 0, s, tabs);
 }
 
 template void launch_aux<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);

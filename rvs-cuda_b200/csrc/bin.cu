@@ -10,6 +10,7 @@ namespace {
 // Exclusive scan of one slot's bin counts (one CTA of 1024 threads per slot).
 template <class Tabs>
 __global__ void __launch_bounds__(1024) bin_scan_kernel(const __grid_constant__ Tabs tabs) {
+    dev::grid_dep_wait();
     __shared__ int warp_sums[32];
     const SlotTable& tab = tabs.at(blockIdx.x);
     const int* counts = tab.b.counts;
@@ -99,6 +100,7 @@ __global__ void __launch_bounds__(1024) bin_scan_kernel(const __grid_constant__ 
 // block of view blockIdx.y of slot blockIdx.z.
 template <class Tabs>
 __global__ void bin_fill_kernel(const __grid_constant__ Tabs tabs) {
+    dev::grid_dep_wait();
     const SlotTable& tab = tabs.at(blockIdx.z);
     const int v = blockIdx.y;
     if (v >= tab.t.n_views || tab.b.status->bin_overflow) return;
@@ -124,8 +126,8 @@ __global__ void bin_fill_kernel(const __grid_constant__ Tabs tabs) {
 template <class Tabs>
 void launch_bin(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
     dim3 grid((sh.max_blocks + 255) / 256, sh.max_views, sh.slots);
-    bin_scan_kernel<<<sh.slots, 1024, 0, s>>>(tabs);
-    bin_fill_kernel<<<grid, 256, 0, s>>>(tabs);
+    launch_dependent(bin_scan_kernel<Tabs>, dim3(sh.slots), dim3(1024), 0, s, tabs);
+    launch_dependent(bin_fill_kernel<Tabs>, grid, dim3(256), 0, s, tabs);
 }
 
 template void launch_bin<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);

@@ -52,6 +52,7 @@ __global__ void decode_color_kernel(const uint16_t* __restrict__ py, const uint1
 
 // All views of a frame in one launch: grid (ceil(max_w / 2 / 128), max_h / 2, views).
 __global__ void decode_views_kernel(const __grid_constant__ DecodeJobs jobs) {
+    grid_dep_wait();
     const DecodeJob& J = jobs.v[blockIdx.z];
     const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y;
     if (bx >= J.w / 2 || by >= J.h / 2) return;
@@ -61,7 +62,7 @@ __global__ void decode_views_kernel(const __grid_constant__ DecodeJobs jobs) {
 }  // namespace
 
 void launch_decode_views(const DecodeJobs& jobs, int n, int max_w, int max_h, cudaStream_t s) {
-    decode_views_kernel<<<dim3((max_w / 2 + 127) / 128, max_h / 2, n), 128, 0, s>>>(jobs);
+    launch_dependent(decode_views_kernel, dim3((max_w / 2 + 127) / 128, max_h / 2, n), dim3(128), 0, s, jobs);
 }
 
 void launch_decode_color(const uint16_t* y, const uint16_t* u, const uint16_t* v, int w, int h, uint64_t* out,

@@ -23,6 +23,13 @@ constexpr uint64_t kCodeMask = (1ull << 48) - 1;
 
 __device__ __forceinline__ float qnan() { return __int_as_float(0x7fffffff); }
 
+// First statement of every synthesis kernel: with programmatic dependent
+// launch (launch_dependent in kernels.hpp) the kernel's CTAs may be resident
+// before the previous kernel on the stream has finished; this waits until
+// it has, and its writes are visible.  Without that launch attribute it
+// returns at once.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // static_cast<int>(float) as compiled for x86-64 (cvttss2si): INT_MIN for
 // NaN or out-of-range values.
 __device__ __forceinline__ int x86_cvt(float x) {

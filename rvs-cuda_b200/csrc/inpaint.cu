@@ -137,6 +137,7 @@ constexpr int SEG = 32 * CB;
 
 template <class Src>
 __global__ void __launch_bounds__(32 * ROW_WARPS) inpaint_row0_kernel(const __grid_constant__ Src src) {
+    grid_dep_wait();
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
@@ -228,6 +229,7 @@ __device__ __forceinline__ GroupRows group_rows(const Region& rg, int G, int w) 
 // from the minima of the groups above it.
 template <class Src, bool PRE>
 __global__ void __launch_bounds__(1024) inpaint_col0_kernel(const __grid_constant__ Src src, int G) {
+    grid_dep_wait();
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
@@ -308,6 +310,7 @@ __device__ __forceinline__ uint64_t ds_at(const uint64_t* DS, const Region& rg, 
 // stay.  Non-holes: (0, q).
 template <class Src>
 __global__ void inpaint_seed1_kernel(const __grid_constant__ Src src) {
+    grid_dep_wait();
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
@@ -347,6 +350,7 @@ __global__ void inpaint_seed1_kernel(const __grid_constant__ Src src) {
 // (T(q).d + q.x, q.x).  One warp per row.
 template <class Src>
 __global__ void __launch_bounds__(32 * ROW_WARPS) inpaint_row1_kernel(const __grid_constant__ Src src) {
+    grid_dep_wait();
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
@@ -399,6 +403,7 @@ __global__ void __launch_bounds__(32 * ROW_WARPS) inpaint_row1_kernel(const __gr
 // inpainting.cpp:191-198).
 template <class Src, bool PRE>
 __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constant__ Src src, int G) {
+    grid_dep_wait();
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
@@ -535,6 +540,7 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constan
 // Writes the 2x2 output blocks of the region that hold at least one hole.
 template <class Src>
 __global__ void inpaint_write_kernel(const __grid_constant__ Src src) {
+    grid_dep_wait();
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
@@ -574,13 +580,13 @@ template <class Src>
 int launch_scans(const Src& src, int max_w, int max_h, int images, int G, cudaStream_t s) {
     const int strips = (max_w + 31) / 32;
     int launches = 0;
-    inpaint_row0_kernel<<<dim3(max_h, 1, images), 32 * ROW_WARPS, 0, s>>>(src);
-    if (G > 1) inpaint_col0_kernel<Src, true><<<dim3(strips, G, images), 1024, 0, s>>>(src, G);
-    inpaint_col0_kernel<Src, false><<<dim3(strips, G, images), 1024, 0, s>>>(src, G);
-    inpaint_seed1_kernel<<<dim3((max_w + 255) / 256, max_h, images), 256, 0, s>>>(src);
-    inpaint_row1_kernel<<<dim3(max_h, 1, images), 32 * ROW_WARPS, 0, s>>>(src);
-    if (G > 1) inpaint_col1_kernel<Src, true><<<dim3(strips, G, images), 1024, 0, s>>>(src, G);
-    inpaint_col1_kernel<Src, false><<<dim3(strips, G, images), 1024, 0, s>>>(src, G);
+    launch_dependent(inpaint_row0_kernel<Src>, dim3(max_h, 1, images), dim3(32 * ROW_WARPS), 0, s, src);
+    if (G > 1) launch_dependent(inpaint_col0_kernel<Src, true>, dim3(strips, G, images), dim3(1024), 0, s, src, G);
+    launch_dependent(inpaint_col0_kernel<Src, false>, dim3(strips, G, images), dim3(1024), 0, s, src, G);
+    launch_dependent(inpaint_seed1_kernel<Src>, dim3((max_w + 255) / 256, max_h, images), dim3(256), 0, s, src);
+    launch_dependent(inpaint_row1_kernel<Src>, dim3(max_h, 1, images), dim3(32 * ROW_WARPS), 0, s, src);
+    if (G > 1) launch_dependent(inpaint_col1_kernel<Src, true>, dim3(strips, G, images), dim3(1024), 0, s, src, G);
+    launch_dependent(inpaint_col1_kernel<Src, false>, dim3(strips, G, images), dim3(1024), 0, s, src, G);
     launches = 5 + (G > 1 ? 2 : 0);
     return launches;
 }
@@ -610,7 +616,8 @@ template <class Tabs>
 int launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
     const FromTables<Tabs> src{tabs};
     const int n = launch_scans(src, sh.max_wo, sh.max_ho, sh.slots, column_groups(sh.max_wo, sh.slots), s);
-    inpaint_write_kernel<<<dim3((sh.max_wo / 2 + 127) / 128, (sh.max_ho + 1) / 2, sh.slots), 128, 0, s>>>(src);
+    launch_dependent(inpaint_write_kernel<FromTables<Tabs>>, dim3((sh.max_wo / 2 + 127) / 128, (sh.max_ho + 1) / 2, sh.slots),
+                     dim3(128), 0, s, src);
     return n + 1;
 }
 

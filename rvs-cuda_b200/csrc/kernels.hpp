@@ -43,6 +43,25 @@ struct TablePtr {
 };
 #undef RVSB_HD
 
+// Launches `kernel` after the previous kernel on `s` with programmatic
+// dependent launch: its CTAs are scheduled while the previous kernel drains
+// and wait in grid_dep_wait() (device_common.cuh) until it has finished, which
+// hides the launch gap between the dependent kernels of a synthesis.
+template <class... KArgs, class... Args>
+void launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Issues one batch of syntheses on `stream`; returns the number of kernel
 // launches, or -1 on a launch error (cudaGetLastError holds the cause).
 // `events` (optional) holds 2 * NUM_STAGES events recorded around the stages.

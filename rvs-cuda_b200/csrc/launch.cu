@@ -26,6 +26,7 @@ namespace {
 // 256), slots).
 template <class Tabs>
 __global__ void slot_init_kernel(const __grid_constant__ Tabs tabs) {
+    dev::grid_dep_wait();
     const SlotTable& tab = tabs.at(blockIdx.y);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int nbins = tab.t.ntx * tab.t.nty * tab.t.n_views;
@@ -51,7 +52,7 @@ int launch_batch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s, cudaEve
         if (ev) cudaEventRecord(ev[k], s);
     };
     mark(8);
-    slot_init_kernel<<<dim3((sh.max_bins + 255) / 256, sh.slots), 256, 0, s>>>(tabs);
+    launch_dependent(slot_init_kernel<Tabs>, dim3((sh.max_bins + 255) / 256, sh.slots), dim3(256), 0, s, tabs);
     mark(0);
     launch_warp(tabs, sh, s);
     mark(1);

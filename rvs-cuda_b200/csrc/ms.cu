@@ -24,6 +24,7 @@ constexpr int MS_THREADS = 256;
 // exclusive prefix (double sums, integer counts) is built in shared memory.
 template <class Tabs>
 __global__ void __launch_bounds__(MS_THREADS) ms_rows_kernel(const __grid_constant__ Tabs tabs) {
+    grid_dep_wait();
     extern __shared__ __align__(16) unsigned char s_raw[];
     const SlotTable& tab = tabs.at(blockIdx.z);
     const MsPtrs& M = tab.ms;
@@ -103,6 +104,7 @@ __global__ void __launch_bounds__(MS_THREADS) ms_rows_kernel(const __grid_consta
 // down the column; writes the blurred luma.
 template <class Tabs>
 __global__ void ms_cols_kernel(const __grid_constant__ Tabs tabs) {
+    grid_dep_wait();
     const SlotTable& tab = tabs.at(blockIdx.z);
     const MsPtrs& M = tab.ms;
     if (!M.on) return;
@@ -146,6 +148,7 @@ __global__ void ms_cols_kernel(const __grid_constant__ Tabs tabs) {
 // and the output samples of hole-free blocks.
 template <class Tabs>
 __global__ void ms_blend_kernel(const __grid_constant__ Tabs tabs) {
+    grid_dep_wait();
     const SlotTable& tab = tabs.at(blockIdx.z);
     const MsPtrs& M = tab.ms;
     if (!M.on) return;
@@ -203,9 +206,10 @@ __global__ void ms_blend_kernel(const __grid_constant__ Tabs tabs) {
 template <class Tabs>
 int launch_ms(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
     const size_t smem = (sizeof(double) + sizeof(int)) * (size_t)(sh.max_wo + 1);
-    ms_rows_kernel<<<dim3(sh.max_ho, sh.max_views, sh.slots), MS_THREADS, smem, s>>>(tabs);
-    ms_cols_kernel<<<dim3((sh.max_wo + 127) / 128, sh.max_views, sh.slots), 128, 0, s>>>(tabs);
-    ms_blend_kernel<<<dim3((sh.max_wo / 2 + 127) / 128, sh.max_ho / 2, sh.slots), 128, 0, s>>>(tabs);
+    launch_dependent(ms_rows_kernel<Tabs>, dim3(sh.max_ho, sh.max_views, sh.slots), dim3(MS_THREADS), smem, s, tabs);
+    launch_dependent(ms_cols_kernel<Tabs>, dim3((sh.max_wo + 127) / 128, sh.max_views, sh.slots), dim3(128), 0, s, tabs);
+    launch_dependent(ms_blend_kernel<Tabs>, dim3((sh.max_wo / 2 + 127) / 128, sh.max_ho / 2, sh.slots), dim3(128), 0, s,
+                     tabs);
     return 3;
 }
 

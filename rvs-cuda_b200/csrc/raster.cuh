@@ -386,6 +386,7 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
 // written.
 template <class C, class Tabs>
 __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_constant__ Tabs tabs) {
+    grid_dep_wait();
     // Dynamic shared memory: the group's z-buffers, the staged bin entries
     // and the tile's blend accumulators.
     extern __shared__ __align__(16) unsigned char s_raw[];
@@ -461,7 +462,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_co
 
 template <class C, class Tabs>
 void launch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
-    raster_kernel<C, Tabs><<<dim3(sh.max_tiles, sh.slots), TILE_THREADS, C::kSmemBytes, s>>>(tabs);
+    launch_dependent(raster_kernel<C, Tabs>, dim3(sh.max_tiles, sh.slots), dim3(TILE_THREADS), C::kSmemBytes, s, tabs);
 }
 
 template <class C>

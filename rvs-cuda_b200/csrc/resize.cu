@@ -75,6 +75,7 @@ __device__ __forceinline__ float3 resized(const DevTarget& T, const Filled& F, i
 // max_out_h / 2, slots).
 template <class Tabs>
 __global__ void resize_write_kernel(const __grid_constant__ Tabs tabs) {
+    grid_dep_wait();
     const SlotTable& tab = tabs.at(blockIdx.z);
     const DevTarget& T = tab.t;
     if (!T.rescale) return;
@@ -100,7 +101,8 @@ __global__ void resize_write_kernel(const __grid_constant__ Tabs tabs) {
 
 template <class Tabs>
 void launch_resize(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
-    resize_write_kernel<<<dim3((sh.max_out_w / 2 + 127) / 128, sh.max_out_h / 2, sh.slots), 128, 0, s>>>(tabs);
+    launch_dependent(resize_write_kernel<Tabs>, dim3((sh.max_out_w / 2 + 127) / 128, sh.max_out_h / 2, sh.slots),
+                     dim3(128), 0, s, tabs);
 }
 
 template void launch_resize<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);

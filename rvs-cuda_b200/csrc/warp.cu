@@ -74,6 +74,7 @@ struct Box {
 // lanes 8*b .. 8*b + 8, rows 4*warp .. 4*warp + 4.
 template <class Tabs>
 __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs tabs, int max_views) {
+    grid_dep_wait();
     __shared__ float2 s_top[8][VT];        // first row of each warp (row 4*w)
     __shared__ float2 s_row[VT + 1];       // row i0 + 32, columns j0 .. j0 + 32
     __shared__ float2 s_col[VT + 1];       // column j0 + 32, rows i0 .. i0 + 32
@@ -208,7 +209,7 @@ void launch_depth_lut(float near_, float far_, float depth_scale, int has_invali
 template <class Tabs>
 void launch_warp(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
     dim3 grid((sh.max_w + VT - 1) / VT, (sh.max_h + VT - 1) / VT, sh.slots * sh.max_views);
-    warp_kernel<<<grid, 256, 0, s>>>(tabs, sh.max_views);
+    launch_dependent(warp_kernel<Tabs>, grid, dim3(256), 0, s, tabs, sh.max_views);
 }
 
 template void launch_warp<TableParam>(const TableParam&, const BatchShape&, cudaStream_t);
