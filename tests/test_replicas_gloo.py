@@ -76,3 +76,40 @@ def test_two_gloo_ranks(tmp_path):
     n0, n1 = 3, 2
     assert list(r0[2 + n0:]) == [0, 1, 2] and list(r1[2 + n1:]) == [3, 4]
     assert len(set(r0[2:2 + n0]) | set(r1[2:2 + n1])) == 1
+
+
+def _bcast_main(rank, world, port, out_dir):
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    sys.path.insert(0, os.path.join(root, "rvs-cuda_b200"))
+    sys.path.insert(0, os.path.join(root, "oracle"))
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    from rvsb import replicas as R
+    from rvsb import scenes
+    import oracle as O
+    w, r, _ = R.init(backend="gloo", timeout_s=60)
+    wl = scenes.random_pose_small(n_views=2, w=48, h=32, seed=78)
+    # only rank 0 "reads" the input set; the others receive it
+    got = R.broadcast_planes(wl.planes if r == 0 else None, w)
+    planes = [tuple(t.numpy().view(np.uint16).reshape(np.asarray(a).shape) for t, a in zip(view, ref))
+              for view, ref in zip(got, wl.planes)]
+    same = all((a == np.asarray(b)).all() for view, ref in zip(planes, wl.planes) for a, b in zip(view, ref))
+    y, u, v = O.synthesize(wl.inputs, planes, wl.targets[0], 5.0)
+    R.barrier(w)
+    np.save(os.path.join(out_dir, f"b{r}.npy"), np.array([float(same), float(np.asarray(y, np.int64).sum())]))
+    R.finish(w)
+
+
+def test_broadcast_input_set(tmp_path):
+    """broadcast_planes: rank 0's input set arrives bit-identical on rank 1,
+    and both synthesise the same view from it."""
+    world = 2
+    port = _free_port()
+    mp.start_processes(_bcast_main, args=(world, port, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    b0 = np.load(tmp_path / "b0.npy")
+    b1 = np.load(tmp_path / "b1.npy")
+    assert b0[0] == 1.0 and b1[0] == 1.0
+    assert b0[1] == b1[1]
