@@ -72,6 +72,30 @@ def test_stages_small(ctx, case, exponent):
     assert_parity(yuv, cpu)
 
 
+@pytest.mark.parametrize("bits,far,invalid", [(10, 10.0, True), (12, 10.0, False), (16, 2000.0, True)],
+                         ids=["10bit", "12bit-valid", "16bit-far-infinite"])
+def test_depth_formats(ctx, bits, far, invalid):
+    """Depth decode through the per-view table of all 65536 samples:
+    bit depths below 16, HasInvalidDepth off, and Depth_range far >= 1000
+    (near / d), each bit-exact in the warped vertices and at parity end to
+    end."""
+    wl = scenes.random_pose_small(n_views=3, w=96, h=54, seed=21)
+    for c in wl.inputs:
+        c.bit_depth_depth = bits
+        c.depth_range[1] = far
+        c.has_invalid_depth = 1 if invalid else 0
+    target = wl.targets[0]
+    yuv, dbg, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, debug=True)
+    warped, _, _, bq = _oracle_stages(wl, target, 5.0)
+    for v, (uv, vd) in enumerate(warped):
+        g = dbg["warped"][v]
+        np.testing.assert_array_equal(g[..., 0], uv[..., 0])
+        np.testing.assert_array_equal(g[..., 1], uv[..., 1])
+        np.testing.assert_array_equal(g[..., 2], vd)
+    np.testing.assert_array_equal(~(dbg["blend_quality"] > 0), ~(bq > 0))
+    assert_parity(yuv, O.synthesize(wl.inputs, wl.planes, target, 5.0))
+
+
 @pytest.mark.parametrize("seed", [11, 12, 13])
 def test_inpaint_sources_match(ctx, seed):
     """Holes copy exactly the pixel the reference's sweeps choose."""
