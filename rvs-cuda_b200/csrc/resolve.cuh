@@ -38,7 +38,15 @@ __device__ __forceinline__ Fragment resolve_fragment(const DevView& V, unsigned 
     const int t = (int)(tri & 3u);
     const int i = (int)(tri >> V.tri_shift), j = (int)((tri >> 2) & ((1u << (V.tri_shift - 2)) - 1u));
     int ax, ay, bx, by, cx, cy;
-    tri_vertices(V.w, i, j, t, ax, ay, bx, by, cx, cy);
+    if (t < 2) {
+        // The two triangles of quad (i, j) without a branch per case:
+        // t = 0: (j, i), (j+1, i), (j, i+1); t = 1: (j+1, i+1), (j, i+1), (j+1, i).
+        ax = j + t; ay = i + t;
+        bx = j + 1 - t; by = i + t;
+        cx = j + t; cy = i + 1 - t;
+    } else {
+        tri_vertices(V.w, i, j, t, ax, ay, bx, by, cx, cy);
+    }
     const float4* vt = V.vert;
     const float4 A = __ldg(vt + (size_t)ay * V.w + ax);
     const float4 B = __ldg(vt + (size_t)by * V.w + bx);
