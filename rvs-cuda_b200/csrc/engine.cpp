@@ -444,25 +444,29 @@ int BatchCore::tune(const SlotRequest* reqs, int n, cudaStream_t s) {
     const bool graphs = use_graphs_, prof = profiling_;
     use_graphs_ = false;
     profiling_ = false;
-    int best = 0;
-    float best_ms = 0.f;
-    for (int v = 0; v < NUM_RASTER_VARIANTS; ++v) {
-        launch_variant(reqs, n, v, s);  // warm-up (first use of the variant's module)
-        // The fastest of three runs: one run alone is too noisy to rank
-        // variants that differ by a few percent.
-        float ms = 0.f;
-        for (int rep = 0; rep < 3; ++rep) {
+    // A warm-up run of every variant (first use of its module), then five
+    // rounds that time each variant once, in turn, so that a drift of the
+    // device's state affects them alike; the variant with the smallest median
+    // wins.  One run alone is too noisy to rank variants a few percent apart.
+    constexpr int kRounds = 5;
+    for (int v = 0; v < NUM_RASTER_VARIANTS; ++v) launch_variant(reqs, n, v, s);
+    float t[NUM_RASTER_VARIANTS][kRounds];
+    for (int r = 0; r < kRounds; ++r)
+        for (int v = 0; v < NUM_RASTER_VARIANTS; ++v) {
             check(cudaEventRecord(tune_ev_[0], s), "record");
             launch_variant(reqs, n, v, s);
             check(cudaEventRecord(tune_ev_[1], s), "record");
             check(cudaEventSynchronize(tune_ev_[1]), "synchronize");
-            float t = 0.f;
-            check(cudaEventElapsedTime(&t, tune_ev_[0], tune_ev_[1]), "elapsed");
-            ms = rep == 0 ? t : std::min(ms, t);
+            check(cudaEventElapsedTime(&t[v][r], tune_ev_[0], tune_ev_[1]), "elapsed");
         }
-        if (v == 0 || ms < best_ms) {
+    int best = 0;
+    float best_ms = 0.f;
+    for (int v = 0; v < NUM_RASTER_VARIANTS; ++v) {
+        std::sort(t[v], t[v] + kRounds);
+        const float med = t[v][kRounds / 2];
+        if (v == 0 || med < best_ms) {
             best = v;
-            best_ms = ms;
+            best_ms = med;
         }
     }
     use_graphs_ = graphs;
