@@ -143,6 +143,22 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
             launch_decode_views(jobs, (int)sc->cams.size(), max_w, max_h, s);
             decodes = 1;
             check(cudaPeekAtLastError(), "decode colour");
+            // Depth ranges of the ERP views' vertex tiles, from this frame's depth.
+            TileDepthJobs tj{};
+            int n_erp = 0, ew = 0, eh = 0;
+            for (size_t v = 0; v < sc->cams.size(); ++v) {
+                const rvsb_camera& c = sc->cams[v];
+                if (c.projection != RVSB_PROJ_EQUIRECTANGULAR) continue;
+                tj.v[n_erp++] = TileDepthJob{frame[v].depth, sc->depth_lut[v]->as<float>(),
+                                             sc->tile_depth[v]->as<float2>(), c.width, c.height};
+                ew = std::max(ew, c.width);
+                eh = std::max(eh, c.height);
+            }
+            if (n_erp > 0) {
+                launch_tile_depth(tj, n_erp, ew, eh, s);
+                decodes = 2;
+                check(cudaPeekAtLastError(), "tile depth ranges");
+            }
         }
         SlotRequest r;
         r.scene = sc;
@@ -259,8 +275,10 @@ rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int 
             }
             auto r = std::make_unique<DevMem>();
             auto c = std::make_unique<DevMem>();
+            auto cone = std::make_unique<DevMem>();
+            auto tdep = std::make_unique<DevMem>();
             if (inputs[v].projection == RVSB_PROJ_EQUIRECTANGULAR) {
-                std::vector<float> rows, cols;
+                std::vector<float> rows, cols, cones;
                 erp_tables(inputs[v], rows, cols);
                 r->alloc(ctx, rows.size() * sizeof(float));
                 c->alloc(ctx, cols.size() * sizeof(float));
@@ -268,7 +286,14 @@ rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int 
                       "upload ERP rows");
                 check(cudaMemcpy(c->ptr, cols.data(), cols.size() * sizeof(float), cudaMemcpyHostToDevice),
                       "upload ERP columns");
+                erp_tile_cones(inputs[v], rows, cols, WARP_TILE, cones);
+                cone->alloc(ctx, cones.size() * sizeof(float));
+                check(cudaMemcpy(cone->ptr, cones.data(), cones.size() * sizeof(float), cudaMemcpyHostToDevice),
+                      "upload ERP tile cones");
+                tdep->alloc(ctx, cones.size() / 4 * sizeof(float2));
             }
+            sc->erp_cone.push_back(std::move(cone));
+            sc->tile_depth.push_back(std::move(tdep));
             sc->erp.push_back(std::move(r));
             sc->erp.push_back(std::move(c));
             auto col = std::make_unique<DevMem>();
@@ -317,6 +342,13 @@ rvsb_status rvsb_scene_upload(rvsb_scene* sc, int view, const rvsb_view_planes* 
                             sc->planes[view * 4 + 2]->as<uint16_t>(), c.width, c.height,
                             sc->color[view]->as<uint64_t>(), s);
         check(cudaPeekAtLastError(), "decode colour");
+        if (c.projection == RVSB_PROJ_EQUIRECTANGULAR) {
+            TileDepthJobs jobs{};
+            jobs.v[0] = TileDepthJob{sc->planes[view * 4 + 3]->as<uint16_t>(), sc->depth_lut[view]->as<float>(),
+                                     sc->tile_depth[view]->as<float2>(), c.width, c.height};
+            launch_tile_depth(jobs, 1, c.width, c.height, s);
+            check(cudaPeekAtLastError(), "tile depth ranges");
+        }
         sc->uploaded[view] = true;
         return RVSB_OK;
     });

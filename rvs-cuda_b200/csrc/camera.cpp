@@ -3,6 +3,7 @@
 // reference's float cos/sin calls.
 #include "camera.hpp"
 
+#include <algorithm>
 #include <cmath>
 
 namespace rvsb {
@@ -79,6 +80,51 @@ void erp_tables(const rvsb_camera& in, std::vector<float>& rows, std::vector<flo
         cols[2 * j] = fcos(phi);
         cols[2 * j + 1] = fsin(phi);
     }
+}
+
+void erp_tile_cones(const rvsb_camera& in, const std::vector<float>& rows, const std::vector<float>& cols,
+                    int tile, std::vector<float>& out) {
+    const int w = in.width, h = in.height;
+    const int ntx = (w + tile - 1) / tile, nty = (h + tile - 1) / tile;
+    out.assign((size_t)ntx * nty * 4, 0.f);
+    auto dir = [&](int i, int j, double d[3]) {
+        d[0] = (double)rows[2 * i] * cols[2 * j];
+        d[1] = (double)rows[2 * i] * cols[2 * j + 1];
+        d[2] = rows[2 * i + 1];
+        const double n = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        for (int k = 0; k < 3; ++k) d[k] /= n;
+    };
+    auto angle = [](const double a[3], const double b[3]) {
+        // atan2(|a x b|, a . b): accurate for small angles
+        const double cx = a[1] * b[2] - a[2] * b[1], cy = a[2] * b[0] - a[0] * b[2], cz = a[0] * b[1] - a[1] * b[0];
+        return std::atan2(std::sqrt(cx * cx + cy * cy + cz * cz), a[0] * b[0] + a[1] * b[1] + a[2] * b[2]);
+    };
+    for (int ty = 0; ty < nty; ++ty)
+        for (int tx = 0; tx < ntx; ++tx) {
+            const int r0 = std::max(0, ty * tile - 1), r1 = std::min(h - 1, ty * tile + tile);
+            const int c0 = std::max(0, tx * tile - 1), c1 = std::min(w - 1, tx * tile + tile);
+            double dc[3], d[3], prev[3];
+            dir((r0 + r1) / 2, (c0 + c1) / 2, dc);
+            double rho = 0.0, step = 0.0;
+            // The angle to a fixed direction peaks on the region's boundary;
+            // between two boundary samples it can exceed both by at most
+            // their separation, so the largest separation is added.
+            auto visit = [&](int i, int j, bool first) {
+                dir(i, j, d);
+                rho = std::max(rho, angle(dc, d));
+                if (!first) step = std::max(step, angle(prev, d));
+                prev[0] = d[0]; prev[1] = d[1]; prev[2] = d[2];
+            };
+            for (int j = c0; j <= c1; ++j) visit(r0, j, j == c0);
+            for (int i = r0; i <= r1; ++i) visit(i, c1, i == r0);
+            for (int j = c1; j >= c0; --j) visit(r1, j, j == c1);
+            for (int i = r1; i >= r0; --i) visit(i, c0, i == r1);
+            float* o = &out[((size_t)ty * ntx + tx) * 4];
+            o[0] = (float)dc[0];
+            o[1] = (float)dc[1];
+            o[2] = (float)dc[2];
+            o[3] = (float)(rho + step + 1e-4);
+        }
 }
 
 void erp_projector_constants(const rvsb_camera& v, float& u0, float& v0, float& du_dphi, float& dv_dtheta) {

@@ -20,6 +20,14 @@ void relative_pose(const rvsb_camera& in, const rvsb_camera& virt, float R[9], f
 // correctly to float.
 void erp_tables(const rvsb_camera& in, std::vector<float>& rows, std::vector<float>& cols);
 
+// Direction cones of an ERP input's vertex tiles (tile x tile pixels, each
+// grown by one pixel on every side and clamped to the image), four floats
+// per tile in row-major tile order: the unit direction of the region's
+// middle pixel and an angle in radians bounding the angle from it to every
+// pixel direction of the region (from the unprojection tables).
+void erp_tile_cones(const rvsb_camera& in, const std::vector<float>& rows, const std::vector<float>& cols,
+                    int tile, std::vector<float>& out);
+
 // Projector constants of EquirectangularProjector.cpp:66-72.
 void erp_projector_constants(const rvsb_camera& virt, float& u0, float& v0, float& du_dphi,
                              float& dv_dtheta);

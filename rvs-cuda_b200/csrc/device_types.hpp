@@ -11,6 +11,9 @@ namespace rvsb {
 // z-buffers in shared memory and is processed by TILE_THREADS threads.
 constexpr int BLOCK_W = 8;
 constexpr int BLOCK_H = 4;
+// Vertex tile of the warp kernel (WARP_TILE x WARP_TILE input pixels per CTA),
+// also the unit of the ERP input culling tables.
+constexpr int WARP_TILE = 32;
 constexpr int TILE_THREADS = 512;
 // Smallest tile of any raster variant (sizes the bin arrays).
 constexpr int MIN_TILE_W = 32;
@@ -35,6 +38,12 @@ struct DevView {
     const float* depth_lut;               // 65536 decoded depths, indexed by the raw sample
     const float* erp_row;                 // ERP: per row (cos theta, sin theta), 2*h floats
     const float* erp_col;                 // ERP: per column (cos phi, sin phi), 2*w floats
+    // ERP inputs, per WARP_TILE x WARP_TILE vertex tile grown by one pixel:
+    // the unit direction of its centre and an angle bounding every vertex
+    // direction from it (x, y, z, radius), and the range of its decoded
+    // depths (min, max); used to skip tiles no output pixel can come from.
+    const float4* erp_cone;
+    const float2* tile_depth;
     const uint64_t* color;                // h*w decoded colour: Y | 4U << 18 | 4V << 36
     float4* vert;                         // h*w warped vertices (u, v, z, 0)
     int4* bbox;                           // per binning block: x0, y0, x1, y1 (x0 > x1: empty)
@@ -48,6 +57,11 @@ struct DevTarget {
     int wo, ho;
     int proj;
     int wrap;                             // horizontal wrap (ERP output, full range)
+    // Perspective output: the planes u = -1, u = W + 1, v = -1, v = H + 1 in
+    // the virtual camera's frame (a . y > 0 beyond each, for y0 > 0); cull
+    // enables skipping ERP input tiles wholly beyond one of them.
+    int cull;
+    float cull_plane[4][3];
     float f0, f1, p0, p1;                 // perspective
     float u0, v0, du_dphi, dv_dtheta;     // equirectangular
     int bits;                             // output bit depth

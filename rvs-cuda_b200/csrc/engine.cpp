@@ -250,6 +250,8 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
         if (c.projection == RVSB_PROJ_EQUIRECTANGULAR) {
             V.erp_row = sc->erp[v * 2 + 0]->as<float>();
             V.erp_col = sc->erp[v * 2 + 1]->as<float>();
+            V.erp_cone = sc->erp_cone[v]->as<float4>();
+            V.tile_depth = sc->tile_depth[v]->as<float2>();
         }
         V.color = sc->color[v]->as<uint64_t>();
         V.depth_lut = sc->depth_lut[v]->as<float>();
@@ -288,6 +290,18 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
     D.p0 = virt.principle_point[0];
     D.p1 = virt.principle_point[1];
     if (virt.projection == RVSB_PROJ_EQUIRECTANGULAR) erp_projector_constants(virt, D.u0, D.v0, D.du_dphi, D.dv_dtheta);
+    // ERP input tiles wholly beyond a side of a perspective output are
+    // skipped, except when the warped vertices themselves are asked for.
+    if (virt.projection == RVSB_PROJ_PERSPECTIVE && p.precision == 1.f && !r.dbg.warped_uvz) {
+        const float f0 = virt.focal[0], f1 = virt.focal[1], p0 = virt.principle_point[0], p1 = virt.principle_point[1];
+        const float W = (float)virt.width, H = (float)virt.height;
+        const float planes[4][3] = {{-(p0 + 1.f), f0, 0.f},      // u < -1
+                                    {p0 - W - 1.f, -f0, 0.f},    // u > W + 1
+                                    {-(p1 + 1.f), 0.f, f1},      // v < -1
+                                    {p1 - H - 1.f, 0.f, -f1}};   // v > H + 1
+        std::memcpy(D.cull_plane, planes, sizeof(planes));
+        D.cull = 1;
+    }
     D.bits = virt.bit_depth_color;
     D.max_val = (1u << virt.bit_depth_color) - 1u;
     D.blend_exp = p.blending_factor;

@@ -184,6 +184,8 @@ struct rvsb_scene {
     std::vector<std::unique_ptr<rvsb::DevMem>> erp;     // 2 per view: rows, cols (ERP inputs)
     std::vector<std::unique_ptr<rvsb::DevMem>> color;   // 1 per view: decoded colour words
     std::vector<std::unique_ptr<rvsb::DevMem>> depth_lut;  // 1 per view: 65536 decoded depths
+    // ERP views: per vertex tile, direction cone and depth range (culling)
+    std::vector<std::unique_ptr<rvsb::DevMem>> erp_cone, tile_depth;
     std::vector<bool> uploaded;
     std::unique_ptr<rvsb::BatchCore> single;            // the per-view calls: a batch of one
     int last_launches = 0;

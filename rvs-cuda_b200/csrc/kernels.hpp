@@ -111,6 +111,19 @@ void launch_decode_views(const DecodeJobs& jobs, int n, int max_w, int max_h, cu
 // of every 16-bit sample, 65536 floats.
 void launch_depth_lut(float near_, float far_, float depth_scale, int has_invalid, float* out, cudaStream_t s);
 
+// Depth range (min, max) of every WARP_TILE x WARP_TILE vertex tile grown by
+// one pixel, for the ERP input culling; up to MAX_VIEWS views in one launch.
+struct TileDepthJob {
+    const uint16_t* depth;   // raw depth plane
+    const float* lut;        // the view's decoded-depth table
+    float2* out;             // one (min, max) per tile, row-major
+    int w, h;
+};
+struct TileDepthJobs {
+    TileDepthJob v[MAX_VIEWS];
+};
+void launch_tile_depth(const TileDepthJobs& jobs, int n, int max_w, int max_h, cudaStream_t s);
+
 // Decodes the colour planes of one input view into packed per-pixel words.
 void launch_decode_color(const uint16_t* y, const uint16_t* u, const uint16_t* v, int w, int h, uint64_t* out,
                          cudaStream_t s);

@@ -8,7 +8,7 @@ namespace {
 
 using namespace dev;
 
-constexpr int VT = 32;             // vertex tile: 32 x 32 vertices per CTA
+constexpr int VT = WARP_TILE;      // vertex tile: 32 x 32 vertices per CTA
 constexpr int ROWS = VT / 8;       // vertex rows per thread (8 warps)
 static_assert(ROWS == BLOCK_H && VT == 4 * BLOCK_W, "a warp covers one row of 4 binning blocks");
 
@@ -72,6 +72,37 @@ struct Box {
 // then reduces the boxes of binning-block row by = 8*blockIdx.y + warp: the
 // (BLOCK_W + 1) x (BLOCK_H + 1) vertices of block bx are the columns of
 // lanes 8*b .. 8*b + 8, rows 4*warp .. 4*warp + 4.
+// Whether vertex tile (blockIdx.x, blockIdx.y) of an ERP input view lies, with
+// its one-pixel ring, wholly beyond one of the output's side planes.  A
+// vertex is x = z * d (d within the tile's cone, z within its depth range),
+// seen by the virtual camera as y = R x + t; beyond plane a when a . y > 0,
+// i.e. z * (b . d) + c > 0 with b = R^T a, c = a . t.  Over the cone
+// b . d >= b . dc - |b| rho; the smallest value over z is at the near or far
+// end of the range.  A relative margin absorbs the float rounding of the
+// vertices, and the planes sit one pixel outside the image.
+template <class View, class Target>
+__device__ __forceinline__ bool tile_culled(const View& V, const Target& T) {
+    const int ntx = (V.w + VT - 1) / VT;
+    const size_t k = (size_t)blockIdx.y * ntx + blockIdx.x;
+    const float4 cone = V.erp_cone[k];
+    const float2 zr = V.tile_depth[k];
+    if (!(zr.x > 0.f && zr.x <= zr.y)) return false;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const float* a = T.cull_plane[p];
+        float b[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) b[j] = a[0] * V.R[j] + a[1] * V.R[3 + j] + a[2] * V.R[6 + j];
+        const float c = a[0] * V.t[0] + a[1] * V.t[1] + a[2] * V.t[2];
+        const float nb = sqrtf(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+        const float m = b[0] * cone.x + b[1] * cone.y + b[2] * cone.z - nb * cone.w;
+        const float z = m >= 0.f ? zr.x : zr.y;
+        const float L = z * m + c;
+        if (L > 1e-3f * (fabsf(c) + z * nb) && isfinite(L)) return true;
+    }
+    return false;
+}
+
 template <class Tabs>
 __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs tabs, int max_views) {
     grid_dep_wait();
@@ -95,6 +126,8 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
         const float* erp_col;
         float4* vert;
         int4* bbox;
+        const float4* erp_cone;
+        const float2* tile_depth;
     } V;
     {
         const DevView& G = tab.v[view];
@@ -106,10 +139,27 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
         for (int k = 0; k < 3; ++k) V.t[k] = G.t[k];
         V.pd = G.pd; V.depth_lut = G.depth_lut; V.erp_row = G.erp_row; V.erp_col = G.erp_col;
         V.vert = G.vert; V.bbox = G.bbox;
+        V.erp_cone = G.erp_cone; V.tile_depth = G.tile_depth;
     }
     const int j0 = blockIdx.x * VT, i0 = blockIdx.y * VT;
     if (j0 >= V.w || i0 >= V.h) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (T.cull && V.erp_cone && tile_culled(V, T)) {
+        // No triangle with a vertex of this tile can cover an output pixel:
+        // every vertex of the tile and of the pixel ring around it lies
+        // beyond one side of the output (or behind the camera).  Its
+        // vertices are stored as NaN, which no triangle is emitted from, and
+        // its blocks get empty boxes.
+        const float nan = qnan();
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+            const int i = i0 + warp * ROWS + r, j = j0 + lane;
+            if (i < V.h && j < V.w) V.vert[(size_t)i * V.w + j] = make_float4(nan, nan, nan, 0.f);
+        }
+        const int bx = blockIdx.x * 4 + (lane >> 3), by = blockIdx.y * 8 + warp;
+        if ((lane & 7) == 0 && bx < V.nbx && by < V.nby) V.bbox[by * V.nbx + bx] = make_int4(1, 1, 0, 0);
+        return;
+    }
     const bool wrap = T.wrap != 0;
     const bool seam = wrap && blockIdx.x == 0;
     const int j = j0 + lane;
@@ -194,6 +244,43 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
     if (lane == 0 && entries > 0) atomicAdd(&tab.b.status->bin_total, entries);
 }
 
+// Range of the decoded depths of one vertex tile grown by one pixel (NaN
+// samples ignored).  Grid (tiles x, tiles y, views), 256 threads.
+__global__ void tile_depth_kernel(const __grid_constant__ TileDepthJobs jobs) {
+    const TileDepthJob& J = jobs.v[blockIdx.z];
+    const int ntx = (J.w + WARP_TILE - 1) / WARP_TILE, nty = (J.h + WARP_TILE - 1) / WARP_TILE;
+    if ((int)blockIdx.x >= ntx || (int)blockIdx.y >= nty) return;
+    const int r0 = max(0, (int)blockIdx.y * WARP_TILE - 1), r1 = min(J.h - 1, (int)blockIdx.y * WARP_TILE + WARP_TILE);
+    const int c0 = max(0, (int)blockIdx.x * WARP_TILE - 1), c1 = min(J.w - 1, (int)blockIdx.x * WARP_TILE + WARP_TILE);
+    const int cols = c1 - c0 + 1, n = (r1 - r0 + 1) * cols;
+    float mn = INFINITY, mx = -INFINITY;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int i = r0 + k / cols, j = c0 + k % cols;
+        const float z = __ldg(J.lut + __ldg(J.depth + (size_t)i * J.w + j));
+        mn = fminf(mn, z);
+        mx = fmaxf(mx, z);
+    }
+    __shared__ float s_mn[8], s_mx[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_mn[warp] = mn;
+        s_mx[warp] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+            mn = fminf(mn, s_mn[k]);
+            mx = fmaxf(mx, s_mx[k]);
+        }
+        J.out[blockIdx.y * ntx + blockIdx.x] = make_float2(mn, mx);
+    }
+}
+
 // Decoded depth of every possible 16-bit sample of one view.
 __global__ void depth_lut_kernel(float near_, float far_, float depth_scale, int has_invalid, float* out) {
     const uint32_t raw = blockIdx.x * blockDim.x + threadIdx.x;
@@ -201,6 +288,11 @@ __global__ void depth_lut_kernel(float near_, float far_, float depth_scale, int
 }
 
 }  // namespace
+
+void launch_tile_depth(const TileDepthJobs& jobs, int n, int max_w, int max_h, cudaStream_t s) {
+    tile_depth_kernel<<<dim3((max_w + WARP_TILE - 1) / WARP_TILE, (max_h + WARP_TILE - 1) / WARP_TILE, n), 256, 0, s>>>(
+        jobs);
+}
 
 void launch_depth_lut(float near_, float far_, float depth_scale, int has_invalid, float* out, cudaStream_t s) {
     depth_lut_kernel<<<256, 256, 0, s>>>(near_, far_, depth_scale, has_invalid, out);

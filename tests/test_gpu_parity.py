@@ -96,6 +96,25 @@ def test_depth_formats(ctx, bits, far, invalid):
     assert_parity(yuv, O.synthesize(wl.inputs, wl.planes, target, 5.0))
 
 
+@pytest.mark.parametrize("seed,yaw", [(31, 0.0), (32, 100.0), (33, -150.0)])
+def test_erp_tile_culling(ctx, seed, yaw):
+    """ERP inputs seen by a perspective output: vertex tiles wholly beyond a
+    side of the output are skipped (no triangle from them can cover a
+    pixel).  The output, with culling, against the oracle, which warps every
+    vertex; and against the GPU's own result with culling off (the debug
+    call, which returns the warped vertices, warps every vertex), bit for
+    bit."""
+    import copy
+    wl = scenes.random_pose_small(n_views=2, w=512, h=256, seed=seed, erp_in=True)
+    target = copy.deepcopy(wl.targets[0])
+    target.rotation[0] = yaw
+    yuv, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0)
+    full, _, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, debug=True)
+    for a, b in zip(yuv, full):
+        np.testing.assert_array_equal(a, b)
+    assert_parity(yuv, O.synthesize(wl.inputs, wl.planes, target, 5.0))
+
+
 @pytest.mark.parametrize("seed", [11, 12, 13])
 def test_inpaint_sources_match(ctx, seed):
     """Holes copy exactly the pixel the reference's sweeps choose."""
