@@ -295,3 +295,30 @@ def test_relative_pose_identity_and_translation():
     # seen from a camera yawed by 90 degrees, +x of the world is -y
     assert np.allclose(np.array(R).reshape(3, 3) @ [1, 0, 0], [0, -1, 0], atol=1e-6)
     assert np.allclose(t, [2.0, -1.0, 3.0], atol=1e-6)
+
+
+def test_pipeline_header_compiles(tmp_path):
+    """include/rvsb_pipeline.hpp (the reference's Pipeline hook points over
+    the C ABI) is self-contained: a class deriving from it with the two
+    required hooks compiles."""
+    import shutil
+    import subprocess
+    if not shutil.which("g++"):
+        pytest.skip("no C++ compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "p.cpp"
+    src.write_text("""
+#include "rvsb_pipeline.hpp"
+struct App : rvsb::Pipeline {
+    rvsb_config* cfg = nullptr;
+    const rvsb_config* getConfig() const override { return cfg; }
+    rvsb::InputPlanes loadInputView(int, int, const rvsb_camera&) override { return {}; }
+    bool wantColor() override { return true; }
+    void saveColor(const uint16_t*, int, int, const rvsb_camera&) override {}
+};
+int main() { App a; (void)a; return 0; }
+""")
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Wextra", "-I", os.path.join(root, "include"),
+                        "-I", cuda_inc, str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
