@@ -107,21 +107,17 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
                                              int tx0, int ty0, unsigned long long* zb, int lane, float precision) {
     const int i = by * BLOCK_H + lane / BLOCK_W, j = bx * BLOCK_W + lane % BLOCK_W;
     const bool quad_ok = i < V.h - 1 && j < V.w - 1;
-    float4 v00, v01, v10, v11, w0, w1;
+    float4 v00, v01, v10, v11;
     bool cond0 = false;
+    const size_t r0 = (size_t)i * V.w, r1 = r0 + V.w;
     if (quad_ok) {
         // All four corners at once (one memory round trip), then the
         // emission test of transform.cpp:161.
-        const size_t r0 = (size_t)i * V.w, r1 = r0 + V.w;
         v00 = __ldg(V.vert + r0 + j);
         v01 = __ldg(V.vert + r0 + j + 1);
         v10 = __ldg(V.vert + r1 + j);
         v11 = __ldg(V.vert + r1 + j + 1);
         cond0 = v01.z > 0.f && v10.z > 0.f && v01.x > 0.f && v10.x > 0.f;
-        if (cond0 && wrap && j == 0) {
-            w0 = __ldg(V.vert + r0 + V.w - 1);
-            w1 = __ldg(V.vert + r1 + V.w - 1);
-        }
     }
     // Scan order of transform.cpp:159-176: row i, column j, then triangle
     // 1, triangle 2, and the two seam triangles at j = 0.
@@ -133,8 +129,22 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
         switch (slot) {
             case 0: A = v00; B = v01; C = v10; active = active && v00.z > 0.f && v00.x > 0.f; break;
             case 1: A = v11; B = v10; C = v01; active = active && v11.z > 0.f && v11.x > 0.f; break;
-            case 2: A = w0; B = v00; C = w1; active = active && j == 0; break;
-            default: A = v10; B = w1; C = v00; active = active && j == 0; break;
+            // Seam triangles (wrapping outputs only): their column W-1
+            // vertices are loaded here, so that they hold no registers
+            // across the common case.
+            case 2:
+                active = active && j == 0;
+                A = B = C = v00;
+                if (active) {
+                    A = __ldg(V.vert + r0 + V.w - 1);
+                    C = __ldg(V.vert + r1 + V.w - 1);
+                }
+                break;
+            default:
+                active = active && j == 0;
+                A = v10; B = v10; C = v00;
+                if (active) B = __ldg(V.vert + r1 + V.w - 1);
+                break;
         }
         TriSetup s;
         int count = 0;
