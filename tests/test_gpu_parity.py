@@ -23,6 +23,7 @@ SMALL_CASES = [
     dict(n_views=2, w=128, h=64, seed=4, erp_in=True),
     dict(n_views=3, w=128, h=64, seed=5, erp_in=True, erp_out=True),
     dict(n_views=1, w=64, h=36, seed=6),
+    dict(n_views=2, w=100, h=50, seed=7),  # width not a multiple of 8: the 2x2 colour decode
 ]
 
 
