@@ -371,6 +371,9 @@ int rvsb_scene_last_launch_count(const rvsb_scene* scene);
 /* The raster autotuner (see rvsb_batch_set_autotune) for the per-view calls
  * of this scene (default off). */
 rvsb_status rvsb_scene_set_autotune(rvsb_scene* scene, int enable);
+/* Pins the raster variant of the scene's per-view calls (0 .. 7), or -1 for
+ * the default or the tuner's choice; as rvsb_batch_set_raster_variant. */
+rvsb_status rvsb_scene_set_raster_variant(rvsb_scene* scene, int variant);
 
 /* ----------------------------------------------------------------------- */
 /* Batches: many virtual views of one resident scene                       */
@@ -397,11 +400,12 @@ rvsb_status rvsb_batch_set_graphs(rvsb_batch* batch, int enable);
 /* Raster autotuner (default off): the first batch of each new shape (batch
  * size bucket, largest input set and output, projections) is run once with
  * every raster variant -- tile size 32x32, 64x32 or 32x16, views per shared
- * z-buffer group, the stretched-triangle threshold and the bin entries
- * staged per round -- and the fastest is kept for that shape.  All variants
- * give identical outputs. */
+ * z-buffer group, the stretched-triangle threshold, the bin entries staged
+ * per round and whether triangles whose candidate box holds 5 to 32 pixels
+ * take the one-lane-per-pixel medium path -- and the fastest is kept for that shape.
+ * All variants give identical outputs. */
 rvsb_status rvsb_batch_set_autotune(rvsb_batch* batch, int enable);
-/* Use one raster variant (0 .. 5) for every call, or -1 for the default or
+/* Use one raster variant (0 .. 7) for every call, or -1 for the default or
  * tuned one; the variant used by the last call. */
 rvsb_status rvsb_batch_set_raster_variant(rvsb_batch* batch, int variant);
 int rvsb_batch_last_raster_variant(const rvsb_batch* batch);

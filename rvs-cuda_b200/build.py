@@ -20,7 +20,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["launch.cu", "decode.cu", "warp.cu", "bin.cu", "tile.cu", "inpaint.cu", "noalloc.cu", "aux.cu", "ms.cu",
               "resize.cu",
-              "raster_v0.cu", "raster_v1.cu", "raster_v2.cu", "raster_v3.cu", "raster_v4.cu", "raster_v5.cu"]
+              "raster_v0.cu", "raster_v1.cu", "raster_v2.cu", "raster_v3.cu", "raster_v4.cu", "raster_v5.cu",
+              "raster_v6.cu", "raster_v7.cu"]
 CPP_SOURCES = ["api.cpp", "engine.cpp", "server.cpp", "frontend.cpp", "camera.cpp"]
 CLI_SOURCES = ["rvsb_cli.cpp"]
 SCENEGEN_SOURCES = ["scenegen.cpp"]

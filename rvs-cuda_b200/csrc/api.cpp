@@ -455,6 +455,15 @@ rvsb_status rvsb_scene_set_autotune(rvsb_scene* sc, int enable) {
     });
 }
 
+rvsb_status rvsb_scene_set_raster_variant(rvsb_scene* sc, int variant) {
+    if (!sc || variant < -1 || variant >= NUM_RASTER_VARIANTS) return RVSB_E_ARG;
+    return guarded(sc->ctx, [&]() -> rvsb_status {
+        check(cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+        single_core(sc).force_variant(variant);
+        return RVSB_OK;
+    });
+}
+
 rvsb_status rvsb_batch_set_profiling(rvsb_batch* batch, int enable) {
     if (!batch) return RVSB_E_ARG;
     return guarded(batch->scene->ctx, [&]() -> rvsb_status {

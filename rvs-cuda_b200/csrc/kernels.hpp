@@ -71,15 +71,17 @@ int launch_batch(const Tabs& tabs, const BatchShape& shape, cudaStream_t stream,
 
 // Raster variants the autotuner chooses from: tile width and height, views
 // per shared z-buffer group, the candidate count above which a triangle is
-// rasterised warp-cooperatively, and the bin entries staged per round.
-// Every variant gives identical results.
+// rasterised warp-cooperatively, the bin entries staged per round, and the
+// candidate count up to which those triangles are flattened across the warp
+// together (med <= small: each one alone, row span by row span).  Every
+// variant gives identical results.
 struct RasterVariant {
-    int tw, th, vg, small, ent;
+    int tw, th, vg, small, ent, med;
 };
-constexpr int NUM_RASTER_VARIANTS = 6;
+constexpr int NUM_RASTER_VARIANTS = 8;
 constexpr RasterVariant kRasterVariants[NUM_RASTER_VARIANTS] = {
-    {32, 32, 4, 4, 1024}, {64, 32, 2, 4, 1024}, {32, 32, 4, 2, 1024},
-    {32, 32, 4, 8, 1024}, {32, 32, 2, 4, 512},  {32, 16, 4, 4, 512},
+    {32, 32, 4, 4, 1024, 0}, {64, 32, 2, 4, 1024, 0}, {32, 32, 4, 2, 1024, 0},  {32, 32, 4, 8, 1024, 0},
+    {32, 32, 2, 4, 512, 0},  {32, 16, 4, 4, 512, 0},  {32, 32, 4, 2, 1024, 32}, {64, 32, 2, 4, 1024, 32},
 };
 
 // One-time kernel attributes of the current device (the raster kernel's

@@ -24,15 +24,21 @@ static_assert(QUADS == 32, "one warp per binning block");
 // gives one lane per row), VG views per shared z-buffer group, triangles
 // with more than SMALL candidate pixels go warp-cooperative, ENT bin
 // entries staged per round.
-template <int TW_, int TH_, int VG_, int SMALL_, int ENT_>
+template <int TW_, int TH_, int VG_, int SMALL_, int ENT_, int MED_>
 struct Cfg {
     static constexpr int TW = TW_, TH = TH_, VG = VG_, SMALL = SMALL_, ENT = ENT_;
+    // Triangles with more than SMALL and at most MED candidate pixels are
+    // rasterised with their candidates flattened across the warp (MED <=
+    // SMALL: none); larger ones one at a time, row span by row span.
+    static constexpr int MED = MED_;
+    static constexpr int BIG = MED_ > SMALL_ ? MED_ : SMALL_;
     static constexpr int NPIX = TW * TH;
     static constexpr size_t kZbBytes = sizeof(unsigned long long) * VG * NPIX;
     static constexpr size_t kEntBytes = sizeof(int) * ENT;
     static constexpr size_t kAccBytes = sizeof(float) * 4 * NPIX;
     static constexpr size_t kSmemBytes = kZbBytes + kEntBytes + kAccBytes;
     static_assert(TH <= 32 && TW % 2 == 0 && TH % 2 == 0, "tile shape");
+    static_assert(MED <= 32, "a medium triangle's candidate index stays below 32");
     static_assert(kZbBytes % 16 == 0 && kEntBytes % 16 == 0, "shared-memory carve alignment");
 };
 
@@ -154,8 +160,9 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
             s.rinv = rcp_approx(s.den);
         }
         const uint32_t tri = quad * 4u + (uint32_t)slot;
-        const bool big = count > C::SMALL;
-        if (count > 0 && !big) {
+        const bool medium = count > C::SMALL && count <= C::MED;
+        const bool big = count > C::BIG;
+        if (count > 0 && count <= C::SMALL) {
             // One flat loop over the candidate box (at most SMALL pixels),
             // with the quality key computed once up front.
             const float invq = key_invq(A, B, C, precision);
@@ -167,6 +174,58 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
                 if (++x > s.x1) {
                     x = s.x0;
                     ++y;
+                }
+            }
+        }
+        // Medium triangles (at most MED candidates in their box): the
+        // candidates of all of the warp's medium triangles flattened into
+        // one sequence, 32 per round; each lane fetches its candidate's
+        // triangle from the lane that set it up.
+        if constexpr (C::MED > C::SMALL) {
+            if (__ballot_sync(0xffffffffu, medium)) {
+                const int mc = medium ? count : 0;
+                int incl = mc;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int excl = incl - mc;
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                const float invq_m = medium ? key_invq(A, B, C, precision) : 0.f;
+                const int bw = s.x1 - s.x0 + 1;
+                for (int base = 0; base < total; base += 32) {
+                    const int c = base + lane;
+                    int own = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const int probe = __shfl_sync(0xffffffffu, incl, own + step - 1);
+                        if (probe <= c) own += step;
+                    }
+                    TriSetup t;
+                    t.b1c1 = __shfl_sync(0xffffffffu, s.b1c1, own);
+                    t.c0b0 = __shfl_sync(0xffffffffu, s.c0b0, own);
+                    t.c1a1 = __shfl_sync(0xffffffffu, s.c1a1, own);
+                    t.a0c0 = __shfl_sync(0xffffffffu, s.a0c0, own);
+                    t.den = __shfl_sync(0xffffffffu, s.den, own);
+                    t.rinv = __shfl_sync(0xffffffffu, s.rinv, own);
+                    const float cx = __shfl_sync(0xffffffffu, C.x, own), cy = __shfl_sync(0xffffffffu, C.y, own);
+                    const float za = __shfl_sync(0xffffffffu, A.z, own), zb_ = __shfl_sync(0xffffffffu, B.z, own);
+                    const float zc = __shfl_sync(0xffffffffu, C.z, own);
+                    const float invq = __shfl_sync(0xffffffffu, invq_m, own);
+                    const uint32_t ttri = __shfl_sync(0xffffffffu, tri, own);
+                    const int ox0 = __shfl_sync(0xffffffffu, s.x0, own), oy0 = __shfl_sync(0xffffffffu, s.y0, own);
+                    const int obw = __shfl_sync(0xffffffffu, bw, own), oex = __shfl_sync(0xffffffffu, excl, own);
+                    if (c >= total) continue;
+                    // k < MED <= 32 and the box width <= 32: (k + 0.5) / width is
+                    // at least 1/64 from an integer, so the fast quotient
+                    // truncates to the exact row.
+                    const int k = c - oex;
+                    const int dy = (int)__fdividef((float)k + 0.5f, (float)obw);
+                    const int x = ox0 + (k - dy * obw), y = oy0 + dy;
+                    float d;
+                    if (test_pixel(t, cx, cy, za, zb_, zc, x, y, d))
+                        atomicMin(&zb[(y - ty0) * C::TW + (x - tx0)], frag_key(d, invq, ttri));
                 }
             }
         }
@@ -488,12 +547,12 @@ void prepare() {
 
 // Defines the host entry points of raster variant N (one per .cu file, so
 // the variants compile in parallel).
-#define RVSB_RASTER_VARIANT(N, TW, TH, VG, SMALL, ENT)                                                    \
+#define RVSB_RASTER_VARIANT(N, TW, TH, VG, SMALL, ENT, MED)                                                    \
     namespace rvsb {                                                                                     \
-    using RasterCfg##N = raster::Cfg<TW, TH, VG, SMALL, ENT>;                                             \
+    using RasterCfg##N = raster::Cfg<TW, TH, VG, SMALL, ENT, MED>;                                             \
     static_assert(kRasterVariants[N].tw == TW && kRasterVariants[N].th == TH &&                          \
                       kRasterVariants[N].vg == VG && kRasterVariants[N].small == SMALL &&                \
-                      kRasterVariants[N].ent == ENT,                                                     \
+                      kRasterVariants[N].ent == ENT && kRasterVariants[N].med == MED,                                                     \
                   "variant table");                                                                      \
     void launch_raster_v##N(const TableParam& t, const BatchShape& sh, cudaStream_t s) {                 \
         raster::launch<RasterCfg##N>(t, sh, s);                                                          \

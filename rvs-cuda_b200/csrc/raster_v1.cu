@@ -2,4 +2,4 @@
 // warp-cooperative above 4 candidate pixels, 1024 bin entries per round.
 #include "raster.cuh"
 
-RVSB_RASTER_VARIANT(1, 64, 32, 2, 4, 1024)
+RVSB_RASTER_VARIANT(1, 64, 32, 2, 4, 1024, 0)

@@ -2,4 +2,4 @@
 // warp-cooperative above 2 candidate pixels, 1024 bin entries per round.
 #include "raster.cuh"
 
-RVSB_RASTER_VARIANT(2, 32, 32, 4, 2, 1024)
+RVSB_RASTER_VARIANT(2, 32, 32, 4, 2, 1024, 0)

@@ -2,4 +2,4 @@
 // warp-cooperative above 8 candidate pixels, 1024 bin entries per round.
 #include "raster.cuh"
 
-RVSB_RASTER_VARIANT(3, 32, 32, 4, 8, 1024)
+RVSB_RASTER_VARIANT(3, 32, 32, 4, 8, 1024, 0)

@@ -2,4 +2,4 @@
 // warp-cooperative above 4 candidate pixels, 512 bin entries per round.
 #include "raster.cuh"
 
-RVSB_RASTER_VARIANT(5, 32, 16, 4, 4, 512)
+RVSB_RASTER_VARIANT(5, 32, 16, 4, 4, 512, 0)

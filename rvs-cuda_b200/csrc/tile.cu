@@ -14,8 +14,10 @@ RVSB_DECLARE_RASTER(2)
 RVSB_DECLARE_RASTER(3)
 RVSB_DECLARE_RASTER(4)
 RVSB_DECLARE_RASTER(5)
+RVSB_DECLARE_RASTER(6)
+RVSB_DECLARE_RASTER(7)
 #undef RVSB_DECLARE_RASTER
-static_assert(NUM_RASTER_VARIANTS == 6, "one declaration per variant");
+static_assert(NUM_RASTER_VARIANTS == 8, "one declaration per variant");
 
 void prepare_kernels() {
     prepare_raster_v0();
@@ -24,6 +26,8 @@ void prepare_kernels() {
     prepare_raster_v3();
     prepare_raster_v4();
     prepare_raster_v5();
+    prepare_raster_v6();
+    prepare_raster_v7();
 }
 
 template <class Tabs>
@@ -34,6 +38,8 @@ void launch_raster(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
         case 3: launch_raster_v3(tabs, sh, s); break;
         case 4: launch_raster_v4(tabs, sh, s); break;
         case 5: launch_raster_v5(tabs, sh, s); break;
+        case 6: launch_raster_v6(tabs, sh, s); break;
+        case 7: launch_raster_v7(tabs, sh, s); break;
         default: launch_raster_v0(tabs, sh, s); break;
     }
 }

@@ -32,14 +32,14 @@ EXPORTED = [
     "rvsb_server_create", "rvsb_server_add_scene", "rvsb_server_reserve", "rvsb_server_submit", "rvsb_server_poll",
     "rvsb_server_drain", "rvsb_server_clock", "rvsb_server_destroy",
     "rvsb_batch_set_autotune", "rvsb_batch_set_raster_variant", "rvsb_batch_last_raster_variant",
-    "rvsb_scene_set_autotune", "rvsb_synthesize_aux", "rvsb_config_output_file", "rvsb_config_validity_threshold",
+    "rvsb_scene_set_autotune", "rvsb_scene_set_raster_variant", "rvsb_synthesize_aux", "rvsb_config_output_file", "rvsb_config_validity_threshold",
     "rvsb_config_virtual_crop", "rvsb_host_stream_create", "rvsb_host_stream_destroy", "rvsb_host_stream_submit",
     "rvsb_host_stream_wait", "rvsb_host_stream_join",
 ]
 
 OUT_COLOR, OUT_MASKED_COLOR, OUT_MASK, OUT_DEPTH, OUT_MASKED_DEPTH = range(5)
 
-RASTER_VARIANTS = 6
+RASTER_VARIANTS = 8
 
 STAGES = ["warp", "bin", "raster", "inpaint", "total"]
 
@@ -128,6 +128,7 @@ def load():
     L.rvsb_batch_set_raster_variant.argtypes = [c_p, ctypes.c_int]
     L.rvsb_batch_last_raster_variant.argtypes = [c_p]
     L.rvsb_scene_set_autotune.argtypes = [c_p, ctypes.c_int]
+    L.rvsb_scene_set_raster_variant.argtypes = [c_p, ctypes.c_int]
     L.rvsb_server_create.argtypes = [c_p, ctypes.c_int, ctypes.c_int, ctypes.c_size_t, P(c_p)]
     L.rvsb_server_add_scene.argtypes = [c_p, c_p, P(ctypes.c_int)]
     L.rvsb_server_reserve.argtypes = [c_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -320,6 +321,10 @@ class Scene:
 
     def set_autotune(self, on=True):
         return self.ctx.check(self.ctx.lib.rvsb_scene_set_autotune(self.h, 1 if on else 0))
+
+    def set_raster_variant(self, v):
+        """Pins the raster variant of this scene's calls (-1: default or tuned)."""
+        return self.ctx.check(self.ctx.lib.rvsb_scene_set_raster_variant(self.h, int(v)))
 
     def stage_times(self):
         """{stage: ms} of the last profiled synthesis (stream must be complete)."""

@@ -135,3 +135,34 @@ def test_every_raster_variant_identical(ctx, erp):
         for x, y in zip(_yuv(o, c), e):
             np.testing.assert_array_equal(x, y)
     b.close()
+
+
+def test_default_raster_variant_follows_magnification(ctx):
+    """With no variant pinned and the tuner off, an output at the inputs'
+    pixels per radian runs variant 0 and a 3x magnified one variant 7 (the
+    medium-triangle path); both give the bytes of every other variant."""
+    import torch
+    wl = scenes.random_pose_small(n_views=2, w=64, h=36, seed=5)
+    sc = _upload(ctx, wl)
+    p = rvsb.params(5.0)
+    same = wl.targets[0]
+    big = copy.deepcopy(same)
+    big.width, big.height = 192, 108
+    for i in range(2):
+        big.focal[i] *= 3.0
+        big.principle_point[i] *= 3.0
+    b = rvsb.Batch(sc, 1)
+    for cam, expected_variant in ((same, 0), (big, 7)):
+        out = yuv_planes_torch(cam.width, cam.height)
+        b.synthesize([cam], p, [out])
+        torch.cuda.synchronize()
+        assert b.last_raster_variant() == expected_variant
+        got = _yuv(out, cam)
+        b.set_raster_variant(3 if expected_variant == 7 else 6)
+        out2 = yuv_planes_torch(cam.width, cam.height)
+        b.synthesize([cam], p, [out2])
+        torch.cuda.synchronize()
+        b.set_raster_variant(-1)
+        for x, y in zip(got, _yuv(out2, cam)):
+            np.testing.assert_array_equal(x, y)
+    b.close()
