@@ -464,6 +464,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_co
     auto acc = reinterpret_cast<float(*)[C::NPIX]>(s_raw + C::kZbBytes + C::kEntBytes);
     __shared__ int s_pref[C::VG + 1];
     __shared__ int s_off[C::VG];
+    __shared__ int s_next;
     const SlotTable& tab = tabs.at(blockIdx.y);
     const DevTarget& T = tab.t;
     if ((int)blockIdx.x >= T.ntx * T.nty) return;
@@ -494,6 +495,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_co
         const int E = s_pref[gn];
         for (int base = 0; base < E; base += C::ENT) {
             const int n = min(C::ENT, E - base);
+            if (tid == 0) s_next = NWARPS;
             for (int q = tid; q < n; q += TILE_THREADS) {
                 const int e = base + q;
                 int k = 0;
@@ -514,11 +516,18 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_co
                 s_ent[q] = b < 0 ? -1 : (k << 26) | b;
             }
             __syncthreads();
-            for (int q = warp; q < n; q += NWARPS) {
+            // Entries are taken dynamically: a warp claims its next entry
+            // before rasterising the current one, so that warps which meet
+            // stretched triangles do not hold the others at the barrier.
+            for (int q = warp; q < n;) {
                 const int ent = s_ent[q];
-                if (ent < 0) continue;
-                const int k = ent >> 26, bx = ent & 2047, by = (ent >> 11) & 32767;
-                raster_block<C>(tab.v[g0 + k], T.wo, T.ho, wrap, bx, by, tx0, ty0, zb[k], lane, T.precision);
+                int next = 0;
+                if (lane == 0) next = atomicAdd(&s_next, 1);
+                if (ent >= 0) {
+                    const int k = ent >> 26, bx = ent & 2047, by = (ent >> 11) & 32767;
+                    raster_block<C>(tab.v[g0 + k], T.wo, T.ho, wrap, bx, by, tx0, ty0, zb[k], lane, T.precision);
+                }
+                q = __shfl_sync(0xffffffffu, next, 0);
             }
             __syncthreads();
         }
