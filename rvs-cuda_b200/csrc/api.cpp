@@ -149,7 +149,7 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
             for (size_t v = 0; v < sc->cams.size(); ++v) {
                 const rvsb_camera& c = sc->cams[v];
                 if (c.projection != RVSB_PROJ_EQUIRECTANGULAR) continue;
-                tj.v[n_erp++] = TileDepthJob{frame[v].depth, sc->depth_lut[v]->as<float>(),
+                tj.v[n_erp++] = TileDepthJob{frame[v].depth, sc->depth_lut[v]->as<float4>(),
                                              sc->tile_depth[v]->as<float2>(), c.width, c.height};
                 ew = std::max(ew, c.width);
                 eh = std::max(eh, c.height);
@@ -300,11 +300,11 @@ rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int 
             col->alloc(ctx, (size_t)inputs[v].width * inputs[v].height * sizeof(uint64_t));
             sc->color.push_back(std::move(col));
             auto lut = std::make_unique<DevMem>();
-            lut->alloc(ctx, 65536 * sizeof(float));
+            lut->alloc(ctx, 65536 * sizeof(float4));
             const rvsb_camera& cam = inputs[v];
             launch_depth_lut(cam.depth_range[0], cam.depth_range[1],
                              1.0f / (float)((1u << cam.bit_depth_depth) - 1u), cam.has_invalid_depth,
-                             lut->as<float>(), nullptr);
+                             cam.focal[0], cam.focal[1], lut->as<float4>(), nullptr);
             check(cudaPeekAtLastError(), "depth table");
             sc->depth_lut.push_back(std::move(lut));
         }
@@ -344,7 +344,7 @@ rvsb_status rvsb_scene_upload(rvsb_scene* sc, int view, const rvsb_view_planes* 
         check(cudaPeekAtLastError(), "decode colour");
         if (c.projection == RVSB_PROJ_EQUIRECTANGULAR) {
             TileDepthJobs jobs{};
-            jobs.v[0] = TileDepthJob{sc->planes[view * 4 + 3]->as<uint16_t>(), sc->depth_lut[view]->as<float>(),
+            jobs.v[0] = TileDepthJob{sc->planes[view * 4 + 3]->as<uint16_t>(), sc->depth_lut[view]->as<float4>(),
                                      sc->tile_depth[view]->as<float2>(), c.width, c.height};
             launch_tile_depth(jobs, 1, c.width, c.height, s);
             check(cudaPeekAtLastError(), "tile depth ranges");

@@ -64,7 +64,8 @@ __device__ __forceinline__ float decode_depth_raw(float near_, float far_, float
 template <class View>
 __device__ __forceinline__ float4 warp_vertex(const View& V, const DevTarget& T, int i, int j) {
     const size_t idx = (size_t)i * V.w + j;
-    const float d = __ldg(V.depth_lut + __ldg(V.pd + idx));
+    const float4 L = __ldg(V.depth_lut + __ldg(V.pd + idx));
+    const float d = L.x;
     float x0, x1, x2;
     if (V.proj == 1) {
         const float ct = V.erp_row[2 * i], st = V.erp_row[2 * i + 1];
@@ -76,8 +77,10 @@ __device__ __forceinline__ float4 warp_vertex(const View& V, const DevTarget& T,
         const float pu = __fadd_rn((float)j, 0.5f), pv = __fadd_rn((float)i, 0.5f);
         if (d > 0.f) {
             x0 = d;
-            x1 = __fmul_rn(-__fdiv_rn(d, V.f0), __fsub_rn(pu, V.p0));
-            x2 = __fmul_rn(-__fdiv_rn(d, V.f1), __fsub_rn(pv, V.p1));
+            // L.y = -(d / f0), L.z = -(d / f1), divided once per sample
+            // value when the table was built.
+            x1 = __fmul_rn(L.y, __fsub_rn(pu, V.p0));
+            x2 = __fmul_rn(L.z, __fsub_rn(pv, V.p1));
         } else {
             x0 = x1 = x2 = qnan();
         }

@@ -35,7 +35,7 @@ struct DevView {
     const uint16_t* pu;
     const uint16_t* pv;
     const uint16_t* pd;
-    const float* depth_lut;               // 65536 decoded depths, indexed by the raw sample
+    const float4* depth_lut;              // 65536 (d, -d/f0, -d/f1, 0), indexed by the raw sample
     const float* erp_row;                 // ERP: per row (cos theta, sin theta), 2*h floats
     const float* erp_col;                 // ERP: per column (cos phi, sin phi), 2*w floats
     // ERP inputs, per WARP_TILE x WARP_TILE vertex tile grown by one pixel:

@@ -254,7 +254,7 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
             V.tile_depth = sc->tile_depth[v]->as<float2>();
         }
         V.color = sc->color[v]->as<uint64_t>();
-        V.depth_lut = sc->depth_lut[v]->as<float>();
+        V.depth_lut = sc->depth_lut[v]->as<float4>();
         V.vert = ws.vert.as<float4>() + voff;
         V.bbox = ws.bbox.as<int4>() + boff;
         V.tri_shift = 2;

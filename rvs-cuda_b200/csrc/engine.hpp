@@ -183,7 +183,7 @@ struct rvsb_scene {
     std::vector<std::unique_ptr<rvsb::DevMem>> planes;  // 4 per view: y, u, v, depth
     std::vector<std::unique_ptr<rvsb::DevMem>> erp;     // 2 per view: rows, cols (ERP inputs)
     std::vector<std::unique_ptr<rvsb::DevMem>> color;   // 1 per view: decoded colour words
-    std::vector<std::unique_ptr<rvsb::DevMem>> depth_lut;  // 1 per view: 65536 decoded depths
+    std::vector<std::unique_ptr<rvsb::DevMem>> depth_lut;  // 1 per view: 65536 x (d, -d/f0, -d/f1, 0)
     // ERP views: per vertex tile, direction cone and depth range (culling)
     std::vector<std::unique_ptr<rvsb::DevMem>> erp_cone, tile_depth;
     std::vector<bool> uploaded;

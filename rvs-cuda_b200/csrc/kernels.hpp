@@ -108,16 +108,18 @@ void launch_resize(const Tabs& tabs, const BatchShape& shape, cudaStream_t strea
 
 void launch_decode_views(const DecodeJobs& jobs, int n, int max_w, int max_h, cudaStream_t s);
 
-// The depth table of one input view: the decoded depth (normalised
-// disparity with near / far, rvs_cuda_lib/src/process_input_frame.cu:346-385)
-// of every 16-bit sample, 65536 floats.
-void launch_depth_lut(float near_, float far_, float depth_scale, int has_invalid, float* out, cudaStream_t s);
+// The depth table of one input view: for every 16-bit sample the decoded
+// depth d (normalised disparity with near / far,
+// rvs_cuda_lib/src/process_input_frame.cu:346-385) and the perspective
+// unprojection factors -(d / f0), -(d / f1); 65536 float4.
+void launch_depth_lut(float near_, float far_, float depth_scale, int has_invalid, float f0, float f1, float4* out,
+                      cudaStream_t s);
 
 // Depth range (min, max) of every WARP_TILE x WARP_TILE vertex tile grown by
 // one pixel, for the ERP input culling; up to MAX_VIEWS views in one launch.
 struct TileDepthJob {
     const uint16_t* depth;   // raw depth plane
-    const float* lut;        // the view's decoded-depth table
+    const float4* lut;       // the view's depth table (decoded depth in .x)
     float2* out;             // one (min, max) per tile, row-major
     int w, h;
 };

@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
         float f0, f1, p0, p1;
         float R[9], t[3];
         const uint16_t* pd;
-        const float* depth_lut;
+        const float4* depth_lut;
         const float* erp_row;
         const float* erp_col;
         float4* vert;
@@ -256,7 +256,7 @@ __global__ void tile_depth_kernel(const __grid_constant__ TileDepthJobs jobs) {
     float mn = INFINITY, mx = -INFINITY;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int i = r0 + k / cols, j = c0 + k % cols;
-        const float z = __ldg(J.lut + __ldg(J.depth + (size_t)i * J.w + j));
+        const float z = __ldg(&J.lut[__ldg(J.depth + (size_t)i * J.w + j)].x);
         mn = fminf(mn, z);
         mx = fmaxf(mx, z);
     }
@@ -281,10 +281,16 @@ __global__ void tile_depth_kernel(const __grid_constant__ TileDepthJobs jobs) {
     }
 }
 
-// Decoded depth of every possible 16-bit sample of one view.
-__global__ void depth_lut_kernel(float near_, float far_, float depth_scale, int has_invalid, float* out) {
+// Decoded depth d of every possible 16-bit sample of one view, with the
+// two per-sample factors of the perspective unprojection, -(d / f0) and
+// -(d / f1) (PerspectiveUnprojector.cpp:75-77), so that the warp reads them
+// instead of dividing per pixel.
+__global__ void depth_lut_kernel(float near_, float far_, float depth_scale, int has_invalid, float f0, float f1,
+                                 float4* out) {
     const uint32_t raw = blockIdx.x * blockDim.x + threadIdx.x;
-    if (raw < 65536u) out[raw] = decode_depth_raw(near_, far_, depth_scale, has_invalid, raw);
+    if (raw >= 65536u) return;
+    const float d = decode_depth_raw(near_, far_, depth_scale, has_invalid, raw);
+    out[raw] = make_float4(d, -__fdiv_rn(d, f0), -__fdiv_rn(d, f1), 0.f);
 }
 
 }  // namespace
@@ -294,8 +300,9 @@ void launch_tile_depth(const TileDepthJobs& jobs, int n, int max_w, int max_h, c
         jobs);
 }
 
-void launch_depth_lut(float near_, float far_, float depth_scale, int has_invalid, float* out, cudaStream_t s) {
-    depth_lut_kernel<<<256, 256, 0, s>>>(near_, far_, depth_scale, has_invalid, out);
+void launch_depth_lut(float near_, float far_, float depth_scale, int has_invalid, float f0, float f1, float4* out,
+                      cudaStream_t s) {
+    depth_lut_kernel<<<256, 256, 0, s>>>(near_, far_, depth_scale, has_invalid, f0, f1, out);
 }
 
 template <class Tabs>
