@@ -437,10 +437,31 @@ def main():
     max_total = allreduce_max(total_s, world)
     value = world * args.steps / max_total
 
-    # e2e: reference-facing call with pinned host buffers.
-    host_planes = [[torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).reshape(-1).pin_memory()
-                    for a in planes] for planes in wl.planes]
-    host_out = [torch.empty(t.numel(), dtype=torch.int16).pin_memory() for t in out]
+    # e2e: reference-facing call with pinned host buffers.  A frame's input
+    # planes lie in one pinned buffer in file order (per view: colour Y, U,
+    # V, then depth), as a loader that reads a frame's files into one buffer
+    # holds them; each output frame is one YUV420 buffer (Y, U, V).
+    frame_in = torch.empty(sum(np.asarray(a).size for planes in wl.planes for a in planes),
+                           dtype=torch.int16).pin_memory()
+    host_planes, off = [], 0
+    for planes in wl.planes:
+        views = []
+        for a in planes:
+            t = frame_in[off:off + np.asarray(a).size]
+            t.copy_(torch.from_numpy(np.ascontiguousarray(a).view(np.int16).reshape(-1)))
+            views.append(t)
+            off += t.numel()
+        host_planes.append(views)
+
+    def frame_out():
+        buf = torch.empty(sum(t.numel() for t in out), dtype=torch.int16).pin_memory()
+        parts, o = [], 0
+        for t in out:
+            parts.append(buf[o:o + t.numel()])
+            o += t.numel()
+        return parts
+
+    host_out = frame_out()
     h2d = sum(t.numel() * 2 for planes in host_planes for t in planes)
     d2h = sum(t.numel() * 2 for t in host_out)
     for _ in range(3):
@@ -464,8 +485,7 @@ def main():
     # events on the caller's stream around all steps (join = every download
     # finished).
     hs = rvsb.HostStream(ctx, wl.inputs)
-    host_outs = [host_out] + [[torch.empty(t.numel(), dtype=torch.int16).pin_memory() for t in out]
-                              for _ in range(2)]
+    host_outs = [host_out] + [frame_out() for _ in range(2)]
     for k in range(3):
         hs.submit(host_planes, target, p, host_outs[k % 3], stream=stream)
     hs.join(stream)

@@ -27,9 +27,13 @@ struct rvsb_batch {
 // `down` (a second upload stream gains nothing: the uploads are bound by
 // the host link).  With three sets the upload of frame k waits only for frame k-3,
 // long finished, so the copy engine and the synthesis both stay busy.
+// A set's planes lie back to back in one device block (per view y, u, v,
+// depth), so planes that are also adjacent in host memory (a frame read
+// into one buffer) go up in one copy: one large copy runs at the link's
+// full rate, many small ones about 12% below it.
 struct rvsb_host_stream {
     struct Set {
-        std::vector<std::unique_ptr<DevMem>> planes;  // 4 per view: y, u, v, depth
+        DevMem frame;                 // every view's y, u, v, depth planes, back to back
         DevMem out;
         cudaEvent_t uploaded = nullptr, computed = nullptr, downloaded = nullptr;
         uint64_t ticket = 0;
@@ -39,6 +43,8 @@ struct rvsb_host_stream {
     rvsb_scene* scene = nullptr;  // cameras, decoded colour, slot workspace
     static constexpr int kDepth = 3;
     Set sets[kDepth];
+    std::vector<size_t> plane_off;  // byte offset of plane 4 * view + k in a set's block
+    std::vector<size_t> plane_len;
     cudaStream_t copy = nullptr, compute = nullptr, down = nullptr;
     cudaEvent_t ordered = nullptr;  // the caller's stream at submit time
     uint64_t next = 0;
@@ -78,6 +84,54 @@ rvsb_status guarded(rvsb_context* ctx, F&& f) {
 size_t plane_bytes(const rvsb_camera& c, int k) {
     const size_t n = (size_t)c.width * c.height;
     return (k == 1 || k == 2) ? (size_t)(c.width / 2) * (c.height / 2) * 2 : n * 2;
+}
+
+// Copies planes that are back to back on both sides: parts[i] = (dst, src,
+// bytes), each part starting where the previous one ends.  One copy moves
+// them all at the link's full rate; but planes adjacent in host memory can
+// belong to different pinned allocations, and the runtime refuses a copy
+// across them (invalid value, reported at the call), so then each part is
+// copied on its own.
+struct CopyPart {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+void copy_run(const CopyPart* parts, int n, cudaMemcpyKind kind, cudaStream_t s, const char* what) {
+    if (n > 1) {
+        size_t total = 0;
+        for (int i = 0; i < n; ++i) total += parts[i].bytes;
+        const cudaError_t e = cudaMemcpyAsync(parts[0].dst, parts[0].src, total, kind, s);
+        if (e == cudaSuccess) return;
+        if (e != cudaErrorInvalidValue) check(e, what);
+        (void)cudaGetLastError();  // the refused copy: clear it and copy per part
+    }
+    for (int i = 0; i < n; ++i) check(cudaMemcpyAsync(parts[i].dst, parts[i].src, parts[i].bytes, kind, s), what);
+}
+
+// Copies planes parts[0..n) in runs of parts that are adjacent on both
+// sides (the library's side is adjacent by construction; the caller's when
+// its planes are one buffer).
+void copy_planes(const CopyPart* parts, int n, cudaMemcpyKind kind, cudaStream_t s, const char* what) {
+    auto follows = [](const void* next, const void* prev, size_t bytes) {
+        return static_cast<const char*>(next) == static_cast<const char*>(prev) + bytes;
+    };
+    for (int k = 0; k < n;) {
+        int e = k + 1;
+        while (e < n && follows(parts[e].src, parts[e - 1].src, parts[e - 1].bytes) &&
+               follows(parts[e].dst, parts[e - 1].dst, parts[e - 1].bytes))
+            ++e;
+        copy_run(parts + k, e - k, kind, s, what);
+        k = e;
+    }
+}
+
+// Copies a YUV420 result from device staging (Y, U, V back to back, ny and
+// nc bytes) to the caller's host planes: one copy when those are one frame
+// buffer as well, else one per plane.
+void download_yuv(const rvsb_yuv420* host, const rvsb_yuv420& dev, size_t ny, size_t nc, cudaStream_t s) {
+    const CopyPart parts[3] = {{host->y, dev.y, ny}, {host->u, dev.u, nc}, {host->v, dev.v, nc}};
+    copy_planes(parts, 3, cudaMemcpyDeviceToHost, s, "download");
 }
 
 void validate_params(const rvsb_synth_params* p) {
@@ -268,11 +322,9 @@ rvsb_status rvsb_scene_create(rvsb_context* ctx, const rvsb_camera* inputs, int 
             sc->cams.push_back(inputs[v]);
         }
         for (int v = 0; v < n_inputs; ++v) {
-            for (int k = 0; k < 4; ++k) {
-                auto m = std::make_unique<DevMem>();
-                m->alloc(ctx, plane_bytes(inputs[v], k));
-                sc->planes.push_back(std::move(m));
-            }
+            auto m = std::make_unique<DevMem>();
+            m->alloc(ctx, plane_bytes(inputs[v], 0) + 2 * plane_bytes(inputs[v], 1) + plane_bytes(inputs[v], 3));
+            sc->raw.push_back(std::move(m));
             auto r = std::make_unique<DevMem>();
             auto c = std::make_unique<DevMem>();
             auto cone = std::make_unique<DevMem>();
@@ -334,17 +386,16 @@ rvsb_status rvsb_scene_upload(rvsb_scene* sc, int view, const rvsb_view_planes* 
         check(cudaSetDevice(sc->ctx->device), "cudaSetDevice");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         const rvsb_camera& c = sc->cams[view];
-        for (int k = 0; k < 4; ++k)
-            check(cudaMemcpyAsync(sc->planes[view * 4 + k]->ptr, src[k], plane_bytes(c, k),
-                                  planes_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s),
-                  "upload plane");
-        launch_decode_color(sc->planes[view * 4 + 0]->as<uint16_t>(), sc->planes[view * 4 + 1]->as<uint16_t>(),
-                            sc->planes[view * 4 + 2]->as<uint16_t>(), c.width, c.height,
+        const cudaMemcpyKind kind = planes_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        CopyPart parts[4];
+        for (int k = 0; k < 4; ++k) parts[k] = {sc->plane(view, k), src[k], plane_bytes(c, k)};
+        copy_planes(parts, 4, kind, s, "upload planes");
+        launch_decode_color(sc->plane(view, 0), sc->plane(view, 1), sc->plane(view, 2), c.width, c.height,
                             sc->color[view]->as<uint64_t>(), s);
         check(cudaPeekAtLastError(), "decode colour");
         if (c.projection == RVSB_PROJ_EQUIRECTANGULAR) {
             TileDepthJobs jobs{};
-            jobs.v[0] = TileDepthJob{sc->planes[view * 4 + 3]->as<uint16_t>(), sc->depth_lut[view]->as<float4>(),
+            jobs.v[0] = TileDepthJob{sc->plane(view, 3), sc->depth_lut[view]->as<float4>(),
                                      sc->tile_depth[view]->as<float2>(), c.width, c.height};
             launch_tile_depth(jobs, 1, c.width, c.height, s);
             check(cudaPeekAtLastError(), "tile depth ranges");
@@ -554,9 +605,7 @@ rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, i
         rvsb_status st = synthesize_impl(sc, virt, params, &dev, nullptr, stream);
         if (st != RVSB_OK) return st;
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        check(cudaMemcpyAsync(out_host->y, dev.y, ny, cudaMemcpyDeviceToHost, s), "download Y");
-        check(cudaMemcpyAsync(out_host->u, dev.u, nc, cudaMemcpyDeviceToHost, s), "download U");
-        check(cudaMemcpyAsync(out_host->v, dev.v, nc, cudaMemcpyDeviceToHost, s), "download V");
+        download_yuv(out_host, dev, ny, nc, s);
         check(cudaStreamSynchronize(s), "synchronize");
         return RVSB_OK;
     });
@@ -585,13 +634,15 @@ rvsb_status rvsb_host_stream_create(rvsb_context* ctx, const rvsb_camera* inputs
     if (st != RVSB_OK) return st;
     return guarded(ctx, [&]() -> rvsb_status {
         check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        size_t total = 0;
+        for (int v = 0; v < n_inputs; ++v)
+            for (int k = 0; k < 4; ++k) {
+                hs->plane_off.push_back(total);
+                hs->plane_len.push_back(plane_bytes(inputs[v], k));
+                total += plane_bytes(inputs[v], k);
+            }
         for (auto& s : hs->sets) {
-            for (int v = 0; v < n_inputs; ++v)
-                for (int k = 0; k < 4; ++k) {
-                    auto m = std::make_unique<DevMem>();
-                    m->alloc(ctx, plane_bytes(inputs[v], k));
-                    s.planes.push_back(std::move(m));
-                }
+            s.frame.alloc(ctx, total);
             for (cudaEvent_t* e : {&s.uploaded, &s.computed, &s.downloaded})
                 check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
         }
@@ -632,16 +683,19 @@ rvsb_status rvsb_host_stream_submit(rvsb_host_stream* hs, const rvsb_view_planes
         check(cudaEventRecord(hs->ordered, static_cast<cudaStream_t>(stream)), "record caller stream");
         check(cudaStreamWaitEvent(hs->copy, hs->ordered, 0), "order after caller stream");
         std::vector<rvsb_view_planes> dev(n);
+        char* block = static_cast<char*>(S.frame.ptr);
+        std::vector<CopyPart> parts(4 * n);
+        for (int p = 0; p < 4 * n; ++p) {
+            const rvsb_view_planes& hp = host_planes[p / 4];
+            const void* srcs[4] = {hp.y, hp.u, hp.v, hp.depth};
+            parts[p] = {block + hs->plane_off[p], srcs[p % 4], hs->plane_len[p]};
+        }
+        copy_planes(parts.data(), 4 * n, cudaMemcpyHostToDevice, hs->copy, "upload planes");
         for (int v = 0; v < n; ++v) {
-            const void* src[4] = {host_planes[v].y, host_planes[v].u, host_planes[v].v, host_planes[v].depth};
-            for (int k = 0; k < 4; ++k)
-                check(cudaMemcpyAsync(S.planes[v * 4 + k]->ptr, src[k], plane_bytes(sc->cams[v], k),
-                                      cudaMemcpyHostToDevice, hs->copy),
-                      "upload plane");
-            dev[v].y = S.planes[v * 4 + 0]->as<uint16_t>();
-            dev[v].u = S.planes[v * 4 + 1]->as<uint16_t>();
-            dev[v].v = S.planes[v * 4 + 2]->as<uint16_t>();
-            dev[v].depth = S.planes[v * 4 + 3]->as<uint16_t>();
+            dev[v].y = reinterpret_cast<uint16_t*>(block + hs->plane_off[v * 4 + 0]);
+            dev[v].u = reinterpret_cast<uint16_t*>(block + hs->plane_off[v * 4 + 1]);
+            dev[v].v = reinterpret_cast<uint16_t*>(block + hs->plane_off[v * 4 + 2]);
+            dev[v].depth = reinterpret_cast<uint16_t*>(block + hs->plane_off[v * 4 + 3]);
         }
         check(cudaEventRecord(S.uploaded, hs->copy), "record upload");
         check(cudaStreamWaitEvent(hs->compute, S.uploaded, 0), "wait for upload");
@@ -654,9 +708,7 @@ rvsb_status rvsb_host_stream_submit(rvsb_host_stream* hs, const rvsb_view_planes
         if (st != RVSB_OK) return st;
         check(cudaEventRecord(S.computed, hs->compute), "record synthesis");
         check(cudaStreamWaitEvent(hs->down, S.computed, 0), "wait for synthesis");
-        check(cudaMemcpyAsync(out_host->y, o.y, ny, cudaMemcpyDeviceToHost, hs->down), "download Y");
-        check(cudaMemcpyAsync(out_host->u, o.u, nc, cudaMemcpyDeviceToHost, hs->down), "download U");
-        check(cudaMemcpyAsync(out_host->v, o.v, nc, cudaMemcpyDeviceToHost, hs->down), "download V");
+        download_yuv(out_host, o, ny, nc, hs->down);
         check(cudaEventRecord(S.downloaded, hs->down), "record download");
         S.ticket = hs->next;
         S.busy = true;

@@ -243,10 +243,10 @@ void BatchCore::fill(SlotTable& T, int k, const SlotRequest& r, int variant) {
         V.chroma_sx = (float)V.cw / c.width;
         V.chroma_sy = (float)V.ch / c.height;
         relative_pose(c, virt, V.R, V.t);
-        V.py = sc->planes[v * 4 + 0]->as<uint16_t>();
-        V.pu = sc->planes[v * 4 + 1]->as<uint16_t>();
-        V.pv = sc->planes[v * 4 + 2]->as<uint16_t>();
-        V.pd = r.frame ? r.frame[v].depth : sc->planes[v * 4 + 3]->as<uint16_t>();
+        V.py = sc->plane(v, 0);
+        V.pu = sc->plane(v, 1);
+        V.pv = sc->plane(v, 2);
+        V.pd = r.frame ? r.frame[v].depth : sc->plane(v, 3);
         if (c.projection == RVSB_PROJ_EQUIRECTANGULAR) {
             V.erp_row = sc->erp[v * 2 + 0]->as<float>();
             V.erp_col = sc->erp[v * 2 + 1]->as<float>();

@@ -180,7 +180,9 @@ private:
 struct rvsb_scene {
     rvsb_context* ctx = nullptr;
     std::vector<rvsb_camera> cams;
-    std::vector<std::unique_ptr<rvsb::DevMem>> planes;  // 4 per view: y, u, v, depth
+    // 1 per view: the raw y, u, v and depth planes back to back, so that a
+    // view whose planes are adjacent in host memory uploads in one copy.
+    std::vector<std::unique_ptr<rvsb::DevMem>> raw;
     std::vector<std::unique_ptr<rvsb::DevMem>> erp;     // 2 per view: rows, cols (ERP inputs)
     std::vector<std::unique_ptr<rvsb::DevMem>> color;   // 1 per view: decoded colour words
     std::vector<std::unique_ptr<rvsb::DevMem>> depth_lut;  // 1 per view: 65536 x (d, -d/f0, -d/f1, 0)
@@ -189,4 +191,12 @@ struct rvsb_scene {
     std::vector<bool> uploaded;
     std::unique_ptr<rvsb::BatchCore> single;            // the per-view calls: a batch of one
     int last_launches = 0;
+
+    // Plane k (y, u, v, depth) of view v in its raw block.
+    uint16_t* plane(int v, int k) const {
+        const rvsb_camera& c = cams[v];
+        const size_t ny = (size_t)c.width * c.height, nc = (size_t)(c.width / 2) * (c.height / 2);
+        const size_t off[4] = {0, ny, ny + nc, ny + 2 * nc};
+        return raw[v]->as<uint16_t>() + off[k];
+    }
 };
