@@ -248,7 +248,9 @@ void rvsb_scene_destroy(rvsb_scene* scene);
  * Replaces InputView::load -> read_color / read_depth and their loader
  * kernels (rvs/src/View.cpp:233-257, rvs/src/image_loading.cpp:74-211,
  * rvs_cuda_lib/src/process_input_frame.cu:95-467); the decode itself is
- * fused into the synthesis kernels. */
+ * fused into the synthesis kernels.  Planes that follow each other in the
+ * caller's memory in the order y, u, v, depth (a view's colour frame and
+ * depth frame read into one buffer) are copied in one transfer. */
 rvsb_status rvsb_scene_upload(rvsb_scene* scene, int view, const rvsb_view_planes* planes,
                               int planes_on_device, void* stream);
 
@@ -278,7 +280,9 @@ rvsb_status rvsb_synthesize_frame(rvsb_scene* scene, const rvsb_view_planes* dev
 /* The same call with host buffers on both sides (the reference's plain
  * per-frame path): uploads the n raw input views from host memory,
  * synthesises, and copies the YUV420 result back into host memory.  Blocks
- * until the result is in `out_host`. */
+ * until the result is in `out_host`.  Planes adjacent in host memory move
+ * in one transfer, as in rvsb_scene_upload; so does an `out_host` whose U
+ * plane follows Y and V follows U (one YUV420 frame buffer). */
 rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, int n_inputs,
                                  const rvsb_view_planes* host_planes, const rvsb_camera* virt,
                                  const rvsb_synth_params* params, const rvsb_yuv420* out_host,
@@ -290,7 +294,11 @@ rvsb_status rvsb_synthesize_host(rvsb_context* ctx, const rvsb_camera* inputs, i
  * k+1 on its own stream while frame k synthesises and the download of frame
  * k-1 on a third.  Up to three frames are in flight; a submit that would
  * start a fourth first waits for the oldest.  Host buffers are best pinned (else
- * the copies are synchronous) and must stay untouched until the frame's
+ * the copies are synchronous) and best laid out as one buffer per frame: the
+ * planes of all views back to back (per view y, u, v, depth, views in order)
+ * go up in one transfer, and a YUV420 output buffer comes back in one; one
+ * large transfer runs at the host link's full rate, sixteen plane-sized ones
+ * about 12% below it.  They must stay untouched until the frame's
  * rvsb_host_stream_wait returns.  Each frame's uploads are ordered after
  * the work queued on `stream` before the submit (NULL: the legacy default
  * stream); rvsb_host_stream_join makes `stream` wait for every frame
