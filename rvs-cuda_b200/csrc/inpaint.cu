@@ -22,7 +22,10 @@
 // Every hole lies inside the region and every source lies within one pixel
 // of a hole, so restricting the scans to the grown bounding box changes
 // nothing.  Loads are issued in batches (RB rows, CB chunks) so each thread
-// keeps several in flight.
+// keeps several in flight.  The last column scan only records each hole's
+// choice (its source, or the seed it takes the source from); the gathers
+// that follow a choice (the seed, then the source pixel's codes) run in the
+// write pass, one thread per 2x2 block, off the scans' serial chains.
 #include <algorithm>
 
 #include "device_common.cuh"
@@ -37,6 +40,10 @@ constexpr int kScanBias = 1 << 20;
 constexpr uint32_t kInfD = 0xFFFFFFFFu;
 constexpr int CB = 4;  // row scans: 32-pixel chunks loaded per batch
 constexpr int RB = 8;  // column scans: rows loaded per batch
+// A hole's sweep-1 choice stored in its D0/S0 word by the last column
+// scan: with this bit, (x << 16 | y) of the seed T(q) whose source it
+// takes; without, its source itself (x << 16 | y in the low 32 bits).
+constexpr uint64_t kSeedRef = 1ull << 63;
 
 struct Region {
     int x0, y0, x1, y1;
@@ -409,11 +416,10 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constan
     const DevStatus* __restrict__ st = im.st;
     uint64_t* __restrict__ codes = im.codes;
     const uint8_t* __restrict__ holes = im.holes;
-    const uint64_t* __restrict__ DS = im.scan[1];
+    uint64_t* __restrict__ DS = im.scan[1];
     const uint64_t* __restrict__ Tq = im.scan[2];
     const uint64_t* __restrict__ Tp = im.scan[3];
     const uint64_t* __restrict__ RR = im.scan[0];
-    int32_t* __restrict__ dbg_source = im.sources;
     __shared__ unsigned long long seg_col[32][33];
     __shared__ unsigned long long seg_off[32][33];
     const Region rg = hole_region(st, wo, ho);
@@ -500,7 +506,10 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constan
             run_o = umin64(run_o, off_key(r[k], y));
             if (h[k]) {
                 const size_t o = (size_t)y * wo + x;
+                // The hole's own words: one load round trip, nothing
+                // gathered after it on this chain.
                 const uint64_t tp = Tp[o];
+                const uint64_t ds = DS[o];
                 uint64_t c_cost = tp == ~0ull ? (uint64_t)1 << 40 : (tp >> 32);
                 int c_y = y;
                 if (run_c != kEmptyKey) {
@@ -517,39 +526,45 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constan
                     o_y = 0xffff - (int)((run_o >> 16) & 0xffff);
                     o_x = (int)(run_o & 0xffff);
                 }
-                const uint64_t ds = DS[o];
                 const uint64_t d0 = ds >> 32;
-                uint64_t src = ds;
+                // The choice: the source itself (stay: S0; own seed T'), or
+                // the seed T(q) of the column or off-column minimum.
+                uint64_t choice = ds & 0xffffffffull;
                 if (c_cost <= o_cost) {
-                    if (c_cost < d0) src = (c_y == y) ? tp : Tq[(size_t)c_y * wo + x];
+                    if (c_cost < d0)
+                        choice = (c_y == y) ? (tp & 0xffffffffull)
+                                            : kSeedRef | ((uint64_t)x << 16) | (uint64_t)c_y;
                 } else {
-                    if (o_cost < d0) src = Tq[(size_t)o_y * wo + o_x];
+                    if (o_cost < d0) choice = kSeedRef | ((uint64_t)o_x << 16) | (uint64_t)o_y;
                 }
-                const int sx = (int)((src >> 16) & 0xffff), sy = (int)(src & 0xffff);
-                codes[o] = (codes[(size_t)sy * wo + sx] & kCodeMask) | kHoleBit;
-                if (dbg_source) {
-                    dbg_source[o * 2 + 0] = sx;
-                    dbg_source[o * 2 + 1] = sy;
-                }
+                DS[o] = choice;
             }
             run_c = umin64(run_c, col_key(t[k], y));
         }
     }
 }
 
-// Writes the 2x2 output blocks of the region that hold at least one hole.
+// The fill of inpaint_color (inpainting.cpp:191-198) for the 2x2 blocks of
+// the region that hold at least one hole: each hole follows its recorded
+// choice to its source and takes the source's codes (written back for the
+// passes that read them later: the resize of Precision != 1, the auxiliary
+// outputs, the source list); then, unless the resize writes the output,
+// the block's Y/U/V samples are written.  Sources are never holes, so the
+// codes read here are never the ones written.
 template <class Src>
 __global__ void inpaint_write_kernel(const __grid_constant__ Src src) {
     grid_dep_wait();
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
-    const uint64_t* __restrict__ codes = im.codes;
+    uint64_t* __restrict__ codes = im.codes;
+    const uint64_t* __restrict__ DS = im.scan[1];
+    const uint64_t* __restrict__ Tq = im.scan[2];
+    int32_t* __restrict__ sources = im.sources;
     uint16_t* __restrict__ out_y = im.out_y;
     uint16_t* __restrict__ out_u = im.out_u;
     uint16_t* __restrict__ out_v = im.out_v;
     const int ties_up = im.ties_up;
-    if (im.no_write) return;
     const Region rg = hole_region(st, wo, ho);
     if (rg.empty) return;
     const int bx0 = rg.x0 / 2, by0 = rg.y0 / 2;
@@ -557,8 +572,25 @@ __global__ void inpaint_write_kernel(const __grid_constant__ Src src) {
     const int y = 2 * (by0 + (int)blockIdx.y);
     if (x > rg.x1 || y > rg.y1 || x >= wo || y >= ho) return;
     const size_t o = (size_t)y * wo + x;
-    const uint64_t c00 = codes[o], c01 = codes[o + 1], c10 = codes[o + wo], c11 = codes[o + wo + 1];
+    uint64_t c00 = codes[o], c01 = codes[o + 1], c10 = codes[o + wo], c11 = codes[o + wo + 1];
     if (!((c00 | c01 | c10 | c11) & kHoleBit)) return;
+    auto fill = [&](uint64_t& c, size_t q) {
+        if (!(c & kHoleBit)) return;
+        uint64_t w = DS[q];
+        if (w & kSeedRef) w = Tq[(size_t)(w & 0xffff) * wo + ((w >> 16) & 0xffff)];
+        const int sx = (int)((w >> 16) & 0xffff), sy = (int)(w & 0xffff);
+        c = (codes[(size_t)sy * wo + sx] & kCodeMask) | kHoleBit;
+        codes[q] = c;
+        if (sources) {
+            sources[q * 2 + 0] = sx;
+            sources[q * 2 + 1] = sy;
+        }
+    };
+    fill(c00, o);
+    fill(c01, o + 1);
+    fill(c10, o + wo);
+    fill(c11, o + wo + 1);
+    if (im.no_write) return;
     out_y[o] = (uint16_t)(c00 & 0xffff);
     out_y[o + 1] = (uint16_t)(c01 & 0xffff);
     out_y[o + wo] = (uint16_t)(c10 & 0xffff);
@@ -639,6 +671,7 @@ void launch_inpaint_scans(DevStatus* st, const uint8_t* holes, uint64_t* codes, 
     src.im.ties_up = 0;
     src.im.no_write = 1;
     launch_scans(src, w, h, 1, 1, s);
+    launch_dependent(inpaint_write_kernel<Direct>, dim3((w / 2 + 127) / 128, (h + 1) / 2, 1), dim3(128), 0, s, src);
 }
 
 }  // namespace rvsb
