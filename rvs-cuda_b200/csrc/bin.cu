@@ -7,93 +7,73 @@
 namespace rvsb {
 namespace {
 
-// Exclusive scan of one slot's bin counts (one CTA of 1024 threads per slot).
+// Exclusive scan of one slot's bin counts (one CTA of 1024 threads per
+// slot), and the raster's launch order of the tiles: those with clearly
+// more bin entries than the average (over all views; mostly tiles crossed
+// by stretched triangles) first, then the others, each part in raster order
+// so that neighbouring tiles, which share input blocks, still run together.
+// Tiles are independent, so the order changes only the schedule.  Each
+// thread takes a run of whole tiles (all views of each), so one pass over
+// the counts yields both its entry sum and its heavy-tile count, and one
+// 64-bit scan (entries << 32 | heavy tiles) gives both prefixes.
 template <class Tabs>
 __global__ void __launch_bounds__(1024) bin_scan_kernel(const __grid_constant__ Tabs tabs) {
     dev::grid_dep_wait();
-    __shared__ int warp_sums[32];
+    __shared__ unsigned long long warp_sums[32];
     const SlotTable& tab = tabs.at(blockIdx.x);
     const int* counts = tab.b.counts;
     int* offsets = tab.b.offsets;
     int* cursor = tab.b.cursor;
-    const int n = tab.t.ntx * tab.t.nty * tab.t.n_views;
-    const int tid = threadIdx.x;
-    const int per = (n + 1023) / 1024;
-    const int beg = min(n, tid * per), end = min(n, beg + per);
-    int local = 0;
-    for (int k = beg; k < end; ++k) local += counts[k];
-    int x = local;
-    const int lane = tid & 31, warp = tid >> 5;
+    const int nv = tab.t.n_views, ntiles = tab.t.ntx * tab.t.nty;
+    const long long total = tab.b.status->bin_total;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tper = (ntiles + 1023) / 1024;
+    const int tb = min(ntiles, tid * tper), te = min(ntiles, tb + tper);
+    auto heavy = [&](long long e) { return 2 * e * ntiles > 3 * total; };  // more than 1.5x the mean
+    unsigned long long local = 0;
+    for (int t = tb; t < te; ++t) {
+        long long e = 0;
+        for (int v = 0; v < nv; ++v) e += counts[t * nv + v];
+        local += ((unsigned long long)e << 32) | (heavy(e) ? 1u : 0u);
+    }
+    unsigned long long x = local;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
     if (lane == 31) warp_sums[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        int s = warp_sums[lane];
+        unsigned long long s = warp_sums[lane];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
             if (lane >= o) s += y;
         }
         warp_sums[lane] = s;
     }
     __syncthreads();
-    int run = x - local + (warp > 0 ? warp_sums[warp - 1] : 0);
-    for (int k = beg; k < end; ++k) {
-        offsets[k] = run;
-        cursor[k] = run;
-        run += counts[k];
-    }
-    if (tid == 0 && tab.b.status->bin_total > tab.b.capacity) tab.b.status->bin_overflow = 1;
-
-    // Raster launch order: the tiles with clearly more bin entries than the
-    // average (over all views; mostly tiles crossed by stretched triangles)
-    // first, then the others, each part in raster order so that
-    // neighbouring tiles, which share input blocks, still run together.
-    // Tiles are independent, so the order changes only the schedule.
-    __syncthreads();
-    const int nv = tab.t.n_views, ntiles = tab.t.ntx * tab.t.nty;
-    const long long total = tab.b.status->bin_total;
-    const int tper = (ntiles + 1023) / 1024;
-    const int tb = min(ntiles, tid * tper), te = min(ntiles, tb + tper);
-    auto heavy = [&](int t) {
-        long long e = 0;
-        for (int v = 0; v < nv; ++v) e += counts[t * nv + v];
-        return 2 * e * ntiles > 3 * total;  // more than 1.5x the mean
-    };
-    int nh = 0;
-    for (int t = tb; t < te; ++t) nh += heavy(t) ? 1 : 0;
-    int hx = nh;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y2 = __shfl_up_sync(0xffffffffu, hx, o);
-        if (lane >= o) hx += y2;
-    }
-    __syncthreads();
-    if (lane == 31) warp_sums[warp] = hx;
-    __syncthreads();
-    if (warp == 0) {
-        int s2 = warp_sums[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y2 = __shfl_up_sync(0xffffffffu, s2, o);
-            if (lane >= o) s2 += y2;
-        }
-        warp_sums[lane] = s2;
-    }
-    __syncthreads();
-    const int hbefore = hx - nh + (warp > 0 ? warp_sums[warp - 1] : 0);
-    const int nheavy = warp_sums[31];
+    const unsigned long long before = x - local + (warp > 0 ? warp_sums[warp - 1] : 0ull);
+    const int nheavy = (int)(warp_sums[31] & 0xffffffffu);
+    int run = (int)(before >> 32);
+    const int hbefore = (int)(before & 0xffffffffu);
     int ph = hbefore, pl = nheavy + (tb - hbefore);
     for (int t = tb; t < te; ++t) {
-        if (heavy(t))
+        long long e = 0;
+        for (int v = 0; v < nv; ++v) {
+            const int c = counts[t * nv + v];
+            offsets[t * nv + v] = run;
+            cursor[t * nv + v] = run;
+            run += c;
+            e += c;
+        }
+        if (heavy(e))
             tab.b.tile_order[ph++] = t;
         else
             tab.b.tile_order[pl++] = t;
     }
+    if (tid == 0 && total > tab.b.capacity) tab.b.status->bin_overflow = 1;
 }
 
 // Grid (ceil(max_blocks / 256), max_views, slots): one thread per binning
@@ -114,11 +94,23 @@ __global__ void bin_fill_kernel(const __grid_constant__ Tabs tabs) {
     const int tx0 = bb.x >> wl, tx1 = bb.z >> wl, ty0 = bb.y >> hl, ty1 = bb.w >> hl;
     int* cursor = tab.b.cursor;
     int* list = tab.b.list;
+    const int entry = ((b / V.nbx) << 11) | (b % V.nbx);  // block row << 11 | block column
+    // Neighbouring blocks (the lanes of a warp) mostly fall in the same
+    // single tile: those lanes take their places with one atomic per tile.
+    const bool single = tx0 == tx1 && ty0 == ty1;
+    const unsigned active = __activemask();
+    const int cell = single ? (ty0 * ntx + tx0) * n + v : -1 - (int)(threadIdx.x & 31);
+    const unsigned same = __match_any_sync(active, cell);
+    if (single) {
+        const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&cursor[cell], __popc(same));
+        base = __shfl_sync(same, base, leader);
+        list[base + __popc(same & ((1u << lane) - 1u))] = entry;
+        return;
+    }
     for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx) {
-            const int pos = atomicAdd(&cursor[(ty * ntx + tx) * n + v], 1);
-            list[pos] = ((b / V.nbx) << 11) | (b % V.nbx);  // block row << 11 | block column
-        }
+        for (int tx = tx0; tx <= tx1; ++tx) list[atomicAdd(&cursor[(ty * ntx + tx) * n + v], 1)] = entry;
 }
 
 }  // namespace
