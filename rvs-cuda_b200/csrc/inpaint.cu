@@ -40,6 +40,7 @@ constexpr int kScanBias = 1 << 20;
 constexpr uint32_t kInfD = 0xFFFFFFFFu;
 constexpr int CB = 4;  // row scans: 32-pixel chunks loaded per batch
 constexpr int RB = 8;  // column scans: rows loaded per batch
+constexpr int RB1 = 4; // last column scan: rows per batch (five words a row)
 // A hole's sweep-1 choice stored in its D0/S0 word by the last column
 // scan: with this bit, (x << 16 | y) of the seed T(q) whose source it
 // takes; without, its source itself (x << 16 | y in the low 32 bits).
@@ -486,30 +487,33 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constan
         run_o = umin64(run_o, src_seg[32 + lane]);
     }
     if (!col_ok) return;
-    // Bottom-up over the segment in batches of RB rows.
-    for (int y1 = ye; y1 >= yb; y1 -= RB) {
-        uint64_t t[RB], r[RB];
-        uint8_t h[RB];
+    // Bottom-up over the segment in batches of RB1 rows; every word a row
+    // needs (the holes' own T' and D0/S0 too) is loaded with the batch, so
+    // nothing on the serial chain below waits for memory.
+    for (int y1 = ye; y1 >= yb; y1 -= RB1) {
+        uint64_t t[RB1], r[RB1], tpk[RB1], dsk[RB1];
+        uint8_t h[RB1];
 #pragma unroll
-        for (int k = 0; k < RB; ++k) {
+        for (int k = 0; k < RB1; ++k) {
             const int y = y1 - k;
             const bool ok = y >= yb;
-            t[k] = ok ? Tq[(size_t)y * wo + x] : ~0ull;
-            r[k] = ok ? RR[(size_t)y * wo + x] : ~0ull;
-            h[k] = ok ? holes[(size_t)y * wo + x] : 0;
+            const size_t o = (size_t)y * wo + x;
+            t[k] = ok ? Tq[o] : ~0ull;
+            r[k] = ok ? RR[o] : ~0ull;
+            h[k] = ok ? holes[o] : 0;
+            tpk[k] = ok ? Tp[o] : 0ull;
+            dsk[k] = ok ? DS[o] : 0ull;
         }
 #pragma unroll
-        for (int k = 0; k < RB; ++k) {
+        for (int k = 0; k < RB1; ++k) {
             const int y = y1 - k;
             if (y < yb) break;
             // run_c holds the exclusive (rows below) column minimum here.
             run_o = umin64(run_o, off_key(r[k], y));
             if (h[k]) {
                 const size_t o = (size_t)y * wo + x;
-                // The hole's own words: one load round trip, nothing
-                // gathered after it on this chain.
-                const uint64_t tp = Tp[o];
-                const uint64_t ds = DS[o];
+                const uint64_t tp = tpk[k];
+                const uint64_t ds = dsk[k];
                 uint64_t c_cost = tp == ~0ull ? (uint64_t)1 << 40 : (tp >> 32);
                 int c_y = y;
                 if (run_c != kEmptyKey) {
