@@ -11,7 +11,7 @@
    against later changes and give the GPU tests fixed expected outputs.
 
 Run from the repository root: python tests/golden/make_golden.py
-(needs cv2, which the GPU box does not need: the tests read the .npz files).
+(needs cv2; the tests themselves only read the .npz files).
 """
 import os
 import sys
