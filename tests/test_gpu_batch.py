@@ -166,3 +166,25 @@ def test_default_raster_variant_follows_magnification(ctx):
         for x, y in zip(got, _yuv(out2, cam)):
             np.testing.assert_array_equal(x, y)
     b.close()
+
+
+@pytest.mark.parametrize("name,n,picks", [("batched_erp", 8, (0, 5)), ("batched_mixed", 6, (0, 1))])
+def test_batched_configuration_full_size(ctx, name, n, picks):
+    """The batched configurations at full size through the tuned batch call:
+    4 ERP 4096x2048 inputs seen by 1920x1080 views (magnified: the tuner
+    takes the medium-triangle variant) and 11 perspective 2048x1088 inputs
+    seen by views of mixed sizes.  Two targets of each against the oracle."""
+    import torch
+    wl = getattr(scenes, name)(n_targets=n)
+    sc = _upload(ctx, wl)
+    p = rvsb.params(wl.blending_factor)
+    b = rvsb.Batch(sc, n)
+    b.set_autotune(True)
+    outs = [yuv_planes_torch(c.width, c.height) for c in wl.targets]
+    b.synthesize(wl.targets, p, outs)
+    torch.cuda.synchronize()
+    print(name, "raster variant", b.last_raster_variant())
+    for k in picks:
+        c = wl.targets[k]
+        print(assert_parity(_yuv(outs[k], c), O.synthesize(wl.inputs, wl.planes, c, wl.blending_factor)))
+    b.close()
