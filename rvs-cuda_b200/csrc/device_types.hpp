@@ -159,7 +159,7 @@ struct SlotBuffers {
     uint64_t* codes;     // Wo*Ho packed output codes + hole bit
     uint8_t* holes;      // Wo*Ho hole mask (1 = no view covers the pixel)
     uint64_t* scan[4];   // Wo*Ho inpainting scratch each
-    uint64_t* inpaint_seg;  // column-group minima of the inpainting passes
+    uint64_t* inpaint_seg;  // column-group and warp-segment minima of the inpainting pre-passes
     int* tile_order;        // output tiles, most bin entries first (raster launch order)
     float4* pcolor;      // Precision != 1: blended colour per raster pixel
     int32_t* psrc;       // Precision != 1: inpainting source of every hole

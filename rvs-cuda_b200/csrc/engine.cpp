@@ -84,7 +84,7 @@ size_t SlotWorkspace::bytes_for(const rvsb_scene* sc, int wo, int ho, bool resca
     const SlotNeeds n = needs_of(sc, wo, ho);
     return sizeof(DevStatus) + n.vert * sizeof(float4) + n.bbox * sizeof(int4) + 3 * n.bins * sizeof(int) +
            n.list * sizeof(int) + n.out * (sizeof(uint64_t) * 5 + 1) +
-           (size_t)INPAINT_MAX_GROUPS * ((wo + 31) / 32) * 64 * sizeof(uint64_t) +
+           inpaint_seg_words(wo) * sizeof(uint64_t) +
            n.bins / std::max<size_t>(1, sc->cams.size()) * sizeof(int) +
            (rescale ? n.out * (sizeof(float4) + 2 * sizeof(int32_t)) : 0);
 }
@@ -124,10 +124,10 @@ void SlotWorkspace::ensure(rvsb_context* ctx, const rvsb_scene* sc, int wo, int 
         tile_order.alloc(ctx, tiles * sizeof(int));
         cap_tiles = tiles;
     }
-    const size_t strips = (size_t)(wo + 31) / 32;
-    if (strips > cap_strips) {
-        inpaint_seg.alloc(ctx, (size_t)INPAINT_MAX_GROUPS * strips * 64 * sizeof(uint64_t));
-        cap_strips = strips;
+    const size_t seg_words = inpaint_seg_words(wo);
+    if (seg_words > cap_seg_words) {
+        inpaint_seg.alloc(ctx, seg_words * sizeof(uint64_t));
+        cap_seg_words = seg_words;
     }
     if (n.out > cap_out) {
         codes.alloc(ctx, n.out * sizeof(uint64_t));

@@ -78,7 +78,7 @@ struct SlotWorkspace {
     DevMem pcolor, psrc;          // Precision != 1: raster-size colour and inpainting sources
     size_t cap_rescale = 0;
     void ensure_rescale(rvsb_context* ctx, int wo, int ho);
-    size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0, cap_aux = 0, cap_strips = 0;
+    size_t cap_vert = 0, cap_bbox = 0, cap_out = 0, cap_bins = 0, cap_list = 0, cap_aux = 0, cap_seg_words = 0;
     void ensure_aux(rvsb_context* ctx, int wo, int ho);
 
     // Bytes a slot needs for `scene` at raster size wo x ho (rescale: plus

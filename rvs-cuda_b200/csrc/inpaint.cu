@@ -232,9 +232,22 @@ __device__ __forceinline__ GroupRows group_rows(const Region& rg, int G, int w) 
     return r;
 }
 
+// The column-minima table of the pre-passes (G > 1): first every group's
+// minima per strip (64 words: 32 lanes, and 32 more for the second key of
+// the backward scan), then every warp segment's minima, 32 segments per
+// group and strip, so that the scan passes need not re-read their own
+// rows to find the carry from the segments before them.
+__device__ __forceinline__ size_t seg_total(int g, int nstrips, int strip) {
+    return ((size_t)g * nstrips + strip) * 64;
+}
+__device__ __forceinline__ size_t seg_warp(int G, int g, int nstrips, int strip, int w) {
+    return (size_t)G * nstrips * 64 + (((size_t)g * nstrips + strip) * 32 + w) * 64;
+}
+
 // Grid (strips of 32 columns, G row groups, images).  With PRE the CTA only
-// stores its group's column minima; otherwise it scans its group starting
-// from the minima of the groups above it.
+// stores its group's and its warp segments' column minima; otherwise it
+// scans its group starting from the minima of the groups and segments
+// above it (recomputed from its own rows when G = 1).
 template <class Src, bool PRE>
 __global__ void __launch_bounds__(1024) inpaint_col0_kernel(const __grid_constant__ Src src, int G) {
     grid_dep_wait();
@@ -254,29 +267,34 @@ __global__ void __launch_bounds__(1024) inpaint_col0_kernel(const __grid_constan
     const GroupRows gr = group_rows(rg, G, w);
     const int yb = gr.yb, ye = gr.ye;
     const bool col_ok = x <= rg.x1;
-    unsigned long long m = kEmptyKey;
-    if (col_ok)
-        for (int y0 = yb; y0 <= ye; y0 += RB) {
-            uint64_t r[RB];
-#pragma unroll
-            for (int k = 0; k < RB; ++k) r[k] = y0 + k <= ye ? R[(size_t)(y0 + k) * wo + x] : ~0ull;
-#pragma unroll
-            for (int k = 0; k < RB; ++k) m = umin64(m, col0_key(r[k], y0 + k));
-        }
-    seg[w][lane] = m;
-    __syncthreads();
-    if (PRE) {
-        if (w == 0) {
-            unsigned long long t = kEmptyKey;
-            for (int s = 0; s < 32; ++s) t = umin64(t, seg[s][lane]);
-            im.seg[((size_t)blockIdx.y * nstrips + blockIdx.x) * 64 + lane] = t;
-        }
-        return;
-    }
     unsigned long long run = kEmptyKey;
-    for (int s = 0; s < w; ++s) run = umin64(run, seg[s][lane]);
-    for (int g = 0; g < (int)blockIdx.y; ++g)
-        run = umin64(run, im.seg[((size_t)g * nstrips + blockIdx.x) * 64 + lane]);
+    if (PRE || G == 1) {
+        unsigned long long m = kEmptyKey;
+        if (col_ok)
+            for (int y0 = yb; y0 <= ye; y0 += RB) {
+                uint64_t r[RB];
+#pragma unroll
+                for (int k = 0; k < RB; ++k) r[k] = y0 + k <= ye ? R[(size_t)(y0 + k) * wo + x] : ~0ull;
+#pragma unroll
+                for (int k = 0; k < RB; ++k) m = umin64(m, col0_key(r[k], y0 + k));
+            }
+        seg[w][lane] = m;
+        __syncthreads();
+        if (PRE) {
+            im.seg[seg_warp(G, blockIdx.y, nstrips, blockIdx.x, w) + lane] = m;
+            if (w == 0) {
+                unsigned long long t = kEmptyKey;
+                for (int s = 0; s < 32; ++s) t = umin64(t, seg[s][lane]);
+                im.seg[seg_total(blockIdx.y, nstrips, blockIdx.x) + lane] = t;
+            }
+            return;
+        }
+        for (int s = 0; s < w; ++s) run = umin64(run, seg[s][lane]);
+    } else {
+        const uint64_t* sw = im.seg + seg_warp(G, blockIdx.y, nstrips, blockIdx.x, 0);
+        for (int s = 0; s < w; ++s) run = umin64(run, sw[s * 64 + lane]);
+    }
+    for (int g = 0; g < (int)blockIdx.y; ++g) run = umin64(run, im.seg[seg_total(g, nstrips, blockIdx.x) + lane]);
     if (!col_ok) return;
     const uint32_t big = (uint32_t)(wo + ho);
     for (int y0 = yb; y0 <= ye; y0 += RB) {
@@ -443,46 +461,57 @@ __global__ void __launch_bounds__(1024) inpaint_col1_kernel(const __grid_constan
         const uint64_t v = (r >> 16) - (uint64_t)x + (uint64_t)y;
         return (v << 32) | ((uint64_t)(0xffff - y) << 16) | (r & 0xffff);
     };
-    unsigned long long mc = kEmptyKey, mo = kEmptyKey;
-    if (col_ok)
-        for (int y0 = yb; y0 <= ye; y0 += RB) {
-            uint64_t t[RB], r[RB];
-#pragma unroll
-            for (int k = 0; k < RB; ++k) {
-                const bool ok = y0 + k <= ye;
-                t[k] = ok ? Tq[(size_t)(y0 + k) * wo + x] : ~0ull;
-                r[k] = ok ? RR[(size_t)(y0 + k) * wo + x] : ~0ull;
-            }
-#pragma unroll
-            for (int k = 0; k < RB; ++k) {
-                if (y0 + k > ye) break;
-                mc = umin64(mc, col_key(t[k], y0 + k));
-                mo = umin64(mo, off_key(r[k], y0 + k));
-            }
-        }
-    seg_col[w][lane] = mc;
-    seg_off[w][lane] = mo;
-    __syncthreads();
-    if (PRE) {
-        if (w == 0) {
-            unsigned long long tc = kEmptyKey, to = kEmptyKey;
-            for (int s = 0; s < 32; ++s) {
-                tc = umin64(tc, seg_col[s][lane]);
-                to = umin64(to, seg_off[s][lane]);
-            }
-            uint64_t* dst = im.seg + ((size_t)blockIdx.y * nstrips + blockIdx.x) * 64;
-            dst[lane] = tc;
-            dst[32 + lane] = to;
-        }
-        return;
-    }
     unsigned long long run_c = kEmptyKey, run_o = kEmptyKey;
-    for (int s = w + 1; s < 32; ++s) {
-        run_c = umin64(run_c, seg_col[s][lane]);
-        run_o = umin64(run_o, seg_off[s][lane]);
+    if (PRE || G == 1) {
+        unsigned long long mc = kEmptyKey, mo = kEmptyKey;
+        if (col_ok)
+            for (int y0 = yb; y0 <= ye; y0 += RB) {
+                uint64_t t[RB], r[RB];
+#pragma unroll
+                for (int k = 0; k < RB; ++k) {
+                    const bool ok = y0 + k <= ye;
+                    t[k] = ok ? Tq[(size_t)(y0 + k) * wo + x] : ~0ull;
+                    r[k] = ok ? RR[(size_t)(y0 + k) * wo + x] : ~0ull;
+                }
+#pragma unroll
+                for (int k = 0; k < RB; ++k) {
+                    if (y0 + k > ye) break;
+                    mc = umin64(mc, col_key(t[k], y0 + k));
+                    mo = umin64(mo, off_key(r[k], y0 + k));
+                }
+            }
+        seg_col[w][lane] = mc;
+        seg_off[w][lane] = mo;
+        __syncthreads();
+        if (PRE) {
+            uint64_t* own = im.seg + seg_warp(G, blockIdx.y, nstrips, blockIdx.x, w);
+            own[lane] = mc;
+            own[32 + lane] = mo;
+            if (w == 0) {
+                unsigned long long tc = kEmptyKey, to = kEmptyKey;
+                for (int s = 0; s < 32; ++s) {
+                    tc = umin64(tc, seg_col[s][lane]);
+                    to = umin64(to, seg_off[s][lane]);
+                }
+                uint64_t* dst = im.seg + seg_total(blockIdx.y, nstrips, blockIdx.x);
+                dst[lane] = tc;
+                dst[32 + lane] = to;
+            }
+            return;
+        }
+        for (int s = w + 1; s < 32; ++s) {
+            run_c = umin64(run_c, seg_col[s][lane]);
+            run_o = umin64(run_o, seg_off[s][lane]);
+        }
+    } else {
+        const uint64_t* sw = im.seg + seg_warp(G, blockIdx.y, nstrips, blockIdx.x, 0);
+        for (int s = w + 1; s < 32; ++s) {
+            run_c = umin64(run_c, sw[s * 64 + lane]);
+            run_o = umin64(run_o, sw[s * 64 + 32 + lane]);
+        }
     }
     for (int g = (int)blockIdx.y + 1; g < G; ++g) {
-        const uint64_t* src_seg = im.seg + ((size_t)g * nstrips + blockIdx.x) * 64;
+        const uint64_t* src_seg = im.seg + seg_total(g, nstrips, blockIdx.x);
         run_c = umin64(run_c, src_seg[lane]);
         run_o = umin64(run_o, src_seg[32 + lane]);
     }
@@ -647,6 +676,13 @@ int column_groups(int max_w, int images) {
 }
 
 }  // namespace
+
+size_t inpaint_seg_words(int wo) {
+    // The most row groups any launch with an output this wide can use (one
+    // image); the table is unused with one group.
+    const int G = column_groups(wo, 1);
+    return G > 1 ? (size_t)G * ((wo + 31) / 32) * 64 * 33 : 1;
+}
 
 template <class Tabs>
 int launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {

@@ -135,6 +135,10 @@ void launch_decode_color(const uint16_t* y, const uint16_t* u, const uint16_t* v
 // Inpainting of one image outside a batch (no slot table): the scans over
 // `holes` with caller-provided scratch (status, codes and four scan buffers
 // of w*h words each); the chosen source of every hole goes to `sources`.
+// Words of a slot's inpainting column-minima table for outputs up to wo
+// wide (group minima and warp-segment minima of the column pre-passes).
+size_t inpaint_seg_words(int wo);
+
 void launch_inpaint_scans(DevStatus* st, const uint8_t* holes, uint64_t* codes, uint64_t* const scan[4], int w,
                           int h, int32_t* sources, cudaStream_t s);
 
