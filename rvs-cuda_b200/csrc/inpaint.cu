@@ -331,29 +331,19 @@ __device__ __forceinline__ uint64_t ds_at(const uint64_t* DS, const Region& rg, 
     return DS[(size_t)y * wo + x];
 }
 
-// Sweep 1 seeds: T(q) = best of stay (D0(q), S0(q)), left (D0+1, S0 of left),
-// up (D0+1, S0 of up) with priority stay > left > up; T'(q) the same without
-// stay.  Non-holes: (0, q).
-template <class Src>
-__global__ void inpaint_seed1_kernel(const __grid_constant__ Src src) {
-    grid_dep_wait();
-    const InpaintImage im = src();
-    const int wo = im.wo, ho = im.ho;
-    const DevStatus* __restrict__ st = im.st;
-    const uint8_t* __restrict__ holes = im.holes;
-    const uint64_t* __restrict__ DS = im.scan[1];
-    uint64_t* __restrict__ Tq = im.scan[2];
-    uint64_t* __restrict__ Tp = im.scan[3];
-    const Region rg = hole_region(st, wo, ho);
-    if (rg.empty) return;
-    const int x = rg.x0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int y = rg.y0 + (int)blockIdx.y;
-    if (x > rg.x1 || y > rg.y1) return;
+// Sweep 1 seeds of region pixel (x, y): T(q) = best of stay (D0(q), S0(q)),
+// left (D0+1, S0 of left), up (D0+1, S0 of up) with priority stay > left >
+// up; T'(q) the same without stay.  Non-holes: (0, q).  Stores both and
+// returns T(q).
+__device__ __forceinline__ uint64_t seed1_at(const uint8_t* __restrict__ holes, const uint64_t* __restrict__ DS,
+                                             uint64_t* __restrict__ Tq, uint64_t* __restrict__ Tp,
+                                             const Region& rg, int wo, int x, int y) {
     const size_t o = (size_t)y * wo + x;
     if (!holes[o]) {
-        Tq[o] = pack_dxy(0, x, y);
-        Tp[o] = pack_dxy(0, x, y);
-        return;
+        const uint64_t self = pack_dxy(0, x, y);
+        Tq[o] = self;
+        Tp[o] = self;
+        return self;
     }
     const uint64_t self = DS[o];
     uint64_t best = self;
@@ -370,17 +360,22 @@ __global__ void inpaint_seed1_kernel(const __grid_constant__ Src src) {
     }
     Tq[o] = best;
     Tp[o] = bp;
+    return best;
 }
 
 // Sweep 1, rows (backward, exclusive): RR(x, y) = min over q.x > x of
-// (T(q).d + q.x, q.x).  One warp per row.
+// (T(q).d + q.x, q.x), with the seeds T, T' computed (and stored for the
+// column pass and the fill) as the row reads them.  One CTA per row.
 template <class Src>
 __global__ void __launch_bounds__(32 * ROW_WARPS) inpaint_row1_kernel(const __grid_constant__ Src src) {
     grid_dep_wait();
     const InpaintImage im = src();
     const int wo = im.wo, ho = im.ho;
     const DevStatus* __restrict__ st = im.st;
-    const uint64_t* __restrict__ Tq = im.scan[2];
+    const uint8_t* __restrict__ holes = im.holes;
+    const uint64_t* __restrict__ DS = im.scan[1];
+    uint64_t* __restrict__ Tq = im.scan[2];
+    uint64_t* __restrict__ Tp = im.scan[3];
     uint64_t* __restrict__ RR = im.scan[0];
     __shared__ unsigned long long s_min[ROW_WARPS];
     const Region rg = hole_region(st, wo, ho);
@@ -401,7 +396,7 @@ __global__ void __launch_bounds__(32 * ROW_WARPS) inpaint_row1_kernel(const __gr
             const int x = rg.x1 - (base + 32 * c + (31 - lane));
             unsigned long long key = kEmptyKey;
             if (x >= rg.x0) {
-                const uint64_t t = Tq[(size_t)y * wo + x];
+                const uint64_t t = seed1_at(holes, DS, Tq, Tp, rg, wo, x, y);
                 key = ((unsigned long long)((t >> 32) + (uint64_t)x) << 16) | (unsigned long long)x;
             }
             const unsigned long long incl = umin64(warp_incl_min_rev(key, lane), local);
@@ -648,11 +643,10 @@ int launch_scans(const Src& src, int max_w, int max_h, int images, int G, cudaSt
     launch_dependent(inpaint_row0_kernel<Src>, dim3(max_h, 1, images), dim3(32 * ROW_WARPS), 0, s, src);
     if (G > 1) launch_dependent(inpaint_col0_kernel<Src, true>, dim3(strips, G, images), dim3(1024), 0, s, src, G);
     launch_dependent(inpaint_col0_kernel<Src, false>, dim3(strips, G, images), dim3(1024), 0, s, src, G);
-    launch_dependent(inpaint_seed1_kernel<Src>, dim3((max_w + 255) / 256, max_h, images), dim3(256), 0, s, src);
     launch_dependent(inpaint_row1_kernel<Src>, dim3(max_h, 1, images), dim3(32 * ROW_WARPS), 0, s, src);
     if (G > 1) launch_dependent(inpaint_col1_kernel<Src, true>, dim3(strips, G, images), dim3(1024), 0, s, src, G);
     launch_dependent(inpaint_col1_kernel<Src, false>, dim3(strips, G, images), dim3(1024), 0, s, src, G);
-    launches = 5 + (G > 1 ? 2 : 0);
+    launches = 4 + (G > 1 ? 2 : 0);
     return launches;
 }
 
