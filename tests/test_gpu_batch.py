@@ -188,3 +188,25 @@ def test_batched_configuration_full_size(ctx, name, n, picks):
         c = wl.targets[k]
         print(assert_parity(_yuv(outs[k], c), O.synthesize(wl.inputs, wl.planes, c, wl.blending_factor)))
     b.close()
+
+
+def test_batch_slot_seeing_nothing(ctx):
+    """A batch whose first slot's camera faces away from the scene (every
+    pixel a hole, nothing to inpaint from) beside slots that see it: each
+    slot's bytes equal its per-view call."""
+    import torch
+    wl = scenes.random_pose_small(n_views=2, w=64, h=36, seed=7)
+    sc = _upload(ctx, wl)
+    p = rvsb.params(5.0)
+    away = copy.deepcopy(wl.targets[0])
+    away.rotation[0] += 180.0
+    cams = [away] + _targets_small(wl)[:3]
+    expected = [_single(sc, c, p) for c in cams]
+    b = rvsb.Batch(sc, len(cams))
+    outs = [yuv_planes_torch(c.width, c.height) for c in cams]
+    b.synthesize(cams, p, outs)
+    torch.cuda.synchronize()
+    for c, o, e in zip(cams, outs, expected):
+        for x, y in zip(_yuv(o, c), e):
+            np.testing.assert_array_equal(x, y)
+    b.close()

@@ -208,3 +208,22 @@ def test_magnified_every_raster_variant(ctx, seed, mag):
     for yuv in results[1:]:
         for a, b in zip(yuv, results[0]):
             np.testing.assert_array_equal(a, b)
+
+
+def test_view_facing_away(ctx):
+    """A virtual camera that sees none of the scene: every pixel is a hole
+    and there is no source to inpaint from, so the output is the empty
+    colour (0, 1, 0) quantised, as the oracle's, with the whole frame in the
+    hole mask; the plain call and the debug call alike."""
+    import copy
+    wl = scenes.random_pose_small(n_views=2, w=64, h=36, seed=7)
+    target = copy.deepcopy(wl.targets[0])
+    target.rotation[0] += 180.0
+    cpu, cq, _ = O.synthesize(wl.inputs, wl.planes, target, 5.0, want_intermediate=True)
+    assert not (cq > 0).any()
+    plain, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0)
+    dyuv, dbg, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, debug=True)
+    assert not (dbg["blend_quality"] > 0).any()
+    for yuv in (plain, dyuv):
+        for a, b in zip(yuv, cpu):
+            np.testing.assert_array_equal(a, b)
