@@ -8,9 +8,12 @@ reference's per-frame InputView::load) and synthesising.
 
   value  views/s with the input planes resident in HBM (device-timed with
          CUDA events around each synthesis; L2 flushed between steps).
-  e2e    the same metric through the reference-facing C-ABI call with host
-         buffers (rvsb_synthesize_host): pinned host -> device upload of the
-         raw planes, synthesis and download of the YUV420 result every step.
+  e2e    the same metric through the reference-facing C-ABI calls with host
+         buffers (rvsb_host_stream_submit, the frame loop with its
+         asynchronous loader and writer): pinned host -> device upload of
+         the raw planes, synthesis and download of the YUV420 result every
+         step, consecutive frames overlapped; the blocking one-frame call
+         rvsb_synthesize_host is reported beside it.
   roofline  of the dominant kernel, with its algorithmic bytes per launch.
   cpu_baseline  the CPU oracle (a restatement of the reference's CPU path)
          on a bounded sample, 1 thread (the reference's loops are serial).

@@ -152,8 +152,11 @@ extern "C" rvsb_status rvsb_inpaint_sources_noalloc(const uint8_t* holes, int wi
         set_error(err, err_len, "%s", "null hole mask or source buffer");
         return RVSB_E_ARG;
     }
-    if (width <= 0 || height <= 0 || width > 65535 || height > 65535) {
-        set_error(err, err_len, "image size %d x %d is invalid (each side 1..65535)", width, height);
+    // The fill pass works on 2x2 blocks (as the synthesis path's inpainting
+    // does), so both sides must be even; the scan words hold 16-bit
+    // coordinates, and 32768 is the synthesis path's largest side.
+    if (width < 2 || height < 2 || (width & 1) || (height & 1) || width > 32768 || height > 32768) {
+        set_error(err, err_len, "image size %d x %d is invalid (each side even, 2..32768)", width, height);
         return RVSB_E_ARG;
     }
     const long long npix = (long long)width * height;
@@ -175,8 +178,15 @@ extern "C" rvsb_status rvsb_inpaint_sources_noalloc(const uint8_t* holes, int wi
     uint64_t* scan[4];
     for (int k = 0; k < 4; ++k) scan[k] = words + (size_t)(k + 1) * (size_t)npix;
     noalloc_reset_kernel<<<1, 32, 0, s>>>(st);
+    int dev = 0, sms = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || sms <= 0) {
+        set_error(err, err_len, "device query failed: %s", cudaGetErrorString(e));
+        return RVSB_E_CUDA;
+    }
     const int threads = 256;
-    const int blocks = (int)std::min<long long>((npix + threads - 1) / threads, 148LL * 8);
+    const int blocks = (int)std::min<long long>((npix + threads - 1) / threads, (long long)sms * 8);
     noalloc_prep_kernel<<<blocks, threads, 0, s>>>(holes, width, height, st, codes, sources);
     launch_inpaint_scans(st, holes, codes, scan, width, height, sources, s);
     e = cudaGetLastError();

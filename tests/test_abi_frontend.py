@@ -57,6 +57,17 @@ def test_create_without_device_fails_cleanly():
     assert e.value.status != 0
 
 
+@pytest.mark.parametrize("w,h", [(97, 54), (96, 55), (1, 2), (2, 1), (0, 10), (32770, 2), (-4, 8)])
+def test_noalloc_rejects_sizes_before_device_work(w, h):
+    """Odd sides, sides below 2 and sides above 32768 fail with RVSB_E_ARG
+    before any device call (the pointers are never dereferenced), so this
+    runs without a GPU."""
+    with pytest.raises(rvsb.RvsbError) as e:
+        rvsb.inpaint_sources_noalloc(0x1000, w, h, 0x2000)
+    assert e.value.status == abi.RVSB_E_ARG
+    assert "each side even, 2..32768" in str(e.value)
+
+
 # ---------------------------------------------------------------------------
 # Camera parameters (Parameters.cpp)
 # ---------------------------------------------------------------------------
