@@ -118,36 +118,154 @@ def workload_plain():
     return wl
 
 
-def cpu_baseline_port(wl, n_views=5):
-    """The CPU oracle on `n_views` syntheses of the workload, 1 thread."""
+def reference_cpu():
+    """The reference's own CPU synthesis (oracle/_ref/libref.so, its sources
+    compiled unmodified against an OpenCV stand-in) when it is built, else
+    the oracle's restatement.  Returns (kind, synthesize(wl, target) -> YUV
+    planes, description)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.lib()
+    try:
+        import ref
+        ref.lib()
+    except Exception:
+        ref = None
+    if ref is None:
+        def synth(inputs, planes, target, exponent):
+            return O.synthesize(inputs, planes, target, exponent)
+        return "port", synth, "the oracle's restatement of the reference's CPU path"
+
+    def synth(inputs, planes, target, exponent):
+        # The reference's CPU mode decodes its inputs with CUDA loader kernels
+        # (process_input_frame.cu); here their CPU restatement, which the GPU
+        # tests check bit for bit against those kernels.
+        cols = [O.decode_color(y, u, v, c.bit_depth_color) for c, (y, u, v, d) in zip(inputs, planes)]
+        deps = [O.decode_depth(d, c) for c, (y, u, v, d) in zip(inputs, planes)]
+        color, quality = ref.synthesize(inputs, cols, deps, target, exponent)
+        return ref.write_color(color, target), quality
+    return "reference", synth, ("the reference's own CPU synthesis (rvs/src transform, blending, inpainting, "
+                                "writer and camera code compiled unmodified), inputs decoded by the CPU "
+                                "restatement of its loader kernels")
+
+
+def cpu_baseline(wl, n_views=4):
+    """The reference's CPU path on `n_views` syntheses of the workload, 1
+    thread (its loops are serial)."""
+    kind, synth, desc = reference_cpu()
     t0 = time.perf_counter()
     for _ in range(n_views):
-        O.synthesize(wl.inputs, wl.planes, wl.targets[0], wl.blending_factor)
+        synth(wl.inputs, wl.planes, wl.targets[0], wl.blending_factor)
     dt = time.perf_counter() - t0
-    return {"value": n_views / dt, "unit": UNIT, "cores": 1, "kind": "port",
+    return {"value": n_views / dt, "unit": UNIT, "cores": 1, "kind": kind,
             "sample": f"{n_views} syntheses of the 4x1920x1080 -> 1920x1080 view, 1 thread, "
-                      f"{dt:.1f} s; host has {os.cpu_count()} cores"}
+                      f"{dt:.1f} s; {desc}; host has {os.cpu_count()} cores"}
+
+
+# With an equirectangular camera the reference's hole mask depends on the
+# last bit of its C runtime's float trigonometry (std::cos/sin/atan2/asin);
+# the CUDA path evaluates those correctly rounded.  There the mask must equal
+# the oracle's (correctly rounded) exactly and the reference's to within this
+# fraction of the pixels.
+ERP_MASK_TOLERANCE = 1e-5
+
+
+def parity_of(gpu_yuv, gpu_hole, ref_yuv, ref_quality, debug_matches=None, oracle_quality=None):
+    """The parity bar of one output: PSNR per plane against the reference's
+    output (10-bit peak), the fraction of samples more than 2 codes off, and
+    whether the hole mask (!(quality > 0) before inpainting) is identical."""
+    import numpy as np
+    out = {}
+    big = total = 0
+    for name, g, c in zip("YUV", gpu_yuv, ref_yuv):
+        d = g.astype(np.float64) - c.astype(np.float64)
+        mse = float(np.mean(d * d))
+        out["psnr_" + name] = float("inf") if mse == 0 else float(10 * np.log10(1023.0 ** 2 / mse))
+        big += int((np.abs(d) > 2).sum())
+        total += d.size
+    out["frac_gt2"] = big / total
+    ref_hole = ~(ref_quality > 0)
+    out["mask_identical"] = bool(np.array_equal(gpu_hole, ref_hole))
+    out["mask_pixels_differing"] = int((gpu_hole != ref_hole).sum())
+    mask_ok = out["mask_identical"]
+    if oracle_quality is not None:
+        out["mask_identical_to_correctly_rounded_trig"] = bool(np.array_equal(gpu_hole, ~(oracle_quality > 0)))
+        mask_ok = (out["mask_identical_to_correctly_rounded_trig"] and
+                   out["mask_pixels_differing"] <= ERP_MASK_TOLERANCE * gpu_hole.size)
+    if debug_matches is not None:
+        out["debug_call_matches_timed_output"] = bool(debug_matches)
+    out["ok"] = bool(min(out["psnr_Y"], out["psnr_U"], out["psnr_V"]) >= 50.0 and out["frac_gt2"] <= 0.005
+                     and mask_ok and debug_matches is not False)
+    return out
+
+
+class ParityJobs:
+    """Outputs of the timed calls kept for the parity check, with the hole
+    mask of the same target from rvsb_synthesize_debug on the same scene
+    (whose YUV must equal the timed output's)."""
+
+    def __init__(self):
+        self.jobs = []
+
+    def add(self, name, scene, inputs, planes, target, p, gpu_planes):
+        import numpy as np
+        import torch
+        wo, ho = target.width, target.height
+        timed = tuple(t.cpu().numpy().view(np.uint16).copy() for t in gpu_planes)
+        dout = [torch.empty(n, dtype=torch.int16, device="cuda")
+                for n in (wo * ho, (wo // 2) * (ho // 2), (wo // 2) * (ho // 2))]
+        dbg = {"blend_quality": torch.full((ho, wo), float("nan"), device="cuda")}
+        scene.synthesize_debug(target, p, dout, dbg)
+        torch.cuda.synchronize()
+        dyuv = tuple(t.cpu().numpy().view(np.uint16) for t in dout)
+        same = all(np.array_equal(a, b) for a, b in zip(dyuv, timed))
+        hole = ~(dbg["blend_quality"].cpu().numpy() > 0)
+        shape = ((ho, wo), (ho // 2, wo // 2), (ho // 2, wo // 2))
+        self.jobs.append((name, list(inputs), list(planes), target, p.blending_factor,
+                          tuple(a.reshape(s) for a, s in zip(timed, shape)), hole, same))
+
+    def run(self):
+        """Computes the reference's output of every job (in parallel over the
+        host cores) and returns {name: parity}."""
+        from concurrent.futures import ThreadPoolExecutor
+        kind, synth, _ = reference_cpu()
+
+        def one(job):
+            name, inputs, planes, target, exponent, yuv, hole, same = job
+            import oracle as O
+            from rvsb import abi
+            t0 = time.perf_counter()
+            oq = None
+            if kind == "reference":
+                ryuv, rq = synth(inputs, planes, target, exponent)
+                if any(c.projection == abi.EQUIRECTANGULAR for c in inputs + [target]):
+                    _, oq, _ = O.synthesize(inputs, planes, target, exponent, want_intermediate=True)
+            else:
+                ryuv, rq, _ = O.synthesize(inputs, planes, target, exponent, want_intermediate=True)
+            r = parity_of(yuv, hole, ryuv, rq, same, oq)
+            r["against"] = kind
+            r["target"] = f"{'ERP' if target.projection else 'perspective'} {target.width}x{target.height}"
+            r["cpu_s"] = round(time.perf_counter() - t0, 2)
+            return name, r
+
+        with ThreadPoolExecutor(max(1, min(len(self.jobs), os.cpu_count() or 1))) as ex:
+            return dict(ex.map(one, self.jobs))
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU synthesis (oracle port) on the
-    host cores, one view per thread per step."""
+    """--impl reference: the reference's CPU synthesis on the host cores,
+    one view per thread per step."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from concurrent.futures import ThreadPoolExecutor
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    O.lib()
+    kind, synth, desc = reference_cpu()
     wl = workload_plain()
     threads = max(1, min(32, os.cpu_count() or 1))
 
     def one(_):
-        O.synthesize(wl.inputs, wl.planes, wl.targets[0], wl.blending_factor)
+        synth(wl.inputs, wl.planes, wl.targets[0], wl.blending_factor)
 
     with ThreadPoolExecutor(threads) as ex:
         for _ in range(args.warmup):
@@ -166,16 +284,14 @@ def run_reference(args):
         "data": "synthetic (seeded scene, RVS file formats)",
         "config": {"workload": "plain_1080p: 4 perspective 1920x1080 inputs -> 1 perspective 1920x1080 view",
                    "step": f"{threads} views synthesised in parallel, one per host thread"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} steps x {threads} views of the 4x1080p workload; the "
-                                   "reference RVS needs OpenCV C++ and does not build here, so its CPU path "
-                                   "runs as the oracle restatement"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{args.steps} steps x {threads} views of the 4x1080p workload; {desc}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
-def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world):
+def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world, jobs=None):
     """Views/s of rvsb_synthesize_batch on the resident scene: `slots` seeded
     poses of the same distribution per batch (one CUDA graph replay), inputs
     resident, L2 flushed between batches outside the timed events."""
@@ -205,6 +321,8 @@ def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world):
     launches = batch.last_launch_count()
     variant = batch.last_raster_variant()
     batch.close()
+    if jobs is not None:
+        jobs.add("batched", scene, wl.inputs, wl.planes, targets[0], p, outs[0])
     from rvsb import replicas
     total = replicas.max_over_ranks(sum(ms) / 1000.0, world)
     return {"value": world * slots * steps / total, "unit": UNIT, "slots": slots, "batches": steps,
@@ -213,7 +331,7 @@ def measure_batched(ctx, scene, wl, slots, steps, flush, stream, world):
             "workload": f"plain_1080p scene, {slots} seeded poses per batch"}
 
 
-def measure_batched_workload(ctx, name, slots, flush, stream, reps=2):
+def measure_batched_workload(ctx, name, slots, flush, stream, reps=2, jobs=None):
     """Views/s of a batched configuration: every target of the workload
     synthesised with rvsb_synthesize_batch in groups of `slots` (one graph
     replay per group), inputs resident; `reps` timed passes over all targets,
@@ -248,6 +366,10 @@ def measure_batched_workload(ctx, name, slots, flush, stream, reps=2):
     n = len(wl.targets)
     variant = batch.last_raster_variant()
     batch.close()
+    if jobs is not None:
+        # the first target and one from the middle of the list (another batch)
+        for k in sorted({0, n // 2}):
+            jobs.add(f"{name}[{k}]", sc, wl.inputs, wl.planes, wl.targets[k], p, outs[k])
     sc.close()
     del outs
     torch.cuda.empty_cache()
@@ -290,7 +412,7 @@ def serving_targets(workloads, n, seed=0x5E7E):
     return out
 
 
-def measure_served(ctx, seconds, rate, lanes, max_batch, p):
+def measure_served(ctx, seconds, rate, lanes, max_batch, p, jobs=None):
     """Open-loop serving: Poisson arrivals at `rate` requests/s for `seconds`
     on the three resident scene sets (2 x 960x540, 4 x 1920x1080, 4 x ERP
     4096x2048 inputs).  Returns views/s and latency percentiles."""
@@ -340,6 +462,14 @@ def measure_served(ctx, seconds, rate, lanes, max_batch, p):
     srv.drain(600000)
     res = srv.poll(n + 16)
     srv.close()
+    if jobs is not None:
+        # the last request of each output class still holds its ring slot
+        last = {}
+        for k, (s, cam, cls) in enumerate(reqs):
+            last[cls] = k
+        for cls, k in sorted(last.items()):
+            s, cam, _ = reqs[k]
+            jobs.add(f"served_{cls}", scs[s], wls[s].inputs, wls[s].planes, cam, p, ring[cls][k % 16])
     for sc in scs:
         sc.close()
     lat = sorted((r[5] - r[3]) * 1000.0 for r in res if r[1] == 0)
@@ -371,6 +501,8 @@ def main():
     ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=2)
     ap.add_argument("--no-batched-configs", action="store_true")
+    # skip the parity check of the timed outputs against the reference's CPU path
+    ap.add_argument("--no-parity", action="store_true")
     # only the per-view lines (value, e2e): for launch lists of the per-view path
     ap.add_argument("--plain-only", action="store_true")
     args = ap.parse_args()
@@ -436,6 +568,9 @@ def main():
     torch.cuda.synchronize()
     barrier(world)
     step_ms = [a.elapsed_time(b) for a, b in ev]
+    jobs = ParityJobs() if rank == 0 and not args.no_parity else None
+    if jobs is not None:
+        jobs.add("plain", scene, wl.inputs, wl.planes, target, p, out)
     total_s = sum(step_ms) / 1000.0
     max_total = allreduce_max(total_s, world)
     value = world * args.steps / max_total
@@ -507,16 +642,17 @@ def main():
     e2e_value = world * args.e2e_steps / pipe_s
     batched = None
     if not args.plain_only:
-        batched = measure_batched(ctx, scene, wl, args.batch_slots, args.batch_steps, flush, stream, world)
+        batched = measure_batched(ctx, scene, wl, args.batch_slots, args.batch_steps, flush, stream, world, jobs)
     batched_configs = None
     if not args.no_batched_configs:
         batched_configs = {
-            "batched_erp": measure_batched_workload(ctx, "batched_erp", 32, flush, stream),
-            "batched_mixed": measure_batched_workload(ctx, "batched_mixed", 64, flush, stream),
+            "batched_erp": measure_batched_workload(ctx, "batched_erp", 32, flush, stream, jobs=jobs),
+            "batched_mixed": measure_batched_workload(ctx, "batched_mixed", 64, flush, stream, jobs=jobs),
         }
     served = None
     if args.serve_seconds > 0:
-        served = measure_served(ctx, args.serve_seconds, args.serve_rate, args.serve_lanes, args.serve_batch, p)
+        served = measure_served(ctx, args.serve_seconds, args.serve_rate, args.serve_lanes, args.serve_batch, p,
+                                jobs)
     clocks = sampler.stop()
 
     # Roofline of the dominant kernel (per launch, averaged over the timed steps).
@@ -562,7 +698,16 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_port(wl)
+        cpu = cpu_baseline(wl)
+    parity = None
+    if jobs is not None:
+        parity = jobs.run()
+        parity = {"all_ok": all(v["ok"] for v in parity.values()), "outputs": parity,
+                  "bar": "Y/U/V PSNR >= 50 dB and <= 0.5% of samples more than 2 codes off against the "
+                         "reference's CPU output, identical hole mask (with an equirectangular camera: identical "
+                         "to the correctly rounded trigonometry's and within 1e-5 of the pixels of the "
+                         "reference's libm result); the mask from rvsb_synthesize_debug of the same target, "
+                         "whose YUV must equal the timed output's"}
 
     if rank == 0:
         line = {
@@ -588,6 +733,7 @@ def main():
             "batched_configs": batched_configs,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clocks,
             "gpu_launches": launches_per_step * args.steps,
         }

@@ -10,7 +10,8 @@ import pytest
 import oracle as O
 import rvsb
 from rvsb import abi, scenes
-from helpers import assert_parity, to_u16, yuv_planes_torch
+from helpers import (assert_mask_against_reference, assert_parity, gpu_hole_mask, parallel_map,
+                     reference_and_oracle, to_u16, yuv_planes_torch)
 
 pytestmark = pytest.mark.gpu
 
@@ -168,12 +169,17 @@ def test_default_raster_variant_follows_magnification(ctx):
     b.close()
 
 
-@pytest.mark.parametrize("name,n,picks", [("batched_erp", 8, (0, 5)), ("batched_mixed", 6, (0, 1))])
+@pytest.mark.parametrize("name,n,picks", [("batched_erp", 32, (0, 4, 9, 13, 18, 22, 27, 31)),
+                                          ("batched_mixed", 64, (0, 1, 2, 9, 20, 33, 47, 63))])
 def test_batched_configuration_full_size(ctx, name, n, picks):
-    """The batched configurations at full size through the tuned batch call:
-    4 ERP 4096x2048 inputs seen by 1920x1080 views (magnified: the tuner
-    takes the medium-triangle variant) and 11 perspective 2048x1088 inputs
-    seen by views of mixed sizes.  Two targets of each against the oracle."""
+    """The batched configurations at full size through the tuned batch call,
+    one launch group of the configuration's size: 4 ERP 4096x2048 inputs
+    seen by 32 1920x1080 views (magnified: the tuner takes the
+    medium-triangle variant) and 11 perspective 2048x1088 inputs seen by 64
+    views of mixed sizes.  Eight targets of each against the reference's CPU
+    output: the parity bar and the hole mask (from the debug call on the
+    same scene, whose output equals the batch slot's) as
+    assert_mask_against_reference states."""
     import torch
     wl = getattr(scenes, name)(n_targets=n)
     sc = _upload(ctx, wl)
@@ -184,10 +190,56 @@ def test_batched_configuration_full_size(ctx, name, n, picks):
     b.synthesize(wl.targets, p, outs)
     torch.cuda.synchronize()
     print(name, "raster variant", b.last_raster_variant())
+    gpu = {}
     for k in picks:
         c = wl.targets[k]
-        print(assert_parity(_yuv(outs[k], c), O.synthesize(wl.inputs, wl.planes, c, wl.blending_factor)))
+        hole, dyuv = gpu_hole_mask(sc, c, p)
+        got = _yuv(outs[k], c)
+        for x, y in zip(got, dyuv):
+            np.testing.assert_array_equal(x, y)
+        gpu[k] = (got, hole)
     b.close()
+    sc.close()
+    refs = parallel_map(lambda k: reference_and_oracle(wl.inputs, wl.planes, wl.targets[k], wl.blending_factor),
+                        list(picks))
+    sizes = set()
+    for k, (ryuv, rq, oq) in zip(picks, refs):
+        got, hole = gpu[k]
+        diff = assert_mask_against_reference(hole, rq, oq)
+        print(k, wl.targets[k].width, "mask pixels off the reference's", diff, assert_parity(got, ryuv))
+        sizes.add((wl.targets[k].width, wl.targets[k].height))
+    if name == "batched_mixed":
+        assert len(sizes) == 3
+
+
+@pytest.mark.parametrize("scene_name", ["plain_1080p", "batched_erp"])
+def test_erp_output_full_size(ctx, scene_name):
+    """The serving mix's largest output class, an equirectangular 4096x2048
+    view, at full size from the 4 x 1920x1080 scene and from the 4 x ERP
+    4096x2048 room: per-view call and a batch slot against the reference's
+    CPU output (parity bar; hole mask as assert_mask_against_reference
+    states)."""
+    import torch
+    wl = getattr(scenes, scene_name)()
+    base = wl.targets[0]
+    cam = abi.make_camera(abi.EQUIRECTANGULAR, 4096, 2048, tuple(base.position),
+                          (base.rotation[0] + 20.0, 0.0, 0.0), tuple(base.depth_range))
+    sc = _upload(ctx, wl)
+    p = rvsb.params(wl.blending_factor)
+    single = _single(sc, cam, p)
+    hole, dyuv = gpu_hole_mask(sc, cam, p)
+    b = rvsb.Batch(sc, 2)
+    outs = [yuv_planes_torch(c.width, c.height) for c in (cam, base)]
+    b.synthesize([cam, base], p, outs)
+    torch.cuda.synchronize()
+    for x, y, z in zip(single, dyuv, _yuv(outs[0], cam)):
+        np.testing.assert_array_equal(x, y)
+        np.testing.assert_array_equal(x, z)
+    b.close()
+    sc.close()
+    ryuv, rq, oq = reference_and_oracle(wl.inputs, wl.planes, cam, wl.blending_factor)
+    diff = assert_mask_against_reference(hole, rq, oq)
+    print("mask pixels off the reference's", diff, assert_parity(single, ryuv))
 
 
 def test_batch_slot_seeing_nothing(ctx):
