@@ -486,6 +486,94 @@ def measure_served(ctx, seconds, rate, lanes, max_batch, p, jobs=None):
             "duration_note": f"{seconds:g} s of arrivals (the serving configuration names 60 s)"}
 
 
+def measure_served_load(ctx, seconds, inflight, lanes, max_batch, p):
+    """Closed-loop serving at a fixed load: `inflight` requests of the
+    serving mix are kept outstanding (a new one is submitted as each
+    completes) for `seconds`; views/s is the capacity at that load, with its
+    latency percentiles and the mean batch the server formed."""
+    import numpy as np
+    import torch
+    import rvsb
+    from rvsb import scenes
+    wls = [scenes.plain_small(), scenes.plain_1080p(n_targets=8), scenes.batched_erp(n_targets=64)]
+    scs = []
+    for wl in wls:
+        scenes.cache_planes(wl, CACHE)
+        sc = rvsb.Scene(ctx, wl.inputs)
+        for i, planes in enumerate(wl.planes):
+            sc.upload(i, [np.ascontiguousarray(a, np.uint16) for a in planes], on_device=False)
+        scs.append(sc)
+    srv = rvsb.Server(ctx, lanes=lanes, max_batch=max_batch)
+    ids = [srv.add_scene(sc) for sc in scs]
+    for sid in ids:
+        srv.reserve(sid, 1920, 1080)
+        srv.reserve(sid, 4096, 2048)
+    reqs = serving_targets(wls, 200000, seed=0x10AD)
+    # one output buffer per request in flight (a request's buffer is reused
+    # only after it completed)
+    sizes = {"960x540": (960, 540), "1920x1080": (1920, 1080), "erp4096x2048": (4096, 2048)}
+    free = {cls: [[torch.empty(k, dtype=torch.int16, device="cuda") for k in (w * h, w * h // 4, w * h // 4)]
+                  for _ in range(inflight)] for cls, (w, h) in sizes.items()}
+    held = {}
+    nxt = 0
+
+    def submit():
+        nonlocal nxt
+        s, cam, cls = reqs[nxt % len(reqs)]
+        nxt += 1
+        buf = free[cls].pop()
+        rid = srv.submit(ids[s], cam, p, buf)
+        held[rid] = (cls, buf)
+
+    def retire(results):
+        for r in results:
+            cls, buf = held.pop(r[0])
+            free[cls].append(buf)
+
+    # warm-up at the same load
+    for _ in range(inflight):
+        submit()
+    t_end = time.perf_counter() + 1.0
+    while time.perf_counter() < t_end:
+        res = srv.poll(4096)
+        retire(res)
+        for _ in res:
+            submit()
+        if not res:
+            time.sleep(2e-5)
+    srv.drain(600000)
+    retire(srv.poll(1 << 16))
+    torch.cuda.synchronize()
+    for _ in range(inflight):
+        submit()
+    done = []
+    t_end = time.perf_counter() + seconds
+    while time.perf_counter() < t_end:
+        res = srv.poll(4096)
+        retire(res)
+        done.extend(res)
+        for _ in res:
+            submit()
+        if not res:
+            time.sleep(2e-5)
+    srv.drain(600000)
+    tail = srv.poll(1 << 16)
+    retire(tail)
+    done.extend(tail)
+    srv.close()
+    for sc in scs:
+        sc.close()
+    ok = [r for r in done if r[1] == 0]
+    lat = sorted((r[5] - r[3]) * 1000.0 for r in ok)
+    t0 = min(r[3] for r in done)
+    t1 = max(r[5] for r in done)
+    return {"value": len(ok) / (t1 - t0), "unit": UNIT, "requests": len(done),
+            "failed": len(done) - len(ok), "in_flight": inflight, "lanes": lanes, "max_batch": max_batch,
+            "seconds": seconds, "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
+            "max_ms": lat[-1] if lat else None, "mean_batch": statistics.mean(r[2] for r in done),
+            "mix": "the serving mix (scene sets and output classes as in 'served'), closed loop"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)

@@ -64,7 +64,7 @@ def _load_in_fresh_process(tmp_path, jobs):
     return [(z[f"c{k}"], z[f"d{k}"]) for k in range(len(jobs))]
 
 
-def _write_view(tmp_path, name, planes, frames, depth_format):
+def _write_view(tmp_path, name, planes, frames, depth_format, color_max=1023):
     """Colour (YUV420) and depth (YUV420 with neutral chroma, or YUV400)
     files holding `frames` frames; frame k's luma is shifted by 5k codes."""
     y, u, v, d = planes
@@ -72,7 +72,7 @@ def _write_view(tmp_path, name, planes, frames, depth_format):
     dpath = tmp_path / f"{name}_depth.yuv"
     with open(cpath, "wb") as f:
         for k in range(frames):
-            f.write(np.clip(y.astype(np.int32) + 5 * k, 0, 1023).astype("<u2").tobytes())
+            f.write(np.clip(y.astype(np.int32) + 5 * k, 0, color_max).astype("<u2").tobytes())
             f.write(u.astype("<u2").tobytes())
             f.write(v.astype("<u2").tobytes())
     with open(dpath, "wb") as f:
@@ -127,7 +127,7 @@ def test_loader_scale_fixed_by_first_call(tmp_path):
     yb, ub, vb = (x.astype(np.uint16) * 4 for x in (yb, ub, vb))
     db = (db >> 4).astype(np.uint16)
     pa = _write_view(tmp_path, "a", (ya, ua, va, da), 1, abi.YUV420)
-    pb = _write_view(tmp_path, "b", (yb, ub, vb, db), 1, abi.YUV420)
+    pb = _write_view(tmp_path, "b", (yb, ub, vb, db), 1, abi.YUV420, color_max=4095)
     (ca, _), (cb, dbr) = _load_in_fresh_process(tmp_path, [(a, *pa, 0), (b, *pb, 0)])
     np.testing.assert_array_equal(ca, O.decode_color(ya, ua, va, 10))
     # the reference: b's samples scaled by a's 10-bit colour level ...
