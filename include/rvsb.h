@@ -490,7 +490,8 @@ const char* rvsb_stage_name(int stage);
  * It is for callers that must not allocate device memory while running;
  * its scratch is one static device array of 20 MiB, so images are limited
  * to 524,288 pixels (e.g. 960x540) and larger ones fail with RVSB_E_ARG and
- * a message in `err`.  The first call on each device (with it current) does
+ * a message in `err`; so do sides that are odd or outside 2..32768 (the
+ * fill works on 2x2 blocks).  The first call on each device (with it current) does
  * a one-time set-up and should precede any stream capture.  Calls on one
  * device share the scratch: calls that overlap in time race, so order them
  * (for example on one stream).  Work is issued on `stream`. */
