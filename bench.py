@@ -15,6 +15,15 @@ reference's per-frame InputView::load) and synthesising.
          step, consecutive frames overlapped; the blocking one-frame call
          rvsb_synthesize_host is reported beside it.
   roofline  of the dominant kernel, with its algorithmic bytes per launch.
+  batched / batched_configs  rvsb_synthesize_batch on the plain scene and on
+         the two batched configurations (CUDA graphs, autotuned raster).
+  served  the serving configuration: Poisson arrivals at 500 req/s for 60 s
+         over three resident scene sets (arrival-limited); served_load the
+         same mix closed-loop with a fixed number of requests in flight
+         (capacity, latency and mean batch at that load).
+  parity  every timed output (plain, a batch slot, two targets of each
+         batched configuration, one served request per output class)
+         against the reference's own CPU synthesis of the same target.
   cpu_baseline  the CPU oracle (a restatement of the reference's CPU path)
          on a bounded sample, 1 thread (the reference's loops are serial).
 
@@ -483,7 +492,8 @@ def measure_served(ctx, seconds, rate, lanes, max_batch, p, jobs=None):
             "mean_batch": statistics.mean(r[2] for r in res),
             "mix": "scene sets 2x960x540 / 4x1920x1080 / 4xERP4096x2048 uniform; outputs 960x540 : 1920x1080 : "
                    "ERP 4096x2048 = 5:4:1; Poisson arrivals; 60 GB budget",
-            "duration_note": f"{seconds:g} s of arrivals (the serving configuration names 60 s)"}
+            "duration_note": f"{seconds:g} s of arrivals (the serving configuration names 60 s)",
+            "note": "open loop at the configured rate: arrival-limited, not a capacity figure (served_load is)"}
 
 
 def measure_served_load(ctx, seconds, inflight, lanes, max_batch, p):
@@ -584,10 +594,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-slots", type=int, default=16)
     ap.add_argument("--batch-steps", type=int, default=8)
-    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-rate", type=float, default=500.0)
     ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=2)
+    # closed-loop capacity of the serving path at a fixed number of requests in flight
+    ap.add_argument("--load-seconds", type=float, default=10.0)
+    ap.add_argument("--load-in-flight", type=int, default=6)
+    ap.add_argument("--load-lanes", type=int, default=2)
+    ap.add_argument("--load-batch", type=int, default=4)
     ap.add_argument("--no-batched-configs", action="store_true")
     # skip the parity check of the timed outputs against the reference's CPU path
     ap.add_argument("--no-parity", action="store_true")
@@ -597,6 +612,7 @@ def main():
     if args.plain_only:
         args.no_batched_configs = True
         args.serve_seconds = 0.0
+        args.load_seconds = 0.0
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
@@ -741,6 +757,10 @@ def main():
     if args.serve_seconds > 0:
         served = measure_served(ctx, args.serve_seconds, args.serve_rate, args.serve_lanes, args.serve_batch, p,
                                 jobs)
+    served_load = None
+    if args.load_seconds > 0:
+        served_load = measure_served_load(ctx, args.load_seconds, args.load_in_flight, args.load_lanes,
+                                          args.load_batch, p)
     clocks = sampler.stop()
 
     # Roofline of the dominant kernel (per launch, averaged over the timed steps).
@@ -818,6 +838,7 @@ def main():
                                       "call": "rvsb_synthesize_host (one frame at a time)"}},
             "batched": batched,
             "served": served,
+            "served_load": served_load,
             "batched_configs": batched_configs,
             "roofline": roofline,
             "cpu_baseline": cpu,

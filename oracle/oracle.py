@@ -42,6 +42,8 @@ def lib():
         L.orc_set_multispectral.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float]
         L.orc_set_precision.argtypes = [ctypes.c_float]
         L.orc_resize_linear3.argtypes = [_F, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, ctypes.c_int]
+        L.orc_resize_nearest_u8.argtypes = [ctypes.POINTER(ctypes.c_uint8), ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_uint8), ctypes.c_int, ctypes.c_int]
         L.orc_decode_color.argtypes = [_U16, _U16, _U16, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F]
         L.orc_decode_depth.argtypes = [_U16, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                        ctypes.c_float, ctypes.c_int, _F]
@@ -105,6 +107,16 @@ def resize_linear3(img, w, h):
     src = np.ascontiguousarray(img, np.float32)
     dst = np.empty((h, w, 3), np.float32)
     lib().orc_resize_linear3(_p(src, _F), src.shape[1], src.shape[0], _p(dst, _F), w, h)
+    return dst
+
+
+def resize_nearest_u8(img, w, h):
+    """cv::resize(img, (w, h), INTER_NEAREST) of an HxW uint8 image (the
+    validity mask at Precision != 1, Pipeline.cpp:303-308)."""
+    src = np.ascontiguousarray(img, np.uint8)
+    dst = np.empty((h, w), np.uint8)
+    U8 = ctypes.POINTER(ctypes.c_uint8)
+    lib().orc_resize_nearest_u8(src.ctypes.data_as(U8), src.shape[1], src.shape[0], dst.ctypes.data_as(U8), w, h)
     return dst
 
 
@@ -243,9 +255,10 @@ def synthesize(inputs, planes, virt, exponent, want_intermediate=False):
     return yuv
 
 
-def synthesize_aux(inputs, planes, virt, exponent, threshold=5000.0):
+def synthesize_aux(inputs, planes, virt, exponent, threshold=5000.0, masked=True):
     """Synthesis with the auxiliary outputs of Pipeline.cpp:303-336.  Returns
-    a dict: yuv, mask (uint8), masked_yuv, depth and masked_depth (uint16)."""
+    a dict: yuv, mask (uint8), masked_yuv (masked=True only), depth and
+    masked_depth (uint16), all at the virtual camera's size."""
     n = len(inputs)
     cams = (abi.Camera * n)(*inputs)
     keep = []
@@ -256,16 +269,18 @@ def synthesize_aux(inputs, planes, virt, exponent, threshold=5000.0):
         vp[i].y, vp[i].u, vp[i].v, vp[i].depth = (a.ctypes.data for a in arrs)
     wo, ho = virt.width, virt.height
     out = np.empty(wo * ho * 3 // 2, np.uint16)
-    masked = np.empty(wo * ho * 3 // 2, np.uint16)
+    masked_out = np.empty(wo * ho * 3 // 2, np.uint16)
     mask = np.empty((ho, wo), np.uint8)
     depth = np.empty((ho, wo), np.uint16)
     mdepth = np.empty((ho, wo), np.uint16)
     rc = lib().orc_synthesize_aux(n, cams, vp, ctypes.byref(virt), float(exponent), _p(out, _U16), None, None,
                                   float(threshold), mask.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
-                                  _p(masked, _U16), _p(depth, _U16), _p(mdepth, _U16))
+                                  _p(masked_out, _U16) if masked else None, _p(depth, _U16), _p(mdepth, _U16))
     assert rc == 0, rc
-    return {"yuv": split_yuv420(out, wo, ho), "mask": mask, "masked_yuv": split_yuv420(masked, wo, ho),
-            "depth": depth, "masked_depth": mdepth}
+    r = {"yuv": split_yuv420(out, wo, ho), "mask": mask, "depth": depth, "masked_depth": mdepth}
+    if masked:
+        r["masked_yuv"] = split_yuv420(masked_out, wo, ho)
+    return r
 
 
 def image_pos(cam):

@@ -74,6 +74,7 @@ def lib():
         L.ref_synthesize.argtypes = [ctypes.c_int, ctypes.POINTER(c_p), PF, PF, c_p, ctypes.c_float, ctypes.c_int,
                                      ctypes.c_float, ctypes.c_float, _F, _F]
         L.ref_load_view.argtypes = [c_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, _F, _F]
+        L.ref_write_aux.argtypes = [ctypes.c_int, _F, _U8, ctypes.c_int, ctypes.c_int, c_p, ctypes.c_char_p]
         _lib = L
     return _lib
 
@@ -87,9 +88,11 @@ def _p(a, t=_F):
     return a.ctypes.data_as(t)
 
 
-def camera_dict(c, name="cam"):
+def camera_dict(c, name="cam", crop=None, padded=None):
     """The camera-parameter JSON object of an rvsb camera (the keys of
-    Parameters.cpp)."""
+    Parameters.cpp).  crop=(x, y, w, h) with padded=(W, H): the camera is
+    the region of a W x H camera (Crop_region; c holds the region's size
+    and its principal point relative to the region)."""
     d = {"Name": name, "Projection": "Equirectangular" if c.projection == abi.EQUIRECTANGULAR else "Perspective",
          "Position": [float(x) for x in c.position], "Rotation": [float(x) for x in c.rotation],
          "Depthmap": 1, "Background": 0, "Depth_range": [float(x) for x in c.depth_range],
@@ -103,15 +106,20 @@ def camera_dict(c, name="cam"):
     else:
         d["Focal"] = [float(x) for x in c.focal]
         d["Principle_point"] = [float(x) for x in c.principle_point]
+    if crop is not None:
+        d["Resolution"] = [int(padded[0]), int(padded[1])]
+        d["Crop_region"] = [int(v) for v in crop]
+        if "Principle_point" in d:
+            d["Principle_point"] = [float(c.principle_point[0]) + crop[0], float(c.principle_point[1]) + crop[1]]
     return d
 
 
 class Camera:
     """A reference Parameters object parsed from an rvsb camera."""
 
-    def __init__(self, cam):
+    def __init__(self, cam, crop=None, padded=None):
         self.cam = cam
-        self.h = lib().ref_camera_new(json.dumps(camera_dict(cam)).encode())
+        self.h = lib().ref_camera_new(json.dumps(camera_dict(cam, crop=crop, padded=padded)).encode())
         if not self.h:
             _check(1)
 
@@ -246,3 +254,23 @@ def load_view(cam, color_path, depth_path, frame):
     depth = np.empty((cam.height, cam.width), np.float32)
     _check(lib().ref_load_view(c.h, color_path.encode(), depth_path.encode(), int(frame), _p(color), _p(depth)))
     return color, depth
+
+
+def write_aux(kind, depth, mask, virt, crop=None, padded=None):
+    """The reference's depth and mask writers (image_writing.cpp:226-302):
+    kind "depth" (write_depth), "masked_depth" (write_maskedDepth) or "mask"
+    (write_mask) of an output-sized float depth / uint8 mask (nonzero =
+    masked) for the virtual camera.  Returns the written file's samples:
+    luma plane (uint16, or uint8 for the mask) of the padded size."""
+    k = {"depth": 0, "masked_depth": 1, "mask": 2}[kind]
+    c = Camera(virt, crop, padded)
+    h, w = (mask if depth is None else depth).shape
+    dp = np.ascontiguousarray(depth, np.float32) if depth is not None else None
+    mp = np.ascontiguousarray(mask, np.uint8) if mask is not None else None
+    W, H = padded if padded is not None else (w, h)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "aux.yuv")
+        _check(lib().ref_write_aux(k, _p(dp) if dp is not None else None, _p(mp, _U8) if mp is not None else None,
+                                   w, h, c.h, path.encode()))
+        raw = np.fromfile(path, np.uint8 if kind == "mask" else np.uint16)
+    return raw[:W * H].reshape(H, W)

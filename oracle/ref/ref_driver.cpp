@@ -252,6 +252,27 @@ int ref_write_color(const float* color, int w, int h, void* virt, const char* pa
     });
 }
 
+// write_depth / write_maskedDepth / write_mask (image_writing.cpp:226-302)
+// of an output-sized depth map (and mask, nonzero = masked) to `path` for
+// the virtual camera `virt`, frame 0.  kind: 0 depth, 1 masked depth, 2 mask.
+int ref_write_aux(int kind, const float* depth, const unsigned char* mask, int w, int h, void* virt,
+                  const char* path) {
+    return guarded([&] {
+        const rvs::Parameters& p = static_cast<Cam*>(virt)->params;
+        cv::Mat1b m;
+        if (mask) {
+            m = cv::Mat1b(h, w);
+            std::memcpy(m.data, mask, (size_t)w * h);
+        }
+        if (kind == 0)
+            rvs::write_depth(path, cv::Mat1f(wrap(depth, w, h, 1)), 0, p);
+        else if (kind == 1)
+            rvs::write_maskedDepth(path, cv::Mat1f(wrap(depth, w, h, 1)), m, 0, p);
+        else
+            rvs::write_mask(path, m, 0, p);
+    });
+}
+
 // One synthesized frame: every input view warped, rasterised and blended in
 // order, then inpainted (Pipeline.cpp:169-262 without the loaders and the
 // file writer).  colors: decoded input colour per view (H*W*3), depths:

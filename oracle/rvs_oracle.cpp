@@ -799,7 +799,7 @@ static void blur_channel0(const float* src, const uint8_t* mask, int w, int h, i
  * source coordinate (d + 0.5) * scale - 0.5, weights (1 - f, f) in float,
  * coordinates clamped to the first and last pixel (weight 0 beyond), a
  * horizontal pass per source row and a vertical pass. */
-static void resize_linear3(const float* src, int ws, int hs, float* dst, int wd, int hd) {
+static void resize_linear(const float* src, int ws, int hs, int cn, float* dst, int wd, int hd) {
     const double scale_x = 1.0 / ((double)wd / ws), scale_y = 1.0 / ((double)hd / hs);
     const int iscale_x = (int)std::lrint(scale_x), iscale_y = (int)std::lrint(scale_y);
     const bool area_fast = std::fabs(scale_x - iscale_x) < 2.220446049250313e-16 &&
@@ -807,12 +807,12 @@ static void resize_linear3(const float* src, int ws, int hs, float* dst, int wd,
     if (area_fast && iscale_x == 2 && iscale_y == 2) {
         for (int y = 0; y < hd; ++y)
             for (int x = 0; x < wd; ++x)
-                for (int k = 0; k < 3; ++k) {
-                    const float a = src[((size_t)(2 * y) * ws + 2 * x) * 3 + k];
-                    const float b = src[((size_t)(2 * y) * ws + 2 * x + 1) * 3 + k];
-                    const float c = src[((size_t)(2 * y + 1) * ws + 2 * x) * 3 + k];
-                    const float d = src[((size_t)(2 * y + 1) * ws + 2 * x + 1) * 3 + k];
-                    dst[((size_t)y * wd + x) * 3 + k] = (((a + b) + c) + d) * 0.25f;
+                for (int k = 0; k < cn; ++k) {
+                    const float a = src[((size_t)(2 * y) * ws + 2 * x) * cn + k];
+                    const float b = src[((size_t)(2 * y) * ws + 2 * x + 1) * cn + k];
+                    const float c = src[((size_t)(2 * y + 1) * ws + 2 * x) * cn + k];
+                    const float d = src[((size_t)(2 * y + 1) * ws + 2 * x + 1) * cn + k];
+                    dst[((size_t)y * wd + x) * cn + k] = (((a + b) + c) + d) * 0.25f;
                 }
         return;
     }
@@ -830,7 +830,7 @@ static void resize_linear3(const float* src, int ws, int hs, float* dst, int wd,
         }
         s0 = s;
     };
-    std::vector<float> rows((size_t)hs * wd * 3);
+    std::vector<float> rows((size_t)hs * wd * cn);
     for (int x = 0; x < wd; ++x) {
         int sx;
         float fx;
@@ -838,9 +838,9 @@ static void resize_linear3(const float* src, int ws, int hs, float* dst, int wd,
         const float a0 = 1.f - fx, a1 = fx;
         const int sx1 = std::min(sx + 1, ws - 1);
         for (int y = 0; y < hs; ++y)
-            for (int k = 0; k < 3; ++k)
-                rows[((size_t)y * wd + x) * 3 + k] =
-                    src[((size_t)y * ws + sx) * 3 + k] * a0 + src[((size_t)y * ws + sx1) * 3 + k] * a1;
+            for (int k = 0; k < cn; ++k)
+                rows[((size_t)y * wd + x) * cn + k] =
+                    src[((size_t)y * ws + sx) * cn + k] * a0 + src[((size_t)y * ws + sx1) * cn + k] * a1;
     }
     for (int y = 0; y < hd; ++y) {
         int sy;
@@ -849,10 +849,33 @@ static void resize_linear3(const float* src, int ws, int hs, float* dst, int wd,
         const float b0 = 1.f - fy, b1 = fy;
         const int sy1 = std::min(sy + 1, hs - 1);
         for (int x = 0; x < wd; ++x)
-            for (int k = 0; k < 3; ++k)
-                dst[((size_t)y * wd + x) * 3 + k] =
-                    rows[((size_t)sy * wd + x) * 3 + k] * b0 + rows[((size_t)sy1 * wd + x) * 3 + k] * b1;
+            for (int k = 0; k < cn; ++k)
+                dst[((size_t)y * wd + x) * cn + k] =
+                    rows[((size_t)sy * wd + x) * cn + k] * b0 + rows[((size_t)sy1 * wd + x) * cn + k] * b1;
     }
+}
+
+static void resize_linear3(const float* src, int ws, int hs, float* dst, int wd, int hd) {
+    resize_linear(src, ws, hs, 3, dst, wd, hd);
+}
+
+/* cv::resize(src, dst, dsize, 0, 0, INTER_NEAREST) of a one-byte image
+ * (imgproc resize.cpp resizeNN): destination x reads source
+ * min(floor(x * (1 / (wd / ws))), ws - 1), the ratio and product in double;
+ * the same for y.  Pinned against cv2 by tests/golden. */
+static void resize_nearest_u8(const uint8_t* src, int ws, int hs, uint8_t* dst, int wd, int hd) {
+    const double ifx = 1.0 / ((double)wd / ws), ify = 1.0 / ((double)hd / hs);
+    for (int y = 0; y < hd; ++y) {
+        const int sy = std::min((int)std::floor(y * ify), hs - 1);
+        for (int x = 0; x < wd; ++x) {
+            const int sx = std::min((int)std::floor(x * ifx), ws - 1);
+            dst[(size_t)y * wd + x] = src[(size_t)sy * ws + sx];
+        }
+    }
+}
+
+extern "C" void orc_resize_nearest_u8(const uint8_t* src, int ws, int hs, uint8_t* dst, int wd, int hd) {
+    resize_nearest_u8(src, ws, hs, dst, wd, hd);
 }
 
 extern "C" void orc_resize_linear3(const float* src, int ws, int hs, float* dst, int wd, int hd) {
@@ -918,7 +941,10 @@ int orc_synthesize_aux(int n, const rvsb_camera* cams, const rvsb_view_planes* p
     // written (image_writing.cpp:188-190).
     const float P = g_precision;
     const bool rescale = P != 1.f;
-    if (rescale && (out_mask || out_masked_yuv || out_depth || out_masked_depth)) return RVSB_E_UNSUPPORTED;
+    // MaskedOutputFiles at Precision != 1: the reference sets the raster-sized
+    // colour with the mask resized to the output size (Pipeline.cpp:314-318),
+    // which OpenCV's setTo rejects (the sizes differ).
+    if (rescale && out_masked_yuv) return RVSB_E_UNSUPPORTED;
     const int wo = rescale ? (int)(0.5f + vt->width * P) : vt->width;
     const int ho = rescale ? (int)(0.5f + vt->height * P) : vt->height;
     const float sxu = (float)wo / vt->width, syv = (float)ho / vt->height;
@@ -1002,7 +1028,24 @@ int orc_synthesize_aux(int n, const rvsb_camera* cams, const rvsb_view_planes* p
     if (rescale) {
         std::vector<float> small((size_t)vt->width * vt->height * 3);
         resize_linear3(filled.data(), wo, ho, small.data(), vt->width, vt->height);
-        return orc_write_yuv420(small.data(), vt->width, vt->height, vt->bit_depth_color, out_yuv);
+        int rc = orc_write_yuv420(small.data(), vt->width, vt->height, vt->bit_depth_color, out_yuv);
+        if (rc || !want_aux) return rc;
+        // Pipeline.cpp:303-336 at Precision != 1: the validity mask resized
+        // with INTER_NEAREST, the blended depth with INTER_LINEAR, both to the
+        // output size before they are written.
+        const int W = vt->width, H = vt->height;
+        const size_t nw = (size_t)W * H;
+        std::vector<uint8_t> rmask(no), mask(nw);
+        for (size_t p = 0; p < no; ++p) rmask[p] = (validity[p] > threshold) ? 0 : 255;
+        resize_nearest_u8(rmask.data(), wo, ho, mask.data(), W, H);
+        std::vector<float> dsmall(nw);
+        resize_linear(depth.data(), wo, ho, 1, dsmall.data(), W, H);
+        if (out_mask) std::memcpy(out_mask, mask.data(), nw);
+        if (out_depth)
+            for (size_t p = 0; p < nw; ++p) out_depth[p] = encode_depth(dsmall[p], vt, false);
+        if (out_masked_depth)
+            for (size_t p = 0; p < nw; ++p) out_masked_depth[p] = encode_depth(dsmall[p], vt, mask[p] != 0);
+        return RVSB_OK;
     }
     int rc = orc_write_yuv420(filled.data(), wo, ho, vt->bit_depth_color, out_yuv);
     if (rc) return rc;

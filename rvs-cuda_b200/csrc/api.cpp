@@ -171,6 +171,7 @@ rvsb_status synthesize_impl(rvsb_scene* sc, const rvsb_camera* virt, const rvsb_
                             const rvsb_view_planes* frame = nullptr, const rvsb_aux_out* aux = nullptr) {
     if (!sc) return RVSB_E_ARG;
     rvsb_context* ctx = sc->ctx;
+    HostRange range("rvsb: synthesize");
     return guarded(ctx, [&]() -> rvsb_status {
         validate_request(sc, virt, params, out);
         if (frame) {
@@ -378,6 +379,7 @@ void rvsb_scene_destroy(rvsb_scene* scene) {
 rvsb_status rvsb_scene_upload(rvsb_scene* sc, int view, const rvsb_view_planes* planes, int planes_on_device,
                               void* stream) {
     if (!sc) return RVSB_E_ARG;
+    HostRange range("rvsb: scene upload");
     return guarded(sc->ctx, [&]() -> rvsb_status {
         if (!planes || view < 0 || view >= (int)sc->cams.size()) throw ArgError("bad view index or planes");
         const void* src[4] = {planes->y, planes->u, planes->v, planes->depth};
@@ -661,6 +663,7 @@ rvsb_status rvsb_host_stream_submit(rvsb_host_stream* hs, const rvsb_view_planes
                                     const rvsb_yuv420* out_host, void* stream, uint64_t* ticket) {
     if (!hs || !host_planes || !virt || !out_host || !ticket) return RVSB_E_ARG;
     rvsb_context* ctx = hs->ctx;
+    HostRange range("rvsb: host frame (upload, synthesis, download)");
     return guarded(ctx, [&]() -> rvsb_status {
         if (!out_host->y || !out_host->u || !out_host->v) throw ArgError("null output planes");
         rvsb_scene* sc = hs->scene;

@@ -317,6 +317,30 @@ __device__ __forceinline__ uint16_t quarter_round(uint32_t s, int ties_up) {
     return (uint16_t)(q + (up & 1u));
 }
 
+// cv::resize with INTER_LINEAR (write_color's resize, image_writing.cpp:190;
+// the depth resize of Pipeline.cpp:323-333): source coordinate of
+// destination index d, (d + 0.5) * scale - 0.5, giving the left (top) tap and
+// the weight of the right (bottom) one, clamped at both borders.
+__device__ __forceinline__ void linear_tap(int d, double scale, int n, int& s0, int& s1, float& f) {
+    f = (float)__dadd_rn(__dmul_rn((double)d + 0.5, scale), -0.5);
+    int s = (int)floorf(f);
+    f = __fsub_rn(f, (float)s);
+    if (s < 0) {
+        f = 0.f;
+        s = 0;
+    }
+    if (s >= n - 1) {
+        f = 0.f;
+        s = n - 1;
+    }
+    s0 = s;
+    s1 = min(s + 1, n - 1);
+}
+
+__device__ __forceinline__ float lerp2(float a, float b, float wa, float wb) {
+    return __fadd_rn(__fmul_rn(a, wa), __fmul_rn(b, wb));
+}
+
 // static_cast<ushort>(v * max_level) (image_writing.cpp:165-172).
 __device__ __forceinline__ uint32_t quantize(float c, unsigned max_val) {
     const uint32_t q = __float2uint_rz(__fmul_rn(c, (float)max_val));

@@ -50,10 +50,10 @@ RasterDims raster_dims(const rvsb_camera& virt, const rvsb_synth_params& p) {
     if (p.precision == 1.f) return {virt.width, virt.height, false};
     const int w = (int)(0.5f + (float)virt.width * p.precision);
     const int h = (int)(0.5f + (float)virt.height * p.precision);
-    if (w < 2 || h < 2 || (w & 1) || (h & 1) || w > 32768 || h > 32768)
+    if (w < 2 || h < 2 || w > 32768 || h > 32768)
         throw Unsupported("Precision " + std::to_string(p.precision) + " gives a raster size of " +
                           std::to_string(w) + "x" + std::to_string(h) +
-                          "; only even sizes of at least 2 and at most 32768 are supported");
+                          "; only sizes of at least 2 and at most 32768 are supported");
     return {w, h, true};
 }
 
@@ -538,13 +538,17 @@ int BatchCore::tune(const SlotRequest* reqs, int n, cudaStream_t s) {
 }
 
 int BatchCore::run(const SlotRequest* reqs, int n, cudaStream_t s) {
+    HostRange range("rvsb: batch (tables, launches)");
     if (n <= 0 || n > slots_) throw ArgError("batch of " + std::to_string(n) + " requests for " +
                                              std::to_string(slots_) + " slots");
     int ms_wo = 0;
     for (int k = 0; k < n; ++k) {
         const SlotRequest& r = reqs[k];
         const RasterDims rd = raster_dims(r.virt, r.params);
-        if (rd.rescale && r.aux) throw Unsupported("auxiliary outputs need Precision 1");
+        if (rd.rescale && r.aux && r.aux->masked.y)
+            throw Unsupported("MaskedOutputFiles needs Precision 1: the reference masks the raster-sized colour "
+                              "with the mask resized to the output size (Pipeline.cpp:314-318), which OpenCV "
+                              "rejects");
         ws_[k]->ensure(ctx_, r.scene, rd.w, rd.h);
         if (r.aux) ws_[k]->ensure_aux(ctx_, rd.w, rd.h);
         if (rd.rescale) ws_[k]->ensure_rescale(ctx_, rd.w, rd.h);

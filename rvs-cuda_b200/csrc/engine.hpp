@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <map>
 #include <memory>
@@ -27,6 +28,16 @@ struct ArgError : std::runtime_error {
 };
 
 void check(cudaError_t e, const char* what);
+
+// An NVTX range over a host stage (header-only NVTX 3: a no-op unless a
+// profiler such as Nsight Systems is attached), so the host side of a
+// synthesis shows beside its kernels on a timeline.
+struct HostRange {
+    explicit HostRange(const char* name) { nvtxRangePushA(name); }
+    ~HostRange() { nvtxRangePop(); }
+    HostRange(const HostRange&) = delete;
+    HostRange& operator=(const HostRange&) = delete;
+};
 
 }  // namespace rvsb
 

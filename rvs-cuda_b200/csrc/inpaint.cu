@@ -600,7 +600,11 @@ __global__ void inpaint_write_kernel(const __grid_constant__ Src src) {
     const int y = 2 * (by0 + (int)blockIdx.y);
     if (x > rg.x1 || y > rg.y1 || x >= wo || y >= ho) return;
     const size_t o = (size_t)y * wo + x;
-    uint64_t c00 = codes[o], c01 = codes[o + 1], c10 = codes[o + wo], c11 = codes[o + wo + 1];
+    // A raster of odd width or height (Precision != 1) ends in partial
+    // blocks: their missing pixels read as non-holes and are not written.
+    const bool has_r = x + 1 < wo, has_b = y + 1 < ho;
+    uint64_t c00 = codes[o], c01 = has_r ? codes[o + 1] : 0ull, c10 = has_b ? codes[o + wo] : 0ull,
+             c11 = has_r && has_b ? codes[o + wo + 1] : 0ull;
     if (!((c00 | c01 | c10 | c11) & kHoleBit)) return;
     auto fill = [&](uint64_t& c, size_t q) {
         if (!(c & kHoleBit)) return;
@@ -615,9 +619,9 @@ __global__ void inpaint_write_kernel(const __grid_constant__ Src src) {
         }
     };
     fill(c00, o);
-    fill(c01, o + 1);
-    fill(c10, o + wo);
-    fill(c11, o + wo + 1);
+    if (has_r) fill(c01, o + 1);
+    if (has_b) fill(c10, o + wo);
+    if (has_r && has_b) fill(c11, o + wo + 1);
     if (im.no_write) return;
     out_y[o] = (uint16_t)(c00 & 0xffff);
     out_y[o + 1] = (uint16_t)(c01 & 0xffff);
@@ -682,7 +686,7 @@ template <class Tabs>
 int launch_inpaint(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
     const FromTables<Tabs> src{tabs};
     const int n = launch_scans(src, sh.max_wo, sh.max_ho, sh.slots, column_groups(sh.max_wo, sh.slots), s);
-    launch_dependent(inpaint_write_kernel<FromTables<Tabs>>, dim3((sh.max_wo / 2 + 127) / 128, (sh.max_ho + 1) / 2, sh.slots),
+    launch_dependent(inpaint_write_kernel<FromTables<Tabs>>, dim3(((sh.max_wo + 1) / 2 + 127) / 128, (sh.max_ho + 1) / 2, sh.slots),
                      dim3(128), 0, s, src);
     return n + 1;
 }

@@ -161,6 +161,9 @@ __global__ void ms_blend_kernel(const __grid_constant__ Tabs tabs) {
     bool any_hole = false;
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
+        code[p] = 0;
+        // partial blocks of a raster of odd width or height (Precision != 1)
+        if (x0 + (p & 1) >= T.wo || y0 + (p >> 1) >= T.ho) continue;
         const size_t o = (size_t)(y0 + (p >> 1)) * T.wo + x0 + (p & 1);
         BlendAcc lo = {0.f, 0.f, 0.f, 0.f}, hi = {0.f, 0.f, 0.f, 0.f};
         for (int v = 0; v < T.n_views; ++v) {
@@ -208,8 +211,8 @@ int launch_ms(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
     const size_t smem = (sizeof(double) + sizeof(int)) * (size_t)(sh.max_wo + 1);
     launch_dependent(ms_rows_kernel<Tabs>, dim3(sh.max_ho, sh.max_views, sh.slots), dim3(MS_THREADS), smem, s, tabs);
     launch_dependent(ms_cols_kernel<Tabs>, dim3((sh.max_wo + 127) / 128, sh.max_views, sh.slots), dim3(128), 0, s, tabs);
-    launch_dependent(ms_blend_kernel<Tabs>, dim3((sh.max_wo / 2 + 127) / 128, sh.max_ho / 2, sh.slots), dim3(128), 0, s,
-                     tabs);
+    launch_dependent(ms_blend_kernel<Tabs>, dim3(((sh.max_wo + 1) / 2 + 127) / 128, (sh.max_ho + 1) / 2, sh.slots),
+                     dim3(128), 0, s, tabs);
     return 3;
 }
 

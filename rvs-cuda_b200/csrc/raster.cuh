@@ -100,6 +100,20 @@ __device__ __forceinline__ float key_invq(float4 A, float4 B, float4 C, float pr
     return rcp_approx(q);
 }
 
+// Upper 32 bits that no fragment of a triangle with vertex depths za, zb,
+// zc and key quality invq can go below.  A covered pixel's depth d is the
+// barycentric mix of the vertex depths with coordinates >= -1e-6 (up to
+// the fast coordinates' error bound), so d >= 0.999 z_min - 1e-5 z_max; the
+// key's bits fl(fl(fl(d d) d) invq) are monotone in d, so the same
+// expression at that bound is below every fragment's.  0 (no bound) when
+// the bound is not a positive finite depth.
+__device__ __forceinline__ uint32_t key_hi_lower_bound(float za, float zb, float zc, float invq) {
+    const float zmin = fminf(fminf(za, zb), zc), zmax = fmaxf(fmaxf(za, zb), zc);
+    const float d = __fsub_rn(__fmul_rn(0.999f, zmin), __fmul_rn(1e-5f, zmax));
+    if (!(d > 0.f) || !isfinite(d) || !(invq > 0.f) || !isfinite(invq)) return 0u;
+    return __float_as_uint(__fmul_rn(__fmul_rn(__fmul_rn(d, d), d), invq));
+}
+
 __device__ __forceinline__ unsigned long long frag_key(float d, float invq, uint32_t tri) {
     uint32_t hi = 0u;
     if (d > 0.f) hi = __float_as_uint(__fmul_rn(__fmul_rn(__fmul_rn(d, d), d), invq));
@@ -232,7 +246,11 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
         unsigned mask = __ballot_sync(0xffffffffu, big);
         if (!mask) continue;
         float invq_own = 0.f;
-        if (big) invq_own = key_invq(A, B, C, precision);
+        uint32_t hi_lb_own = 0u;
+        if (big) {
+            invq_own = key_invq(A, B, C, precision);
+            hi_lb_own = key_hi_lower_bound(A.z, B.z, C.z, invq_own);
+        }
         while (mask) {
             const int src = __ffs(mask) - 1;
             mask &= mask - 1;
@@ -247,6 +265,7 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
             const float za = __shfl_sync(0xffffffffu, A.z, src), zb_ = __shfl_sync(0xffffffffu, B.z, src);
             const float zc = __shfl_sync(0xffffffffu, C.z, src);
             const float invq = __shfl_sync(0xffffffffu, invq_own, src);
+            const unsigned long long key_lb = (unsigned long long)__shfl_sync(0xffffffffu, hi_lb_own, src) << 32;
             const uint32_t ttri = __shfl_sync(0xffffffffu, tri, src);
             t.x0 = __shfl_sync(0xffffffffu, s.x0, src);
             t.x1 = __shfl_sync(0xffffffffu, s.x1, src);
@@ -281,9 +300,14 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
                 const int rex = __shfl_sync(0xffffffffu, excl, row);
                 if (c >= total) continue;
                 const int x = rxl + (c - rex), yy = t.y0 + row;
+                unsigned long long* slot = &zb[(yy - ty0) * C::TW + (x - tx0)];
+                // Nothing to do where the pixel already holds a better key
+                // than any fragment of this triangle could have (atomicMin
+                // only ever lowers a key, so the skip changes nothing).
+                if (*slot < key_lb) continue;
                 float d;
                 if (!test_pixel(t, cx, cy, za, zb_, zc, x, yy, d)) continue;
-                atomicMin(&zb[(yy - ty0) * C::TW + (x - tx0)], frag_key(d, invq, ttri));
+                atomicMin(slot, frag_key(d, invq, ttri));
             }
         }
     }
@@ -367,9 +391,13 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
         const bool inside = t < NB && x0 < T.wo && y0 < T.ho;
         uint64_t code[4] = {0, 0, 0, 0};
         bool any_hole = false;
+        // A raster of odd width or height (Precision != 1 only: the output
+        // itself has even sides) ends in partial blocks.
+        const bool full = x0 + 1 < T.wo && y0 + 1 < T.ho;
         if (inside) {
 #pragma unroll
             for (int p = 0; p < 4; ++p) {
+                if (!full && (x0 + (p & 1) >= T.wo || y0 + (p >> 1) >= T.ho)) continue;
                 const int sp = (ly + (p >> 1)) * C::TW + lx + (p & 1);
                 const float c0 = acc[0][sp], c1 = acc[1][sp], c2 = acc[2][sp], q = acc[3][sp];
                 const bool hole = !(q > 0.f);
@@ -393,12 +421,25 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
                 if (T.rescale) pcolor[o] = make_float4(c0, c1, c2, 0.f);
             }
             const size_t o = (size_t)y0 * T.wo + x0;
-            reinterpret_cast<ulonglong2*>(codes + o)[0] = make_ulonglong2(code[0], code[1]);
-            reinterpret_cast<ulonglong2*>(codes + o + T.wo)[0] = make_ulonglong2(code[2], code[3]);
             auto hole_of = [](uint64_t c) -> uint16_t { return (c & kHoleBit) ? 1 : 0; };
-            reinterpret_cast<uint16_t*>(holes + o)[0] = (uint16_t)(hole_of(code[0]) | (hole_of(code[1]) << 8));
-            reinterpret_cast<uint16_t*>(holes + o + T.wo)[0] =
-                (uint16_t)(hole_of(code[2]) | (hole_of(code[3]) << 8));
+            if (!(T.wo & 1)) {
+                reinterpret_cast<ulonglong2*>(codes + o)[0] = make_ulonglong2(code[0], code[1]);
+                reinterpret_cast<uint16_t*>(holes + o)[0] = (uint16_t)(hole_of(code[0]) | (hole_of(code[1]) << 8));
+                if (full) {
+                    reinterpret_cast<ulonglong2*>(codes + o + T.wo)[0] = make_ulonglong2(code[2], code[3]);
+                    reinterpret_cast<uint16_t*>(holes + o + T.wo)[0] =
+                        (uint16_t)(hole_of(code[2]) | (hole_of(code[3]) << 8));
+                }
+            } else {
+                // odd width: the second row of a block is not 16-byte aligned
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const int x = x0 + (p & 1), y = y0 + (p >> 1);
+                    if (x >= T.wo || y >= T.ho) continue;
+                    codes[(size_t)y * T.wo + x] = code[p];
+                    holes[(size_t)y * T.wo + x] = (uint8_t)hole_of(code[p]);
+                }
+            }
             if (!any_hole && !T.rescale) {
                 reinterpret_cast<uint32_t*>(out_y + o)[0] =
                     (uint32_t)(code[0] & 0xffff) | ((uint32_t)(code[1] & 0xffff) << 16);

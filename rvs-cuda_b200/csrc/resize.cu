@@ -25,28 +25,6 @@ struct Filled {
     }
 };
 
-// Source coordinate of destination index d for INTER_LINEAR: the left (top)
-// tap and the weight of the right (bottom) one, clamped at both borders.
-__device__ __forceinline__ void linear_tap(int d, double scale, int n, int& s0, int& s1, float& f) {
-    f = (float)__dadd_rn(__dmul_rn((double)d + 0.5, scale), -0.5);
-    int s = (int)floorf(f);
-    f = __fsub_rn(f, (float)s);
-    if (s < 0) {
-        f = 0.f;
-        s = 0;
-    }
-    if (s >= n - 1) {
-        f = 0.f;
-        s = n - 1;
-    }
-    s0 = s;
-    s1 = min(s + 1, n - 1);
-}
-
-__device__ __forceinline__ float lerp2(float a, float b, float wa, float wb) {
-    return __fadd_rn(__fmul_rn(a, wa), __fmul_rn(b, wb));
-}
-
 // Resized colour of output pixel (x, y).
 __device__ __forceinline__ float3 resized(const DevTarget& T, const Filled& F, int x, int y) {
     if (T.rs_area) {

@@ -11,8 +11,8 @@
 // outputs MaskedOutputFiles, OutputMasks, DepthOutputFiles and
 // MaskedDepthOutputFiles are written when configured (Pipeline.cpp:303-336).
 // A virtual camera's Crop_region gives colour outputs of the region's size
-// and depth and mask outputs placed into a zero image of the padded
-// resolution (image_writing.cpp:262-267, 285-290).
+// and depth and mask outputs of the padded resolution whose luma is zero,
+// as the reference writes them (image_writing.cpp:262-267, 285-290).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -21,15 +21,20 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "rvsb.h"
 #include "rvsb_pipeline.hpp"
 
 namespace {
 
-void read_at(const char* path, long offset_per_frame, int frame, std::vector<uint16_t*> dst,
+// Reads frame `frame` of a raw YUV file.  Errors throw with the reference's
+// texts (image_loading.cpp:84-90, 155-161, 66-71); its CLI prints them and
+// exits with status 1 (view_synthesis.cpp:171-175).
+void read_at(const char* path, const char* kind, long offset_per_frame, int frame, std::vector<uint16_t*> dst,
              std::vector<size_t> counts) {
     FILE* f = std::fopen(path, "rb");
-    if (!f) throw std::runtime_error(std::string("Failed to read raw YUV file \"") + path + "\"");
+    if (!f) throw std::runtime_error(std::string("Failed to read raw YUV ") + kind + " file \"" + path + "\"");
     std::fseek(f, 0, SEEK_END);
     const long size = std::ftell(f);
     long off = offset_per_frame * frame;
@@ -38,7 +43,7 @@ void read_at(const char* path, long offset_per_frame, int frame, std::vector<uin
     for (size_t k = 0; k < dst.size(); ++k) {
         if (std::fread(dst[k], 2, counts[k], f) != counts[k]) {
             std::fclose(f);
-            throw std::runtime_error(std::string("Failed to read the expected amount of data from \"") + path + "\"");
+            throw std::runtime_error("Failed to read the expected amount of data");
         }
     }
     std::fclose(f);
@@ -77,16 +82,20 @@ protected:
     const rvsb_config* getConfig() const override { return cfg_; }
 
     rvsb::InputPlanes loadInputView(int frame, int view, const rvsb_camera& c) override {
+        nvtxRangePushA("rvsb cli: load input view");
+        struct Pop {
+            ~Pop() { nvtxRangePop(); }
+        } pop;
         rvsb::InputPlanes p;
         const size_t cy = (size_t)c.width * c.height, cc = (size_t)(c.width / 2) * (c.height / 2);
         p.y.resize(cy);
         p.u.resize(cc);
         p.v.resize(cc);
         p.depth.resize(cy);
-        read_at(rvsb_config_texture_path(cfg_, view), (long)(cy * 2 * 3 / 2), frame, {p.y.data(), p.u.data(), p.v.data()},
-                {cy, cc, cc});
+        read_at(rvsb_config_texture_path(cfg_, view), "color", (long)(cy * 2 * 3 / 2), frame,
+                {p.y.data(), p.u.data(), p.v.data()}, {cy, cc, cc});
         const long depth_frame = c.depth_color_format == RVSB_FMT_YUV420 ? (long)(cy * 2 * 3 / 2) : (long)(cy * 2);
-        read_at(rvsb_config_depth_path(cfg_, view), depth_frame, frame, {p.depth.data()}, {cy});
+        read_at(rvsb_config_depth_path(cfg_, view), "depth", depth_frame, frame, {p.depth.data()}, {cy});
         return p;
     }
 
@@ -97,7 +106,9 @@ protected:
     bool wantMaskedDepth() override { return files_[RVSB_OUT_MASKED_DEPTH] != nullptr; }
 
     void saveColor(const uint16_t* yuv, int frame, int, const rvsb_camera&) override {
+        nvtxRangePushA("rvsb cli: save colour");
         append(files_[RVSB_OUT_COLOR], frame == 0, yuv, (ny_ + 2 * nc_) * 2);
+        nvtxRangePop();
     }
     void saveMaskedColor(const uint16_t* yuv, int frame, int, const rvsb_camera&) override {
         append(files_[RVSB_OUT_MASKED_COLOR], frame == 0, yuv, (ny_ + 2 * nc_) * 2);
@@ -122,12 +133,16 @@ protected:
     }
 
 private:
-    // The region's rows placed into a zero luma plane of the padded size.
+    // The luma plane of a depth or mask output.  Without Crop_region it is
+    // the output itself.  With one, the reference pads with
+    // `padded(region) = image` (image_writing.cpp:262-267, 285-290): an
+    // OpenCV header assignment to a temporary region, which copies no data,
+    // so its file holds an all-zero luma plane of the padded size.  That is
+    // reproduced here.
     template <class T>
     void pad(T* dst, const T* src) const {
-        for (int r = 0; r < crop_[3]; ++r)
-            std::memcpy(dst + (size_t)(crop_[1] + r) * padded_[0] + crop_[0], src + (size_t)r * crop_[2],
-                        (size_t)crop_[2] * sizeof(T));
+        if (crop_[0] != 0 || crop_[1] != 0 || crop_[2] != padded_[0] || crop_[3] != padded_[1]) return;
+        std::memcpy(dst, src, (size_t)crop_[2] * crop_[3] * sizeof(T));
     }
     void write_depth(const char* path, int frame, const uint16_t* depth) const {
         std::vector<uint16_t> img(depth_chroma_ ? py_ + 2 * pc_ : py_, neutral_);

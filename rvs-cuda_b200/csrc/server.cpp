@@ -130,6 +130,7 @@ void rvsb_server::loop() {
                 L.bytes = 0;
                 break;  // nothing admissible: later lanes would admit nothing either
             }
+            HostRange range("rvsb: serve (launch a lane's batch)");
             batch.clear();
             for (const Pending& p : L.reqs) batch.push_back(p.req);
             L.start_s = now();

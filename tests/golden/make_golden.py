@@ -9,9 +9,13 @@
 3. synth_small_*.npz: small seeded syntheses by the CPU oracle (inputs,
    cameras, blended quality and the YUV420 result), which pin the oracle
    against later changes and give the GPU tests fixed expected outputs.
+4. cv2_resize_nearest.npz: cv::resize with INTER_NEAREST of one-byte masks
+   from the raster sizes of Precision != 1 to the output size (the validity
+   mask, Pipeline.cpp:303-308), recorded from cv2.
 
-Run from the repository root: python tests/golden/make_golden.py
-(needs cv2; the tests themselves only read the .npz files).
+Run from the repository root: python tests/golden/make_golden.py [NAME...]
+(NAME: resize_half, norm, synth, resize_nearest; all by default; needs
+cv2; the tests themselves only read the .npz files).
 """
 import os
 import sys
@@ -30,11 +34,32 @@ def camera_to_array(c):
     return np.frombuffer(raw, np.uint8).copy()
 
 
-def main():
+def resize_nearest():
+    import cv2
+    rng = np.random.default_rng(20261204)
+    arrays = {}
+    # (output w, h) and Precision: the raster is int(0.5 + W * P) x int(0.5 + H * P)
+    cases = [(128, 64, 2.0), (128, 64, 1.5), (96, 54, 1.5), (128, 64, 0.75), (100, 50, 0.9), (64, 36, 0.5),
+             (1920, 1080, 1.5), (960, 540, 0.7)]
+    for k, (w, h, P) in enumerate(cases):
+        P32 = np.float32(P)
+        rw, rh = int(np.float32(0.5) + np.float32(w) * P32), int(np.float32(0.5) + np.float32(h) * P32)
+        m = (rng.random((rh, rw)) < 0.3).astype(np.uint8) * 255
+        arrays[f"in{k}"] = m
+        arrays[f"out{k}"] = cv2.resize(m, (w, h), interpolation=cv2.INTER_NEAREST)
+    np.savez_compressed(os.path.join(HERE, "cv2_resize_nearest.npz"), n=len(cases), **arrays)
+
+
+def main(names=("resize_half", "norm", "synth", "resize_nearest")):
     import cv2
     import oracle as O
     from rvsb import scenes
 
+    if "resize_nearest" in names:
+        resize_nearest()
+    if not {"resize_half", "norm", "synth"} & set(names):
+        print("golden fixtures written to", HERE)
+        return
     rng = np.random.default_rng(20261203)
     # 1. cv::resize(0.5, 0.5, INTER_LINEAR) of uint16 planes
     #    recorded with Intel IPP on (outK, ties to even) and off (outK_noipp,
@@ -86,4 +111,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]) or ("resize_half", "norm", "synth", "resize_nearest"))

@@ -69,27 +69,78 @@ def test_precision_differs_from_one(ctx):
     assert any((x != y).any() for x, y in zip(a, b))
 
 
-def test_odd_raster_size_rejected(ctx):
-    """96 x 54 at P = 1.5 rasterises at 144 x 81: rejected, nothing written."""
+@pytest.mark.parametrize("w,h,P", [(96, 54, 1.5), (98, 54, 1.5), (64, 36, 0.75), (100, 50, 0.9)],
+                         ids=["144x81", "147x81", "48x27", "90x45"])
+def test_odd_raster_size(ctx, w, h, P):
+    """Raster sizes with an odd side (SynthesizedView.cpp:324-331 allows
+    any): the 2x2 blocks of the tile writer, the inpainting fill and the
+    multispectral blend end in partial blocks.  Hole mask identical to the
+    oracle's, output at parity, per-view call and multispectral."""
+    wl = scenes.random_pose_small(n_views=2, w=w, h=h, seed=127)
+    target = wl.targets[0]
+    target.rotation[0] += 4.0  # border holes reach the odd edge
+    yuv, dbg, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, debug=True, params=_params(P))
+    cpu, cq, _ = _oracle(wl, target, P)
+    rw, rh = int(np.float32(0.5) + np.float32(w) * np.float32(P)), int(np.float32(0.5) + np.float32(h) * np.float32(P))
+    assert cq.shape == (rh, rw) and (rw % 2 or rh % 2)
+    np.testing.assert_array_equal(~(dbg["blend_quality"] > 0), ~(cq > 0))
+    assert (~(cq > 0)).any()
+    assert_parity(yuv, cpu)
+    plain, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, params=_params(P))
+    for a, b in zip(plain, yuv):
+        np.testing.assert_array_equal(a, b)
+    ms, _ = gpu_synthesize(ctx, wl.inputs, wl.planes, target, 5.0, params=_params(P, multispectral=(1.0, 8.0)))
+    assert_parity(ms, _oracle(wl, target, P, multispectral=(1.0, 8.0))[0])
+
+
+def test_invalid_precision_rejected(ctx):
     wl = scenes.random_pose_small(n_views=2, w=96, h=54, seed=127)
-    with pytest.raises(rvsb.RvsbError) as e:
-        gpu_synthesize(ctx, wl.inputs, wl.planes, wl.targets[0], 5.0, params=_params(1.5))
-    assert e.value.status == 7
-    with pytest.raises(rvsb.RvsbError) as e:
-        gpu_synthesize(ctx, wl.inputs, wl.planes, wl.targets[0], 5.0, params=_params(-2.0))
-    assert e.value.status == 7
+    for P in (-2.0, 0.01):
+        with pytest.raises(rvsb.RvsbError) as e:
+            gpu_synthesize(ctx, wl.inputs, wl.planes, wl.targets[0], 5.0, params=_params(P))
+        assert e.value.status == 7
 
 
-def test_aux_outputs_need_precision_one(ctx):
-    wl = scenes.random_pose_small(n_views=2, w=128, h=64, seed=128)
+@pytest.mark.parametrize("case,P,threshold", [(dict(n_views=2, w=128, h=64, seed=128), 2.0, 5000.0),
+                                              (dict(n_views=3, w=96, h=54, seed=130), 1.5, 5000.0),
+                                              (dict(n_views=2, w=128, h=64, seed=131, erp_in=True), 0.75, 1000.0)],
+                         ids=["P2", "P1.5-odd", "P0.75-erp"])
+def test_aux_outputs_at_precision(ctx, case, P, threshold):
+    """OutputMasks, DepthOutputFiles and MaskedDepthOutputFiles at
+    Precision != 1 (Pipeline.cpp:303-333): validity and depth blended at the
+    raster size, the mask resized with INTER_NEAREST and the depth with
+    INTER_LINEAR to the output size; against the oracle with the tolerances
+    of test_gpu_aux.py.  MaskedOutputFiles is refused there: the reference
+    masks the raster-sized colour with the output-sized mask, which OpenCV
+    rejects."""
+    wl = scenes.random_pose_small(**case)
     sc = rvsb.Scene(ctx, wl.inputs)
     for i, p in enumerate(wl.planes):
         sc.upload(i, [np.ascontiguousarray(a, np.uint16) for a in p], on_device=False)
     t = wl.targets[0]
-    out = yuv_planes_torch(t.width, t.height)
-    mask = torch.zeros(t.height * t.width, dtype=torch.uint8, device="cuda")
+    t.rotation[0] += 3.0
+    wo, ho = t.width, t.height
+    out = yuv_planes_torch(wo, ho)
+    mask = torch.zeros(ho * wo, dtype=torch.uint8, device="cuda")
+    depth = torch.zeros(ho * wo, dtype=torch.int16, device="cuda")
+    mdepth = torch.zeros(ho * wo, dtype=torch.int16, device="cuda")
+    sc.synthesize_aux(t, _params(P), out, mask=mask, depth=depth, masked_depth=mdepth, validity_threshold=threshold)
+    torch.cuda.synchronize()
+    O.set_precision(P)
+    try:
+        ref = O.synthesize_aux(wl.inputs, wl.planes, t, 5.0, threshold, masked=False)
+    finally:
+        O.set_precision(1.0)
+    assert_parity(_yuv(out, t), ref["yuv"])
+    gmask = mask.cpu().numpy().reshape(ho, wo)
+    assert set(np.unique(gmask)) <= {0, 255} and ref["mask"].any() and (~ref["mask"].astype(bool)).any()
+    assert (gmask != ref["mask"]).mean() <= 1e-3
+    for g, r in ((depth, ref["depth"]), (mdepth, ref["masked_depth"])):
+        diff = np.abs(to_u16(g, (ho, wo)).astype(np.int64) - r.astype(np.int64))
+        assert (diff > 1).mean() <= 5e-3, f"{(diff > 1).mean():.4f} of depth samples differ by more than 1"
+    masked = yuv_planes_torch(wo, ho)
     with pytest.raises(rvsb.RvsbError) as e:
-        sc.synthesize_aux(t, _params(2.0), out, mask=mask)
+        sc.synthesize_aux(t, _params(P), out, masked=masked)
     assert e.value.status == 7
 
 

@@ -2,12 +2,16 @@
 is OpenCV's INTER_LINEAR resize of a float image (write_color,
 image_writing.cpp:188-190), checked against OpenCV itself; and the
 synthesis at P != 1 against the same synthesis at P = 1."""
+import os
+
 import numpy as np
 import pytest
 
 import oracle as O
 from rvsb import scenes
 from helpers import psnr
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 SIZES = [(192, 108, 96, 54), (144, 96, 96, 64), (64, 32, 128, 64), (96, 48, 128, 64), (200, 100, 128, 64),
          (100, 60, 128, 64), (384, 216, 192, 108), (128, 64, 128, 64)]
@@ -66,3 +70,14 @@ def test_synthesis_close_to_precision_one(P):
     assert q.shape == (int(0.5 + 64 * P), int(0.5 + 128 * P))
     assert any((a != b).any() for a, b in zip(yuv, base))
     assert psnr(yuv[0], base[0]) > 25.0
+
+
+def test_nearest_resize_matches_cv2():
+    """The validity mask's resize at Precision != 1 (cv::resize with
+    INTER_NEAREST, Pipeline.cpp:303-308) against cv2, from the raster sizes
+    of P = 2, 1.5, 0.75, 0.9, 0.5 and 0.7 (odd sides included)."""
+    z = np.load(os.path.join(GOLDEN, "cv2_resize_nearest.npz"))
+    for k in range(int(z["n"])):
+        src, expected = z[f"in{k}"], z[f"out{k}"]
+        h, w = expected.shape
+        np.testing.assert_array_equal(O.resize_nearest_u8(src, w, h), expected)

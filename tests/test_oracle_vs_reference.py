@@ -227,3 +227,23 @@ def test_reference_writer_chroma_matches_cv2(ties_up):
             _eq(U, expected)
     finally:
         ref.set_resize_ties_up(0)
+
+
+def test_reference_padded_aux_outputs_are_zero():
+    """The reference's depth and mask writers with a virtual Crop_region
+    (image_writing.cpp:262-267, 285-290) pad with `padded(region) = image`,
+    an OpenCV header assignment that copies no data: the file's luma is all
+    zero at the padded resolution.  Without a crop the image itself is
+    written.  The CLI reproduces both (test_gpu_cli.py)."""
+    cam = abi.make_camera(abi.PERSPECTIVE, 32, 16)
+    depth = np.linspace(1.0, 5.0, 32 * 16, dtype=np.float32).reshape(16, 32)
+    mask = np.zeros((16, 32), np.uint8)
+    mask[3:5, 4:9] = 1
+    plain = ref.write_aux("depth", depth, None, cam)
+    assert plain.shape == (16, 32) and plain.min() > 0
+    m = ref.write_aux("mask", None, mask, cam)
+    np.testing.assert_array_equal(m, mask * 255)
+    crop, padded = (8, 4, 32, 16), (64, 32)
+    assert not ref.write_aux("depth", depth, None, cam, crop, padded).any()
+    assert not ref.write_aux("masked_depth", depth, mask, cam, crop, padded).any()
+    assert not ref.write_aux("mask", None, mask, cam, crop, padded).any()
