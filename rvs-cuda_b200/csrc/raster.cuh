@@ -100,20 +100,6 @@ __device__ __forceinline__ float key_invq(float4 A, float4 B, float4 C, float pr
     return rcp_approx(q);
 }
 
-// Upper 32 bits that no fragment of a triangle with vertex depths za, zb,
-// zc and key quality invq can go below.  A covered pixel's depth d is the
-// barycentric mix of the vertex depths with coordinates >= -1e-6 (up to
-// the fast coordinates' error bound), so d >= 0.999 z_min - 1e-5 z_max; the
-// key's bits fl(fl(fl(d d) d) invq) are monotone in d, so the same
-// expression at that bound is below every fragment's.  0 (no bound) when
-// the bound is not a positive finite depth.
-__device__ __forceinline__ uint32_t key_hi_lower_bound(float za, float zb, float zc, float invq) {
-    const float zmin = fminf(fminf(za, zb), zc), zmax = fmaxf(fmaxf(za, zb), zc);
-    const float d = __fsub_rn(__fmul_rn(0.999f, zmin), __fmul_rn(1e-5f, zmax));
-    if (!(d > 0.f) || !isfinite(d) || !(invq > 0.f) || !isfinite(invq)) return 0u;
-    return __float_as_uint(__fmul_rn(__fmul_rn(__fmul_rn(d, d), d), invq));
-}
-
 __device__ __forceinline__ unsigned long long frag_key(float d, float invq, uint32_t tri) {
     uint32_t hi = 0u;
     if (d > 0.f) hi = __float_as_uint(__fmul_rn(__fmul_rn(__fmul_rn(d, d), d), invq));
@@ -246,11 +232,7 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
         unsigned mask = __ballot_sync(0xffffffffu, big);
         if (!mask) continue;
         float invq_own = 0.f;
-        uint32_t hi_lb_own = 0u;
-        if (big) {
-            invq_own = key_invq(A, B, C, precision);
-            hi_lb_own = key_hi_lower_bound(A.z, B.z, C.z, invq_own);
-        }
+        if (big) invq_own = key_invq(A, B, C, precision);
         while (mask) {
             const int src = __ffs(mask) - 1;
             mask &= mask - 1;
@@ -265,7 +247,6 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
             const float za = __shfl_sync(0xffffffffu, A.z, src), zb_ = __shfl_sync(0xffffffffu, B.z, src);
             const float zc = __shfl_sync(0xffffffffu, C.z, src);
             const float invq = __shfl_sync(0xffffffffu, invq_own, src);
-            const unsigned long long key_lb = (unsigned long long)__shfl_sync(0xffffffffu, hi_lb_own, src) << 32;
             const uint32_t ttri = __shfl_sync(0xffffffffu, tri, src);
             t.x0 = __shfl_sync(0xffffffffu, s.x0, src);
             t.x1 = __shfl_sync(0xffffffffu, s.x1, src);
@@ -300,14 +281,9 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
                 const int rex = __shfl_sync(0xffffffffu, excl, row);
                 if (c >= total) continue;
                 const int x = rxl + (c - rex), yy = t.y0 + row;
-                unsigned long long* slot = &zb[(yy - ty0) * C::TW + (x - tx0)];
-                // Nothing to do where the pixel already holds a better key
-                // than any fragment of this triangle could have (atomicMin
-                // only ever lowers a key, so the skip changes nothing).
-                if (*slot < key_lb) continue;
                 float d;
                 if (!test_pixel(t, cx, cy, za, zb_, zc, x, yy, d)) continue;
-                atomicMin(slot, frag_key(d, invq, ttri));
+                atomicMin(&zb[(yy - ty0) * C::TW + (x - tx0)], frag_key(d, invq, ttri));
             }
         }
     }
