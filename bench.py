@@ -672,7 +672,10 @@ def main():
     torch.cuda.synchronize()
     barrier(world)
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    jobs = ParityJobs() if rank == 0 and not args.no_parity else None
+    # Parity of the timed outputs: one GPU (every rank runs the same code;
+    # with several, rank 0 alone would spend seconds of CPU after the others
+    # finished).
+    jobs = ParityJobs() if rank == 0 and world == 1 and not args.no_parity else None
     if jobs is not None:
         jobs.add("plain", scene, wl.inputs, wl.planes, target, p, out)
     total_s = sum(step_ms) / 1000.0
