@@ -24,14 +24,16 @@ reference's per-frame InputView::load) and synthesising.
   parity  every timed output (plain, a batch slot, two targets of each
          batched configuration, one served request per output class)
          against the reference's own CPU synthesis of the same target.
-  cpu_baseline  the CPU oracle (a restatement of the reference's CPU path)
-         on a bounded sample, 1 thread (the reference's loops are serial).
+  cpu_baseline  the reference's own CPU synthesis (oracle/_ref, its
+         sources compiled unmodified against an OpenCV stand-in; the
+         oracle's restatement when that library is not built) on a bounded
+         sample, 1 thread (the reference's loops are serial).
 
 Multi-GPU: pose-parallel replicas (each rank synthesises its own views;
 no collective on the data path), value = all ranks' views / max time.
 
---impl reference times the reference's CPU path (the oracle port; the
-reference itself does not build here) on the host cores.
+--impl reference times the same reference CPU synthesis on the host cores,
+one view per thread per step.
 """
 import argparse
 import json
