@@ -216,11 +216,18 @@ rvsb_status rvsb_config_virtual_camera_at(const rvsb_config* cfg, int i, int fra
  * 245-249).  Colour outputs have the region's size; depth and mask outputs
  * are placed into a zero image of the padded size (write_maskedDepth /
  * write_mask, image_writing.cpp:262-267, 285-290).  Without the key the
- * region is the whole resolution.  Input cameras with a region other than
- * the whole resolution are rejected (RVSB_E_UNSUPPORTED): the reference
- * reads their colour at the region's size and their depth at the padded
- * size. */
+ * region is the whole resolution. */
 rvsb_status rvsb_config_virtual_crop(const rvsb_config* cfg, int i, int32_t region[4], int32_t padded_size[2]);
+/* "Crop_region" of input camera i, as rvsb_config_virtual_crop.  The camera
+ * returned by rvsb_config_input_camera has the region's size (and moved
+ * principal point).  The reference reads such a view's colour frames at the
+ * region's size (image_loading.cpp:76) and its depth frames at the padded
+ * size (image_loading.cpp:149), decodes the padded depth and then takes its
+ * first width x height samples in memory order as the region-sized depth
+ * map (SynthesizedView.cpp:89-94).  The depth plane to pass for the view is
+ * therefore the first width * height samples of the padded frame's luma
+ * plane, which is what the rvsb CLI loads. */
+rvsb_status rvsb_config_input_crop(const rvsb_config* cfg, int i, int32_t region[4], int32_t padded_size[2]);
 
 /* Relative pose of an input camera seen from the virtual camera:
  * R = R_virt^T * R_in, t = -R_virt^T * (t_virt - t_in), in float with the

@@ -25,7 +25,9 @@ namespace rvsb {
 
 /* Raw planes of one input view at one frame, as read_color_YUV and
  * read_depth_YUV read them (rvs/src/image_loading.cpp:74-211): Y W*H, U and V
- * (W/2)*(H/2) colour samples, and the W*H luma plane of the depth map. */
+ * (W/2)*(H/2) colour samples, and the W*H luma plane of the depth map
+ * (W x H the camera's size; with an input Crop_region, the first W*H
+ * samples of the padded depth frame's luma: rvsb_config_input_crop). */
 struct InputPlanes {
     std::vector<uint16_t> y, u, v, depth;
 };

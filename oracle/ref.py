@@ -245,11 +245,14 @@ def set_raster_precision(p):
     set_precision(p)
 
 
-def load_view(cam, color_path, depth_path, frame):
+def load_view(cam, color_path, depth_path, frame, crop=None, padded=None):
     """The reference's loader (read_color / read_depth, image_loading.cpp,
     with its CUDA kernels from process_input_frame.cu): decoded colour
-    (H, W, 3) and depth (H, W) of `frame`.  Needs a CUDA device."""
-    c = Camera(cam)
+    (H, W, 3) and depth (H, W) of `frame`, H x W the camera's (region's)
+    size; with crop / padded (camera_dict) the depth is read at the padded
+    size and its first H * W samples returned, as the reference's CPU mode
+    copies them (SynthesizedView.cpp:89-94).  Needs a CUDA device."""
+    c = Camera(cam, crop, padded)
     color = np.empty((cam.height, cam.width, 3), np.float32)
     depth = np.empty((cam.height, cam.width), np.float32)
     _check(lib().ref_load_view(c.h, color_path.encode(), depth_path.encode(), int(frame), _p(color), _p(depth)))

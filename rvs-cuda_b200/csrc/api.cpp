@@ -807,9 +807,9 @@ rvsb_status rvsb_config_virtual_camera(const rvsb_config* c, int i, rvsb_camera*
     return RVSB_OK;
 }
 
-rvsb_status rvsb_config_virtual_crop(const rvsb_config* c, int i, int32_t region[4], int32_t padded_size[2]) {
-    if (!c || !region || !padded_size || i < 0 || i >= (int)c->cfg.crop_virtual.size()) return RVSB_E_ARG;
-    const CropRegion& r = c->cfg.crop_virtual[i];
+static rvsb_status crop_of(const std::vector<CropRegion>& v, int i, int32_t region[4], int32_t padded_size[2]) {
+    if (!region || !padded_size || i < 0 || i >= (int)v.size()) return RVSB_E_ARG;
+    const CropRegion& r = v[i];
     region[0] = r.x;
     region[1] = r.y;
     region[2] = r.w;
@@ -817,6 +817,14 @@ rvsb_status rvsb_config_virtual_crop(const rvsb_config* c, int i, int32_t region
     padded_size[0] = r.padded_w;
     padded_size[1] = r.padded_h;
     return RVSB_OK;
+}
+
+rvsb_status rvsb_config_virtual_crop(const rvsb_config* c, int i, int32_t region[4], int32_t padded_size[2]) {
+    return c ? crop_of(c->cfg.crop_virtual, i, region, padded_size) : RVSB_E_ARG;
+}
+
+rvsb_status rvsb_config_input_crop(const rvsb_config* c, int i, int32_t region[4], int32_t padded_size[2]) {
+    return c ? crop_of(c->cfg.crop_real, i, region, padded_size) : RVSB_E_ARG;
 }
 
 const char* rvsb_config_texture_path(const rvsb_config* c, int i) {

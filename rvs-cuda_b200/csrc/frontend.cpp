@@ -254,10 +254,7 @@ rvsb_camera parse_camera(const json::Node& root, CropRegion* crop) {
         int v[4];
         int_vec<4>(n, v);
         if (v[0] != 0 || v[1] != 0 || v[2] != c.width || v[3] != c.height) {
-            // An input camera's colour is read at the region's size and its
-            // depth at the padded size (image_loading.cpp:76, 149), which do
-            // not describe one image; only output cameras are cropped.
-            if (!crop) throw Unsupported("Crop_region is supported on virtual cameras only");
+            if (!crop) throw Unsupported("Crop_region needs the camera's padded resolution reported beside it");
             if (v[0] < 0 || v[1] < 0 || v[2] <= 0 || v[3] <= 0 || v[0] > c.width - v[2] || v[1] > c.height - v[3])
                 throw ConfigError("Crop_region must lie inside the resolution");
             cr.x = v[0];
@@ -335,7 +332,7 @@ namespace {
 
 // Config::loadCamerasParametersFromFile (Config.cpp:122-175).
 std::vector<rvsb_camera> load_cameras(const std::string& path, const std::vector<std::string>& names,
-                                      const json::Node& overrides, std::vector<CropRegion>* crops = nullptr) {
+                                      const json::Node& overrides, std::vector<CropRegion>& crops) {
     json::Node root = json::Node::parse(read_text_file(path, "camera parameters file"));
     std::string version = root.require("Version").asString();
     std::string v2 = version.substr(0, 2);
@@ -356,11 +353,8 @@ std::vector<rvsb_camera> load_cameras(const std::string& path, const std::vector
     for (const auto& n : names) {
         auto it = index.find(n);
         if (it == index.end()) throw ConfigError("Camera parameters file does not have camera '" + n + "'");
-        const CropRegion& cr = it->second.second;
-        if (!crops && (cr.w != cr.padded_w || cr.h != cr.padded_h))
-            throw Unsupported("Crop_region is supported on virtual cameras only (camera '" + n + "')");
         out.push_back(it->second.first);
-        if (crops) crops->push_back(cr);
+        crops.push_back(it->second.second);
     }
     return out;
 }
@@ -382,9 +376,9 @@ Config load_config(const std::string& path) {
     c.input_names = string_list(root.require("InputCameraNames"));
     c.virtual_names = string_list(root.require("VirtualCameraNames"));
     c.params_real = load_cameras(root.require("InputCameraParameterFile").asString(), c.input_names,
-                                 root.optional("InputOverrides"));
+                                 root.optional("InputOverrides"), c.crop_real);
     c.params_virtual = load_cameras(root.require("VirtualCameraParameterFile").asString(), c.virtual_names,
-                                    root.optional("VirtualOverrides"), &c.crop_virtual);
+                                    root.optional("VirtualOverrides"), c.crop_virtual);
     auto inputs = [&](const char* key, std::vector<std::string>& dst) {
         json::Node n = root.require(key);
         if (n.size() != c.input_names.size())

@@ -80,8 +80,9 @@ struct CropRegion {
 // is the region's (getSize, Parameters.cpp:187-190) and a perspective
 // principal point is moved by the region's top-left corner
 // (getPrinciplePoint, Parameters.cpp:245-249); ERP ranges already refer to
-// the region.  Without `crop`, a region other than the whole resolution is
-// rejected.
+// the region.  Without `crop` (a camera parsed alone, with nowhere to
+// report its padded resolution), a region other than the whole resolution
+// is rejected.
 rvsb_camera parse_camera(const json::Node& node, CropRegion* crop = nullptr);
 
 struct Pose {
@@ -96,7 +97,7 @@ struct Config {
     std::string version;
     std::vector<std::string> input_names, virtual_names;
     std::vector<rvsb_camera> params_real, params_virtual;
-    std::vector<CropRegion> crop_virtual;
+    std::vector<CropRegion> crop_real, crop_virtual;
     std::vector<std::string> texture_names, depth_names;
     std::vector<std::string> outfilenames, outmaskedfilenames, outmaskfilenames, outdepthfilenames,
         outmaskdepthfilenames;

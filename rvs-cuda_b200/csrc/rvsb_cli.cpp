@@ -12,7 +12,9 @@
 // MaskedDepthOutputFiles are written when configured (Pipeline.cpp:303-336).
 // A virtual camera's Crop_region gives colour outputs of the region's size
 // and depth and mask outputs of the padded resolution whose luma is zero,
-// as the reference writes them (image_writing.cpp:262-267, 285-290).
+// as the reference writes them (image_writing.cpp:262-267, 285-290).  An
+// input camera's Crop_region is read as the reference reads it: colour
+// frames of the region's size, depth frames of the padded size.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -91,11 +93,18 @@ protected:
         p.y.resize(cy);
         p.u.resize(cc);
         p.v.resize(cc);
-        p.depth.resize(cy);
         read_at(rvsb_config_texture_path(cfg_, view), "color", (long)(cy * 2 * 3 / 2), frame,
                 {p.y.data(), p.u.data(), p.v.data()}, {cy, cc, cc});
-        const long depth_frame = c.depth_color_format == RVSB_FMT_YUV420 ? (long)(cy * 2 * 3 / 2) : (long)(cy * 2);
-        read_at(rvsb_config_depth_path(cfg_, view), "depth", depth_frame, frame, {p.depth.data()}, {cy});
+        // Depth frames have the padded size (image_loading.cpp:149); with a
+        // Crop_region the view's depth is the first region-area samples of
+        // that frame's luma (SynthesizedView.cpp:89-94).
+        int32_t region[4], padded[2];
+        size_t py = cy;
+        if (rvsb_config_input_crop(cfg_, view, region, padded) == RVSB_OK) py = (size_t)padded[0] * padded[1];
+        const long depth_frame = c.depth_color_format == RVSB_FMT_YUV420 ? (long)(py * 2 * 3 / 2) : (long)(py * 2);
+        p.depth.resize(py);
+        read_at(rvsb_config_depth_path(cfg_, view), "depth", depth_frame, frame, {p.depth.data()}, {py});
+        p.depth.resize(cy);
         return p;
     }
 

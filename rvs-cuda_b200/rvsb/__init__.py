@@ -33,7 +33,7 @@ EXPORTED = [
     "rvsb_server_drain", "rvsb_server_clock", "rvsb_server_destroy",
     "rvsb_batch_set_autotune", "rvsb_batch_set_raster_variant", "rvsb_batch_last_raster_variant",
     "rvsb_scene_set_autotune", "rvsb_scene_set_raster_variant", "rvsb_synthesize_aux", "rvsb_config_output_file", "rvsb_config_validity_threshold",
-    "rvsb_config_virtual_crop", "rvsb_host_stream_create", "rvsb_host_stream_destroy", "rvsb_host_stream_submit",
+    "rvsb_config_virtual_crop", "rvsb_config_input_crop", "rvsb_host_stream_create", "rvsb_host_stream_destroy", "rvsb_host_stream_submit",
     "rvsb_host_stream_wait", "rvsb_host_stream_join",
 ]
 
@@ -88,6 +88,7 @@ def load():
     L.rvsb_config_synth_params.restype = None
     L.rvsb_config_virtual_camera_at.argtypes = [c_p, ctypes.c_int, ctypes.c_int, P(Camera)]
     L.rvsb_config_virtual_crop.argtypes = [c_p, ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_int32)]
+    L.rvsb_config_input_crop.argtypes = [c_p, ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_int32)]
     L.rvsb_relative_pose.argtypes = [P(Camera), P(Camera), P(ctypes.c_float), P(ctypes.c_float)]
     L.rvsb_scene_create.argtypes = [c_p, P(Camera), ctypes.c_int, P(c_p)]
     L.rvsb_scene_destroy.argtypes = [c_p]
@@ -513,6 +514,19 @@ def camera_from_json(text):
     return c
 
 
+def crop_depth_plane(padded_luma, width, height):
+    """The depth plane of an input camera with Crop_region: the reference
+    decodes the padded depth frame and takes its first width * height
+    samples in memory order as the region-sized map (image_loading.cpp:149,
+    SynthesizedView.cpp:89-94).  padded_luma: the padded frame's luma plane
+    (any shape, row-major)."""
+    import numpy as np
+    flat = np.ascontiguousarray(padded_luma).reshape(-1)
+    if flat.size < width * height:
+        raise ValueError("the padded depth frame is smaller than the region")
+    return flat[:width * height].reshape(height, width)
+
+
 class Config:
     """rvsb_config: an RVS configuration file and its camera files."""
 
@@ -551,6 +565,17 @@ class Config:
         st = self.lib.rvsb_config_virtual_crop(self.h, i, r, s)
         if st != RVSB_OK:
             raise RvsbError(st, "no such virtual camera")
+        return tuple(r), tuple(s)
+
+    def input_crop(self, i=0):
+        """((x, y, width, height), (padded width, padded height)) of input
+        camera i.  The view's depth plane is the first width * height
+        samples of the padded depth frame's luma (crop_depth_plane)."""
+        r = (ctypes.c_int32 * 4)()
+        s = (ctypes.c_int32 * 2)()
+        st = self.lib.rvsb_config_input_crop(self.h, i, r, s)
+        if st != RVSB_OK:
+            raise RvsbError(st, "no such input camera")
         return tuple(r), tuple(s)
 
     def frames(self):

@@ -145,7 +145,8 @@ def test_camera_from_json_missing_key():
 @pytest.mark.parametrize("extra", [dict(DisplacementMethod="Polynomial"), dict(Crop_region=[0, 0, 960, 540])])
 def test_camera_from_json_unsupported(extra):
     """A single camera outside a configuration: a crop region is only
-    supported on a configuration's virtual cameras."""
+    supported where its padded resolution can be reported (a
+    configuration's cameras)."""
     with pytest.raises(rvsb.RvsbError) as e:
         rvsb.camera_from_json(json.dumps(_persp(**extra)))
     assert e.value.status == 7  # RVSB_E_UNSUPPORTED
@@ -211,8 +212,8 @@ def test_config_virtual_crop(tmp_path, monkeypatch):
 
 
 @pytest.mark.parametrize("where,region,status", [
-    ("input", [0, 0, 800, 400], 7),      # input crops: colour and depth sizes disagree in the reference
-    ("viewport", [400, 0, 640, 360], 2),  # outside the resolution
+    ("input", [1200, 0, 800, 400], 2),   # outside the resolution
+    ("viewport", [400, 0, 640, 360], 2),
     ("viewport", [0, 0, 0, 360], 2),
 ])
 def test_config_crop_rejected(tmp_path, monkeypatch, where, region, status):
@@ -221,6 +222,34 @@ def test_config_crop_rejected(tmp_path, monkeypatch, where, region, status):
     with pytest.raises(rvsb.RvsbError) as e:
         rvsb.Config(_write_setup(tmp_path, **kw))
     assert e.value.status == status
+
+
+def test_config_input_crop(tmp_path, monkeypatch):
+    """Crop_region of an input camera: the camera takes the region's size
+    and moved principal point, as a virtual camera does, and the region
+    and padded size are reported for the loader (colour frames of the
+    region's size, depth frames of the padded size)."""
+    monkeypatch.chdir(tmp_path)
+    res = _persp()["Resolution"]
+    pp = _persp()["Principle_point"]
+    c = rvsb.Config(_write_setup(tmp_path, input_extra=dict(Crop_region=[64, 32, 800, 400])))
+    v1, v2 = c.inputs()
+    assert (v1.width, v1.height) == (800, 400)
+    assert list(v1.principle_point) == [pp[0] - 64, pp[1] - 32]
+    assert c.input_crop(0) == ((64, 32, 800, 400), tuple(res))
+    assert c.input_crop(1) == ((0, 0, res[0], res[1]), tuple(res))
+    with pytest.raises(rvsb.RvsbError):
+        c.input_crop(2)
+
+
+def test_crop_depth_plane():
+    """The region-sized depth map of a cropped input: the padded frame's
+    first width * height samples in memory order, not the region's window."""
+    padded = np.arange(8 * 6, dtype=np.uint16).reshape(6, 8)
+    d = rvsb.crop_depth_plane(padded, 4, 3)
+    np.testing.assert_array_equal(d, np.arange(12, dtype=np.uint16).reshape(3, 4))
+    with pytest.raises(ValueError):
+        rvsb.crop_depth_plane(padded, 8, 7)
 
 
 def test_config_input_crop_full_resolution(tmp_path, monkeypatch):

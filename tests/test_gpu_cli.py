@@ -224,3 +224,95 @@ def test_cli_frames_past_end_wrap(tmp_path):
     assert_parity(O.split_yuv420(out[0], t.width, t.height), O.synthesize(wl.inputs, wl.planes, t, 5.0))
     np.testing.assert_array_equal(out[1], out[0])
     np.testing.assert_array_equal(out[2], out[0])
+
+
+def test_cli_input_crop_region(tmp_path):
+    """An input camera with Crop_region, read as the reference reads it:
+    colour frames of the region's size (image_loading.cpp:76), depth frames
+    of the padded size (image_loading.cpp:149) whose first region-area
+    samples, in memory order, are the view's depth (SynthesizedView.cpp:
+    89-94).  The padded depth frames hold the true depth there and other
+    values in the region's window, so reading the window would fail; two
+    frames check the padded frame offset.  The output matches the oracle's
+    synthesis of the uncropped inputs, and, where the reference harness is
+    built, the reference's own loader gives the same depth."""
+    wl = scenes.random_pose_small(n_views=2, w=96, h=54, seed=95)
+    names = [f"v{i}" for i in range(len(wl.inputs))]
+    target = wl.targets[0]
+    c0 = wl.inputs[0]
+    w, h = c0.width, c0.height
+    cx, cy, pw, ph = 6, 4, w + 10, h + 8
+    v0 = _cam_json(names[0], c0)
+    v0["Resolution"] = [pw, ph]
+    v0["Crop_region"] = [cx, cy, w, h]
+    v0["Principle_point"] = [float(c0.principle_point[0]) + cx, float(c0.principle_point[1]) + cy]
+    cams = {"Version": "2.0", "cameras": [v0] + [_cam_json(n, c) for n, c in zip(names[1:], wl.inputs[1:])] +
+            [_cam_json("viewport", target)]}
+    (tmp_path / "cams.json").write_text(json.dumps(cams))
+    n_frames = 2
+    rng = np.random.default_rng(17)
+
+    def depth_k(d, k):
+        return np.clip(d.astype(np.int32) + 300 * k, 0, 65535).astype(np.uint16)
+
+    padded_frames = []
+    for i, planes in enumerate(wl.planes):
+        y, u, v, d = planes
+        with open(tmp_path / f"t{i}.yuv", "wb") as ft, open(tmp_path / f"d{i}.yuv", "wb") as fd:
+            for k in range(n_frames):
+                yk, uk, vk, _ = _frame_planes(planes, k)
+                ft.write(yk.tobytes() + uk.tobytes() + vk.tobytes())
+                dk = depth_k(d, k)
+                if i == 0:
+                    pad = rng.integers(0, 65536, (ph, pw)).astype(np.uint16)
+                    pad.reshape(-1)[:w * h] = dk.reshape(-1)
+                    padded_frames.append(pad)
+                    dk = pad
+                chroma = np.full((dk.shape[0] // 2) * (dk.shape[1] // 2), 32768, np.uint16)
+                fd.write(dk.tobytes() + chroma.tobytes() + chroma.tobytes())
+    window = padded_frames[0][cy:cy + h, cx:cx + w]
+    assert (window != wl.planes[0][3]).mean() > 0.9  # the window is not the depth
+    cfg = {"Version": "3.0", "InputCameraParameterFile": "cams.json", "VirtualCameraParameterFile": "cams.json",
+           "InputCameraNames": names, "VirtualCameraNames": ["viewport"],
+           "ViewImageNames": [f"t{i}.yuv" for i in range(len(names))],
+           "DepthMapNames": [f"d{i}.yuv" for i in range(len(names))],
+           "OutputFiles": ["out.yuv"], "NumberOfFrames": n_frames, "BlendingFactor": 5.0}
+    (tmp_path / "rvs.json").write_text(json.dumps(cfg))
+    r = subprocess.run([CLI, "rvs.json"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    wo, ho = target.width, target.height
+    out = np.fromfile(tmp_path / "out.yuv", np.uint16).reshape(n_frames, -1)
+    import rvsb
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        conf = rvsb.Config("rvs.json")
+        assert conf.input_crop(0) == ((cx, cy, w, h), (pw, ph))
+        cin = conf.inputs()[0]
+    finally:
+        os.chdir(cwd)
+    assert list(cin.principle_point) == list(c0.principle_point)
+    for k in range(n_frames):
+        planes = []
+        for i, p in enumerate(wl.planes):
+            yk, uk, vk, _ = _frame_planes(p, k)
+            dk = rvsb.crop_depth_plane(padded_frames[k], w, h) if i == 0 else depth_k(p[3], k)
+            planes.append((yk, uk, vk, dk))
+        np.testing.assert_array_equal(planes[0][3], depth_k(wl.planes[0][3], k))
+        ref = O.synthesize(wl.inputs, planes, target, 5.0)
+        assert_parity(O.split_yuv420(out[k], wo, ho), ref)
+    import ref as R
+    if R.available():
+        import sys
+        script = (f"import sys, numpy as np; sys.path.insert(0, {os.path.join(ROOT, 'oracle')!r}); "
+                  f"sys.path.insert(0, {os.path.join(ROOT, 'rvs-cuda_b200')!r}); import ref; from rvsb import abi; "
+                  f"cam = abi.Camera.from_buffer_copy(bytes.fromhex(sys.argv[1])); "
+                  f"out = [ref.load_view(cam, 't0.yuv', 'd0.yuv', k, ({cx}, {cy}, {w}, {h}), ({pw}, {ph}))[1] "
+                  f"for k in range({n_frames})]; np.save(sys.argv[2], np.stack(out))")
+        r = subprocess.run([sys.executable, "-c", script, bytes(c0).hex(), str(tmp_path / "rd.npy")], cwd=tmp_path,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        rd = np.load(tmp_path / "rd.npy")
+        for k in range(n_frames):
+            want = O.decode_depth(depth_k(wl.planes[0][3], k), c0)
+            np.testing.assert_array_equal(rd[k], want)
