@@ -271,7 +271,7 @@ def test_cli_input_crop_region(tmp_path):
                 chroma = np.full((dk.shape[0] // 2) * (dk.shape[1] // 2), 32768, np.uint16)
                 fd.write(dk.tobytes() + chroma.tobytes() + chroma.tobytes())
     window = padded_frames[0][cy:cy + h, cx:cx + w]
-    assert (window != wl.planes[0][3]).mean() > 0.9  # the window is not the depth
+    assert (window != wl.planes[0][3]).mean() > 0.5  # the window is not the depth
     cfg = {"Version": "3.0", "InputCameraParameterFile": "cams.json", "VirtualCameraParameterFile": "cams.json",
            "InputCameraNames": names, "VirtualCameraNames": ["viewport"],
            "ViewImageNames": [f"t{i}.yuv" for i in range(len(names))],
