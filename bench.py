@@ -30,7 +30,9 @@ reference's per-frame InputView::load) and synthesising.
          sample, 1 thread (the reference's loops are serial).
 
 Multi-GPU: pose-parallel replicas (each rank synthesises its own views;
-no collective on the data path), value = all ranks' views / max time.
+no collective on the data path), value = all ranks' views / max time.  The
+serving and batched-configuration lines are per-GPU figures and are then
+skipped unless asked for (--serve-seconds, --load-seconds).
 
 --impl reference times the same reference CPU synthesis on the host cores,
 one view per thread per step.
@@ -596,21 +598,31 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-slots", type=int, default=16)
     ap.add_argument("--batch-steps", type=int, default=8)
-    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    # the serving and batched-configuration lines are per-GPU figures: by
+    # default measured on one GPU only (under torchrun each rank would hold
+    # its GPU for them without adding to the job's aggregate)
+    ap.add_argument("--serve-seconds", type=float, default=None)
     ap.add_argument("--serve-rate", type=float, default=500.0)
     ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=2)
     # closed-loop capacity of the serving path at a fixed number of requests in flight
-    ap.add_argument("--load-seconds", type=float, default=10.0)
+    ap.add_argument("--load-seconds", type=float, default=None)
     ap.add_argument("--load-in-flight", type=int, default=6)
     ap.add_argument("--load-lanes", type=int, default=2)
     ap.add_argument("--load-batch", type=int, default=4)
-    ap.add_argument("--no-batched-configs", action="store_true")
+    ap.add_argument("--no-batched-configs", action="store_true", default=None)
     # skip the parity check of the timed outputs against the reference's CPU path
     ap.add_argument("--no-parity", action="store_true")
     # only the per-view lines (value, e2e): for launch lists of the per-view path
     ap.add_argument("--plain-only", action="store_true")
     args = ap.parse_args()
+    single = int(os.environ.get("WORLD_SIZE", "1")) == 1
+    if args.serve_seconds is None:
+        args.serve_seconds = 60.0 if single else 0.0
+    if args.load_seconds is None:
+        args.load_seconds = 10.0 if single else 0.0
+    if args.no_batched_configs is None:
+        args.no_batched_configs = not single
     if args.plain_only:
         args.no_batched_configs = True
         args.serve_seconds = 0.0

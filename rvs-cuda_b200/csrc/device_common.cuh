@@ -61,10 +61,17 @@ __device__ __forceinline__ float decode_depth_raw(float near_, float far_, float
 // EquirectangularProjector.cpp:60-99.
 // View: DevView, or a copy of the fields used here (the warp kernel keeps
 // them in registers).
+// The depth-table entry of input pixel (i, j): the decoded depth and the
+// perspective factors of its raw sample.
 template <class View>
-__device__ __forceinline__ float4 warp_vertex(const View& V, const DevTarget& T, int i, int j) {
-    const size_t idx = (size_t)i * V.w + j;
-    const float4 L = __ldg(V.depth_lut + __ldg(V.pd + idx));
+__device__ __forceinline__ float4 depth_entry(const View& V, int i, int j) {
+    return __ldg(V.depth_lut + __ldg(V.pd + (size_t)i * V.w + j));
+}
+
+// L: depth_entry(V, i, j), loaded by the caller (the warp kernel issues a
+// thread's loads ahead of its arithmetic).
+template <class View>
+__device__ __forceinline__ float4 warp_vertex(const View& V, const DevTarget& T, int i, int j, float4 L) {
     const float d = L.x;
     float x0, x1, x2;
     if (V.proj == 1) {
@@ -122,6 +129,11 @@ __device__ __forceinline__ float4 warp_vertex(const View& V, const DevTarget& T,
         v = sv;
     }
     return make_float4(u, v, z, 0.f);
+}
+
+template <class View>
+__device__ __forceinline__ float4 warp_vertex(const View& V, const DevTarget& T, int i, int j) {
+    return warp_vertex(V, T, i, j, depth_entry(V, i, j));
 }
 
 // Triangle quality of transform.cpp:62-75 (valid_tri): the longest edge by

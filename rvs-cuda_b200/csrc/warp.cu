@@ -163,13 +163,22 @@ __global__ void __launch_bounds__(256) warp_kernel(const __grid_constant__ Tabs 
     const bool wrap = T.wrap != 0;
     const bool seam = wrap && blockIdx.x == 0;
     const int j = j0 + lane;
+    // The thread's depth samples, then their table entries, before any
+    // arithmetic: the dependent gathers of the four rows overlap instead of
+    // each waiting behind the previous row's vertex store.
+    float4 L[ROWS];
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+        const int i = i0 + warp * ROWS + r;
+        if (i < V.h && j < V.w) L[r] = depth_entry(V, i, j);
+    }
     Box col;
 #pragma unroll
     for (int r = 0; r < ROWS; ++r) {
         const int i = i0 + warp * ROWS + r;
         float2 q = make_float2(qnan(), qnan());
         if (i < V.h && j < V.w) {
-            const float4 p = warp_vertex(V, T, i, j);
+            const float4 p = warp_vertex(V, T, i, j, L[r]);
             V.vert[(size_t)i * V.w + j] = p;
             q = box_point(p, wrap);
         }
