@@ -292,7 +292,10 @@ __device__ __forceinline__ void raster_block(const DevView& V, int wo, int ho, b
 
 // Resolves and blends the views g0 .. g0 + gn - 1 of the tile, one pixel per
 // thread and step, into the accumulators (c0, c1, c2, q per pixel).
-template <class C>
+// Extras: the per-view multispectral, auxiliary and debug outputs are
+// written (without them the view loop holds no global store, so a view's
+// loads may be issued while the previous view is blended).
+template <class C, bool Extras>
 __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int gn, int tx0, int ty0,
                                               const unsigned long long (*zb)[C::NPIX], float (*acc)[C::NPIX],
                                               const DebugPtrs& dbg) {
@@ -305,7 +308,7 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
         if (g0 > 0) {
             a.c0 = acc[0][p]; a.c1 = acc[1][p]; a.c2 = acc[2][p]; a.q = acc[3][p];
         }
-        const bool aux = tab.aux.on != 0;
+        const bool aux = Extras && tab.aux.on != 0;
         const size_t po = (size_t)y * T.wo + x;
         float adepth = 0.f, avalid = 0.f;
         if (aux && g0 > 0) {
@@ -316,7 +319,7 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
             const int v = g0 + k;
             const Fragment f = resolve_fragment(tab.v[v], zb[k][p], x, y, T.precision);
             const float qv = __fdiv_rn(f.validity, f.depth);
-            if (tab.ms.on) tab.ms.view[(size_t)v * npo + po] = make_float4(f.col.x, f.col.y, f.col.z, qv);
+            if (Extras && tab.ms.on) tab.ms.view[(size_t)v * npo + po] = make_float4(f.col.x, f.col.y, f.col.z, qv);
             if (aux) {
                 // BlendedView.cpp:205-208: the view's depth where its quality
                 // beats the accumulator's before this blend (view 0: its
@@ -331,7 +334,7 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
                     avalid = smax(avalid, f.validity);
                 }
             }
-            if (dbg.view_color || dbg.view_depth || dbg.view_validity) {
+            if (Extras && (dbg.view_color || dbg.view_depth || dbg.view_validity)) {
                 const size_t o = (size_t)y * T.wo + x;
                 if (dbg.view_color) {
                     float* c = dbg.view_color + ((size_t)v * npo + o) * 3;
@@ -548,7 +551,10 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_co
             }
             __syncthreads();
         }
-        resolve_group<C>(tab, g0, gn, tx0, ty0, zb, acc, tab.dbg);
+        if (tab.ms.on || tab.aux.on || tab.dbg.view_color || tab.dbg.view_depth || tab.dbg.view_validity)
+            resolve_group<C, true>(tab, g0, gn, tx0, ty0, zb, acc, tab.dbg);
+        else
+            resolve_group<C, false>(tab, g0, gn, tx0, ty0, zb, acc, tab.dbg);
         __syncthreads();
     }
     write_tile<C>(T, tx0, ty0, acc, tab.b.status, tab.b.codes, tab.b.holes, tab.out_y, tab.out_u, tab.out_v,
