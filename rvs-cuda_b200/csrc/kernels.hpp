@@ -81,7 +81,7 @@ struct RasterVariant {
 constexpr int NUM_RASTER_VARIANTS = 8;
 constexpr RasterVariant kRasterVariants[NUM_RASTER_VARIANTS] = {
     {32, 32, 4, 4, 1024, 0}, {64, 32, 2, 4, 1024, 0}, {32, 32, 4, 2, 1024, 0},  {32, 32, 4, 8, 1024, 0},
-    {32, 32, 2, 4, 512, 0},  {32, 16, 4, 4, 512, 0},  {32, 32, 4, 2, 1024, 32}, {64, 32, 2, 4, 1024, 32},
+    {64, 32, 4, 4, 1024, 0}, {32, 16, 4, 4, 512, 0},  {32, 32, 4, 2, 1024, 32}, {64, 32, 2, 4, 1024, 32},
 };
 
 // One-time kernel attributes of the current device (the raster kernel's

@@ -1,5 +1,6 @@
-// Raster variant 4: 32x32 tiles, 2 views per z-buffer group,
-// warp-cooperative above 4 candidate pixels, 512 bin entries per round.
+// Raster variant 4: 64x32 tiles, 4 views per z-buffer group (100 KB of
+// shared memory per CTA, still two CTAs per SM), warp-cooperative above 4
+// candidate pixels, 1024 bin entries per round.
 #include "raster.cuh"
 
-RVSB_RASTER_VARIANT(4, 32, 32, 2, 4, 512, 0)
+RVSB_RASTER_VARIANT(4, 64, 32, 4, 4, 1024, 0)
