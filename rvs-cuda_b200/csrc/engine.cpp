@@ -477,12 +477,14 @@ float pixels_per_radian(const rvsb_camera& c) {
 // equirectangular output stretches its rows by 1 / cos(latitude), sqrt(2) at
 // the median row, which its m includes (equirectangular to equirectangular
 // at m = 1: 4.30 -> 3.25 ms).  The largest m of the batch decides.
-// At m close to 1 a perspective output with enough tiles runs variant 4
-// (64x32 tiles, all four views in one z-buffer group): a binning block then
-// lands in 1.35 tiles instead of 1.53 and the bins are half as many, 4 x
-// 1920x1080 into 1920x1080 0.651 -> 0.636 ms; with fewer than about two
-// waves of its tiles (960x540: 255), or minified (1920x1080 into an
-// equirectangular 4096x2048, m = 0.62: 1.03 -> 1.22 ms), it is slower.
+// At m close to 1 a single perspective output with enough tiles runs
+// variant 4 (64x32 tiles, all four views in one z-buffer group): a binning
+// block then lands in 1.35 tiles instead of 1.53 and the bins are half as
+// many, 4 x 1920x1080 into 1920x1080 0.651 -> 0.636 ms; with fewer than
+// about two waves of its tiles (960x540: 255), or minified (1920x1080 into
+// an equirectangular 4096x2048, m = 0.62: 1.03 -> 1.22 ms), it is slower,
+// and a batch of 16 such views runs faster with variant 1 (1797 against
+// 1762 views/s), which the tuner finds from the default variant 0.
 constexpr int kMagnifiedVariant = 7;
 constexpr int kWideTileVariant = 4;
 constexpr long long kWideTileMinTiles = 600;  // two waves of two CTAs on 148 SMs
@@ -513,7 +515,7 @@ int default_variant(const SlotRequest* reqs, int n) {
         wide_tiles += (long long)((rd.w + 63) / 64) * ((rd.h + 31) / 32);
     }
     if (m > 1.1f) return kMagnifiedVariant;
-    if (!erp_out && m_min >= 0.9f && wide_tiles >= kWideTileMinTiles) return kWideTileVariant;
+    if (n == 1 && !erp_out && m_min >= 0.9f && wide_tiles >= kWideTileMinTiles) return kWideTileVariant;
     return 0;
 }
 

@@ -141,9 +141,9 @@ def test_every_raster_variant_identical(ctx, erp):
 def test_default_raster_variant_follows_magnification(ctx):
     """With no variant pinned and the tuner off, an output at the inputs'
     pixels per radian runs variant 0, a 3x magnified one variant 7 (the
-    medium-triangle path) and an unmagnified one with at least 600 tiles of
-    64x32 (here 1920x1080) variant 4 (64x32 tiles of four views); each
-    gives the bytes of another variant."""
+    medium-triangle path) and a single unmagnified one with at least 600
+    tiles of 64x32 (here 1920x1080) variant 4 (64x32 tiles of four views);
+    each gives the bytes of another variant."""
     import torch
     wl = scenes.random_pose_small(n_views=2, w=64, h=36, seed=5)
     sc = _upload(ctx, wl)
