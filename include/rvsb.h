@@ -414,9 +414,9 @@ rvsb_status rvsb_batch_reserve(rvsb_batch* batch, int max_width, int max_height)
 rvsb_status rvsb_batch_set_graphs(rvsb_batch* batch, int enable);
 /* Raster autotuner (default off): the first batch of each new shape (batch
  * size bucket, largest input set and output, projections) is run once with
- * every raster variant -- tile size 32x32, 64x32 or 32x16, views per shared
- * z-buffer group, the stretched-triangle threshold, the bin entries staged
- * per round and whether triangles whose candidate box holds 5 to 32 pixels
+ * every raster variant -- tile size 32x32 or 64x32, views per shared
+ * z-buffer group, the stretched-triangle threshold, threads per tile (512 or
+ * 1024) and whether triangles whose candidate box holds up to 32 pixels
  * take the one-lane-per-pixel medium path -- and the fastest is kept for that shape.
  * All variants give identical outputs. */
 rvsb_status rvsb_batch_set_autotune(rvsb_batch* batch, int enable);

@@ -17,7 +17,7 @@ constexpr int WARP_TILE = 32;
 constexpr int TILE_THREADS = 512;
 // Smallest tile of any raster variant (sizes the bin arrays).
 constexpr int MIN_TILE_W = 32;
-constexpr int MIN_TILE_H = 16;
+constexpr int MIN_TILE_H = 32;
 
 // Per input view parameters of one synthesis (device copy in a table).
 struct DevView {

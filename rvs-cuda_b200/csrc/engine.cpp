@@ -473,50 +473,38 @@ float pixels_per_radian(const rvsb_camera& c) {
 // leave the small path (at most 4 candidates) and the medium path of variant
 // 7 rasterises them faster: 960x540 inputs into a 1920x1080 output (m = 2)
 // 0.359 -> 0.285 ms, 4096x2048 equirectangular inputs into 1920x1080
-// (m = 1.47) 1.03 -> 0.62 ms.  At m <= 1 variant 0 is 2 to 26% faster.  An
+// (m = 1.47) 1.03 -> 0.62 ms; at m <= 1 it is 2 to 26% slower.  An
 // equirectangular output stretches its rows by 1 / cos(latitude), sqrt(2) at
 // the median row, which its m includes (equirectangular to equirectangular
 // at m = 1: 4.30 -> 3.25 ms).  The largest m of the batch decides.
-// At m close to 1 a single perspective output with enough tiles runs
-// variant 4 (64x32 tiles, all four views in one z-buffer group): a binning
-// block then lands in 1.35 tiles instead of 1.53 and the bins are half as
-// many, 4 x 1920x1080 into 1920x1080 0.651 -> 0.636 ms; with fewer than
-// about two waves of its tiles (960x540: 255), or minified (1920x1080 into
-// an equirectangular 4096x2048, m = 0.62: 1.03 -> 1.22 ms), it is slower,
-// and a batch of 16 such views runs faster with variant 1 (1797 against
-// 1762 views/s), which the tuner finds from the default variant 0.
+// At m <= 1.1 variant 4 (64x32 tiles, all four views in one z-buffer
+// group, 1024-thread CTAs, one per SM) runs: a binning block lands in 1.35
+// of its tiles instead of 1.53 of 32x32, the bins are half as many, and a
+// tile's 32 warps finish it in about half the time of 16, which keeps the
+// last wave short.  Against variant 0 (ms per view, median of 36 calls):
+// 4 x 1920x1080 into 1920x1080 0.648 -> 0.621, into 960x540 0.459 -> 0.453,
+// into an equirectangular 4096x2048 1.027 -> 0.943; 2 x 960x540 into
+// 960x540 0.153 -> 0.150.
 constexpr int kMagnifiedVariant = 7;
-constexpr int kWideTileVariant = 4;
-constexpr long long kWideTileMinTiles = 600;  // two waves of two CTAs on 148 SMs
+constexpr int kDefaultVariant = 4;
 static_assert(kRasterVariants[kMagnifiedVariant].med > kRasterVariants[kMagnifiedVariant].small,
               "the magnified default has the medium-triangle path");
-static_assert(kRasterVariants[kWideTileVariant].tw == 64 && kRasterVariants[kWideTileVariant].th == 32 &&
-                  kRasterVariants[kWideTileVariant].vg == 4,
-              "the wide-tile default holds 64x32 tiles of four views");
+static_assert(kRasterVariants[kDefaultVariant].tw == 64 && kRasterVariants[kDefaultVariant].vg == 4 &&
+                  kRasterVariants[kDefaultVariant].threads == 1024,
+              "the default holds 64x32 tiles of four views in 1024-thread CTAs");
 
 int default_variant(const SlotRequest* reqs, int n) {
-    float m = 0.f, m_min = INFINITY;
-    bool erp_out = false;
-    long long wide_tiles = 0;
+    float m = 0.f;
     for (int k = 0; k < n; ++k) {
         const SlotRequest& r = reqs[k];
         float in = 0.f;
         for (const rvsb_camera& c : r.scene->cams) in = std::max(in, pixels_per_radian(c));
         const RasterDims rd = raster_dims(r.virt, r.params);
         float out = pixels_per_radian(r.virt) * (float)rd.w / (float)r.virt.width;
-        if (r.virt.projection == RVSB_PROJ_EQUIRECTANGULAR) {
-            out *= 1.41421356f;
-            erp_out = true;
-        }
-        if (in > 0.f) {
-            m = std::max(m, out / in);
-            m_min = std::min(m_min, out / in);
-        }
-        wide_tiles += (long long)((rd.w + 63) / 64) * ((rd.h + 31) / 32);
+        if (r.virt.projection == RVSB_PROJ_EQUIRECTANGULAR) out *= 1.41421356f;
+        if (in > 0.f) m = std::max(m, out / in);
     }
-    if (m > 1.1f) return kMagnifiedVariant;
-    if (n == 1 && !erp_out && m_min >= 0.9f && wide_tiles >= kWideTileMinTiles) return kWideTileVariant;
-    return 0;
+    return m > 1.1f ? kMagnifiedVariant : kDefaultVariant;
 }
 
 }  // namespace

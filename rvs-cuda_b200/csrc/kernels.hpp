@@ -76,13 +76,21 @@ int launch_batch(const Tabs& tabs, const BatchShape& shape, cudaStream_t stream,
 // together (med <= small: each one alone, row span by row span).  Every
 // variant gives identical results.
 struct RasterVariant {
-    int tw, th, vg, small, ent, med;
+    int tw, th, vg, small, ent, med, threads;
 };
 constexpr int NUM_RASTER_VARIANTS = 8;
 constexpr RasterVariant kRasterVariants[NUM_RASTER_VARIANTS] = {
-    {32, 32, 4, 4, 1024, 0}, {64, 32, 2, 4, 1024, 0}, {32, 32, 4, 2, 1024, 0},  {32, 32, 4, 8, 1024, 0},
-    {64, 32, 4, 4, 1024, 0}, {32, 16, 4, 4, 512, 0},  {32, 32, 4, 2, 1024, 32}, {64, 32, 2, 4, 1024, 32},
+    {32, 32, 4, 4, 1024, 0, 512},  {64, 32, 2, 4, 1024, 0, 512},   {32, 32, 4, 4, 1024, 0, 1024},
+    {32, 32, 4, 8, 1024, 0, 512},  {64, 32, 4, 4, 1024, 0, 1024},  {64, 32, 2, 4, 1024, 32, 1024},
+    {32, 32, 4, 2, 1024, 32, 512}, {64, 32, 2, 4, 1024, 32, 512},
 };
+// The bin arrays are sized for tiles of MIN_TILE_W x MIN_TILE_H.
+constexpr bool tiles_at_least_minimum() {
+    for (const RasterVariant& v : kRasterVariants)
+        if (v.tw < MIN_TILE_W || v.th < MIN_TILE_H) return false;
+    return true;
+}
+static_assert(tiles_at_least_minimum(), "a raster variant's tiles are smaller than the bins are sized for");
 
 // One-time kernel attributes of the current device (the raster kernel's
 // dynamic shared memory); call before launching or capturing a batch.

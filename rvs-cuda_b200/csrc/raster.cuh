@@ -16,7 +16,6 @@ namespace raster {
 
 using namespace dev;
 
-constexpr int NWARPS = TILE_THREADS / 32;
 constexpr int QUADS = BLOCK_W * BLOCK_H;
 static_assert(QUADS == 32, "one warp per binning block");
 
@@ -24,9 +23,12 @@ static_assert(QUADS == 32, "one warp per binning block");
 // gives one lane per row), VG views per shared z-buffer group, triangles
 // with more than SMALL candidate pixels go warp-cooperative, ENT bin
 // entries staged per round.
-template <int TW_, int TH_, int VG_, int SMALL_, int ENT_, int MED_>
+template <int TW_, int TH_, int VG_, int SMALL_, int ENT_, int MED_, int THREADS_ = TILE_THREADS>
 struct Cfg {
     static constexpr int TW = TW_, TH = TH_, VG = VG_, SMALL = SMALL_, ENT = ENT_;
+    // Threads per CTA (one CTA per tile); CTAs resident per SM with 64
+    // registers per thread (1024 threads fill the 65536 registers).
+    static constexpr int THREADS = THREADS_, NWARPS = THREADS_ / 32, MIN_CTAS = 1024 / THREADS_;
     // Triangles with more than SMALL and at most MED candidate pixels are
     // rasterised with their candidates flattened across the warp (MED <=
     // SMALL: none); larger ones one at a time, row span by row span.
@@ -40,6 +42,7 @@ struct Cfg {
     static_assert(TH <= 32 && TW % 2 == 0 && TH % 2 == 0, "tile shape");
     static_assert(MED <= 32, "a medium triangle's candidate index stays below 32");
     static_assert(kZbBytes % 16 == 0 && kEntBytes % 16 == 0, "shared-memory carve alignment");
+    static_assert(THREADS % 32 == 0 && 1024 % THREADS == 0, "whole warps, whole CTAs per SM");
 };
 
 // Candidate pixel (x, y) of a set-up triangle: the coverage test of
@@ -301,7 +304,7 @@ __device__ __forceinline__ void resolve_group(const SlotTable& tab, int g0, int 
                                               const DebugPtrs& dbg) {
     const DevTarget& T = tab.t;
     const size_t npo = (size_t)T.wo * T.ho;
-    for (int p = threadIdx.x; p < C::NPIX; p += TILE_THREADS) {
+    for (int p = threadIdx.x; p < C::NPIX; p += C::THREADS) {
         const int x = tx0 + p % C::TW, y = ty0 + p / C::TW;
         if (x >= T.wo || y >= T.ho) continue;
         BlendAcc a = {0.f, 0.f, 0.f, 0.f};
@@ -363,7 +366,7 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
     constexpr int BW = C::TW / 2, NB = (C::TW / 2) * (C::TH / 2);
     int hx0 = INT_MAX, hy0 = INT_MAX, hx1 = INT_MIN, hy1 = INT_MIN;
     bool warp_hole = false;
-    for (int base = 0; base < NB; base += TILE_THREADS) {
+    for (int base = 0; base < NB; base += C::THREADS) {
         const int t = base + (int)threadIdx.x;
         const int lx = 2 * (t % BW), ly = 2 * (t / BW);
         const int x0 = tx0 + lx, y0 = ty0 + ly;
@@ -474,7 +477,7 @@ __device__ __forceinline__ void write_tile(const DevTarget& T, int tx0, int ty0,
 // the tile's accumulators.  After the last group the tile is quantised and
 // written.
 template <class C, class Tabs>
-__global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_constant__ Tabs tabs) {
+__global__ void __launch_bounds__(C::THREADS, C::MIN_CTAS) raster_kernel(const __grid_constant__ Tabs tabs) {
     grid_dep_wait();
     // Dynamic shared memory: the group's z-buffers, the staged bin entries
     // and the tile's blend accumulators.
@@ -499,7 +502,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_co
 
     for (int g0 = 0; g0 < T.n_views; g0 += C::VG) {
         const int gn = min(C::VG, T.n_views - g0);
-        for (int k = tid; k < gn * C::NPIX; k += TILE_THREADS) zb[k / C::NPIX][k % C::NPIX] = kEmptyKey;
+        for (int k = tid; k < gn * C::NPIX; k += C::THREADS) zb[k / C::NPIX][k % C::NPIX] = kEmptyKey;
         if (tid == 0) {
             int run = 0;
             for (int k = 0; k < gn; ++k) {
@@ -515,8 +518,8 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_co
         const int E = s_pref[gn];
         for (int base = 0; base < E; base += C::ENT) {
             const int n = min(C::ENT, E - base);
-            if (tid == 0) s_next = NWARPS;
-            for (int q = tid; q < n; q += TILE_THREADS) {
+            if (tid == 0) s_next = C::NWARPS;
+            for (int q = tid; q < n; q += C::THREADS) {
                 const int e = base + q;
                 int k = 0;
                 while (k + 1 < gn && e >= s_pref[k + 1]) ++k;
@@ -563,7 +566,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) raster_kernel(const __grid_co
 
 template <class C, class Tabs>
 void launch(const Tabs& tabs, const BatchShape& sh, cudaStream_t s) {
-    launch_dependent(raster_kernel<C, Tabs>, dim3(sh.max_tiles, sh.slots), dim3(TILE_THREADS), C::kSmemBytes, s, tabs);
+    launch_dependent(raster_kernel<C, Tabs>, dim3(sh.max_tiles, sh.slots), dim3(C::THREADS), C::kSmemBytes, s, tabs);
 }
 
 template <class C>
@@ -579,12 +582,13 @@ void prepare() {
 
 // Defines the host entry points of raster variant N (one per .cu file, so
 // the variants compile in parallel).
-#define RVSB_RASTER_VARIANT(N, TW, TH, VG, SMALL, ENT, MED)                                                    \
+#define RVSB_RASTER_VARIANT(N, TW, TH, VG, SMALL, ENT, MED, THREADS)                                      \
     namespace rvsb {                                                                                     \
-    using RasterCfg##N = raster::Cfg<TW, TH, VG, SMALL, ENT, MED>;                                             \
+    using RasterCfg##N = raster::Cfg<TW, TH, VG, SMALL, ENT, MED, THREADS>;                              \
     static_assert(kRasterVariants[N].tw == TW && kRasterVariants[N].th == TH &&                          \
                       kRasterVariants[N].vg == VG && kRasterVariants[N].small == SMALL &&                \
-                      kRasterVariants[N].ent == ENT && kRasterVariants[N].med == MED,                                                     \
+                      kRasterVariants[N].ent == ENT && kRasterVariants[N].med == MED &&                  \
+                      kRasterVariants[N].threads == THREADS,                                             \
                   "variant table");                                                                      \
     void launch_raster_v##N(const TableParam& t, const BatchShape& sh, cudaStream_t s) {                 \
         raster::launch<RasterCfg##N>(t, sh, s);                                                          \

@@ -1,5 +1,6 @@
 // Raster variant 2: 32x32 tiles, 4 views per z-buffer group,
-// warp-cooperative above 2 candidate pixels, 1024 bin entries per round.
+// warp-cooperative above 4 candidate pixels, 1024 bin entries per round,
+// 1024-thread CTAs (one per SM).
 #include "raster.cuh"
 
-RVSB_RASTER_VARIANT(2, 32, 32, 4, 2, 1024, 0)
+RVSB_RASTER_VARIANT(2, 32, 32, 4, 4, 1024, 0, 1024)

@@ -1,5 +1,7 @@
-// Raster variant 5: 32x16 tiles, 4 views per z-buffer group,
-// warp-cooperative above 4 candidate pixels, 512 bin entries per round.
+// Raster variant 5: 64x32 tiles, 2 views per z-buffer group,
+// medium triangles (5 to 32 candidate pixels) flattened across the warp,
+// larger ones warp-cooperative, 1024 bin entries per round, 1024-thread
+// CTAs (one per SM).
 #include "raster.cuh"
 
-RVSB_RASTER_VARIANT(5, 32, 16, 4, 4, 512, 0)
+RVSB_RASTER_VARIANT(5, 64, 32, 2, 4, 1024, 32, 1024)

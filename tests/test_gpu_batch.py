@@ -140,10 +140,9 @@ def test_every_raster_variant_identical(ctx, erp):
 
 def test_default_raster_variant_follows_magnification(ctx):
     """With no variant pinned and the tuner off, an output at the inputs'
-    pixels per radian runs variant 0, a 3x magnified one variant 7 (the
-    medium-triangle path) and a single unmagnified one with at least 600
-    tiles of 64x32 (here 1920x1080) variant 4 (64x32 tiles of four views);
-    each gives the bytes of another variant."""
+    pixels per radian (small or 1920x1080) runs variant 4 (64x32 tiles of
+    four views, 1024-thread CTAs) and a 3x magnified one variant 7 (the
+    medium-triangle path); each gives the bytes of another variant."""
     import torch
     wl = scenes.random_pose_small(n_views=2, w=64, h=36, seed=5)
     sc = _upload(ctx, wl)
@@ -158,7 +157,7 @@ def test_default_raster_variant_follows_magnification(ctx):
     wide.width, wide.height = 1920, 1080
     wide.principle_point[0], wide.principle_point[1] = 960.0, 540.0
     b = rvsb.Batch(sc, 1)
-    for cam, expected_variant in ((same, 0), (big, 7), (wide, 4)):
+    for cam, expected_variant in ((same, 4), (big, 7), (wide, 4)):
         out = yuv_planes_torch(cam.width, cam.height)
         b.synthesize([cam], p, [out])
         torch.cuda.synchronize()
