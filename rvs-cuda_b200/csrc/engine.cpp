@@ -484,27 +484,40 @@ float pixels_per_radian(const rvsb_camera& c) {
 // last wave short.  Against variant 0 (ms per view, median of 36 calls):
 // 4 x 1920x1080 into 1920x1080 0.648 -> 0.621, into 960x540 0.459 -> 0.453,
 // into an equirectangular 4096x2048 1.027 -> 0.943; 2 x 960x540 into
-// 960x540 0.153 -> 0.150.
+// 960x540 0.153 -> 0.150.  A perspective output minified to m <= 0.6 has
+// many small triangles per tile, and the 32x32 tiles of variant 2 (also
+// 1024-thread CTAs) rasterise it faster: 4 x 1920x1080 into 960x540 (m =
+// 0.5) 0.450 -> 0.406 ms, into 640x360 (m = 0.33) 0.521 -> 0.440 ms; at m =
+// 0.67 variant 4 is ahead again (0.452 against 0.466).
 constexpr int kMagnifiedVariant = 7;
 constexpr int kDefaultVariant = 4;
+constexpr int kMinifiedVariant = 2;
 static_assert(kRasterVariants[kMagnifiedVariant].med > kRasterVariants[kMagnifiedVariant].small,
               "the magnified default has the medium-triangle path");
 static_assert(kRasterVariants[kDefaultVariant].tw == 64 && kRasterVariants[kDefaultVariant].vg == 4 &&
                   kRasterVariants[kDefaultVariant].threads == 1024,
               "the default holds 64x32 tiles of four views in 1024-thread CTAs");
+static_assert(kRasterVariants[kMinifiedVariant].tw == 32 && kRasterVariants[kMinifiedVariant].threads == 1024,
+              "the minified default holds 32x32 tiles in 1024-thread CTAs");
 
 int default_variant(const SlotRequest* reqs, int n) {
     float m = 0.f;
+    bool erp_out = false;
     for (int k = 0; k < n; ++k) {
         const SlotRequest& r = reqs[k];
         float in = 0.f;
         for (const rvsb_camera& c : r.scene->cams) in = std::max(in, pixels_per_radian(c));
         const RasterDims rd = raster_dims(r.virt, r.params);
         float out = pixels_per_radian(r.virt) * (float)rd.w / (float)r.virt.width;
-        if (r.virt.projection == RVSB_PROJ_EQUIRECTANGULAR) out *= 1.41421356f;
+        if (r.virt.projection == RVSB_PROJ_EQUIRECTANGULAR) {
+            out *= 1.41421356f;
+            erp_out = true;
+        }
         if (in > 0.f) m = std::max(m, out / in);
     }
-    return m > 1.1f ? kMagnifiedVariant : kDefaultVariant;
+    if (m > 1.1f) return kMagnifiedVariant;
+    if (!erp_out && m <= 0.6f) return kMinifiedVariant;
+    return kDefaultVariant;
 }
 
 }  // namespace

@@ -141,8 +141,10 @@ def test_every_raster_variant_identical(ctx, erp):
 def test_default_raster_variant_follows_magnification(ctx):
     """With no variant pinned and the tuner off, an output at the inputs'
     pixels per radian (small or 1920x1080) runs variant 4 (64x32 tiles of
-    four views, 1024-thread CTAs) and a 3x magnified one variant 7 (the
-    medium-triangle path); each gives the bytes of another variant."""
+    four views, 1024-thread CTAs), a 3x magnified one variant 7 (the
+    medium-triangle path) and a perspective one minified 3x variant 2
+    (32x32 tiles, 1024-thread CTAs); each gives the bytes of another
+    variant."""
     import torch
     wl = scenes.random_pose_small(n_views=2, w=64, h=36, seed=5)
     sc = _upload(ctx, wl)
@@ -156,8 +158,13 @@ def test_default_raster_variant_follows_magnification(ctx):
     wide = copy.deepcopy(same)
     wide.width, wide.height = 1920, 1080
     wide.principle_point[0], wide.principle_point[1] = 960.0, 540.0
+    small = copy.deepcopy(same)
+    small.width, small.height = 22, 12
+    for i in range(2):
+        small.focal[i] /= 3.0
+        small.principle_point[i] /= 3.0
     b = rvsb.Batch(sc, 1)
-    for cam, expected_variant in ((same, 4), (big, 7), (wide, 4)):
+    for cam, expected_variant in ((same, 4), (big, 7), (wide, 4), (small, 2)):
         out = yuv_planes_torch(cam.width, cam.height)
         b.synthesize([cam], p, [out])
         torch.cuda.synchronize()
