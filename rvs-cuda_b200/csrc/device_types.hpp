@@ -8,7 +8,8 @@ namespace rvsb {
 // Tiling constants.  A binning block is BLOCK_W x BLOCK_H quads of an input
 // view (each quad = two triangles, transform.cpp:159-176); an output tile
 // (its size is chosen per batch among the raster variants) holds 64-bit
-// z-buffers in shared memory and is processed by TILE_THREADS threads.
+// z-buffers in shared memory and is processed by one CTA of the variant's
+// thread count (TILE_THREADS unless the variant names another).
 constexpr int BLOCK_W = 8;
 constexpr int BLOCK_H = 4;
 // Vertex tile of the warp kernel (WARP_TILE x WARP_TILE input pixels per CTA),
