@@ -18,6 +18,12 @@ using namespace dev;
 
 constexpr int QUADS = BLOCK_W * BLOCK_H;
 static_assert(QUADS == 32, "one warp per binning block");
+// A binning block whose pixel box exceeds four times its (BLOCK_W + 1) x
+// (BLOCK_H + 1) vertices holds stretched triangles (a depth discontinuity)
+// and is rasterised before the others of its tile, the longest work first:
+// on the plain 1080p view the median box is 60 pixels and 2.5% of the
+// blocks exceed this.
+constexpr int kBigBlockArea = 4 * (BLOCK_W + 1) * (BLOCK_H + 1);
 
 // TW x TH output pixels per tile (TH <= 32: the stretched-triangle path
 // gives one lane per row), VG views per shared z-buffer group, triangles
@@ -487,7 +493,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MIN_CTAS) raster_kernel(const _
     auto acc = reinterpret_cast<float(*)[C::NPIX]>(s_raw + C::kZbBytes + C::kEntBytes);
     __shared__ int s_pref[C::VG + 1];
     __shared__ int s_off[C::VG];
-    __shared__ int s_next;
+    __shared__ int s_next, s_front, s_back;
     const SlotTable& tab = tabs.at(blockIdx.y);
     const DevTarget& T = tab.t;
     if ((int)blockIdx.x >= T.ntx * T.nty) return;
@@ -518,7 +524,15 @@ __global__ void __launch_bounds__(C::THREADS, C::MIN_CTAS) raster_kernel(const _
         const int E = s_pref[gn];
         for (int base = 0; base < E; base += C::ENT) {
             const int n = min(C::ENT, E - base);
-            if (tid == 0) s_next = C::NWARPS;
+            if (tid == 0) {
+                s_next = C::NWARPS;
+                s_front = 0;
+                s_back = 0;
+            }
+            __syncthreads();
+            // Staged big blocks first (from the front), the others from the
+            // back; the order within each part does not matter (the keys
+            // are order independent).
             for (int q = tid; q < n; q += C::THREADS) {
                 const int e = base + q;
                 int k = 0;
@@ -536,7 +550,15 @@ __global__ void __launch_bounds__(C::THREADS, C::MIN_CTAS) raster_kernel(const _
                 } else {
                     b = list[s_off[k] + (e - s_pref[k])];
                 }
-                s_ent[q] = b < 0 ? -1 : (k << 26) | b;
+                int code = -1;
+                bool big_block = false;
+                if (b >= 0) {
+                    code = (k << 26) | b;
+                    const DevView& V = tab.v[g0 + k];
+                    const int4 bb = V.bbox[(b >> 11) * V.nbx + (b & 2047)];
+                    big_block = (bb.z - bb.x + 1) * (bb.w - bb.y + 1) > kBigBlockArea;
+                }
+                s_ent[big_block ? atomicAdd(&s_front, 1) : n - 1 - atomicAdd(&s_back, 1)] = code;
             }
             __syncthreads();
             // Entries are taken dynamically: a warp claims its next entry
