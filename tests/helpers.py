@@ -72,6 +72,26 @@ def psnr(a, b, peak=1023.0):
     return float("inf") if m == 0 else 10 * np.log10(peak * peak / m)
 
 
+def two_region_psnr(actual, reference, bits=10):
+    """PSNR of a YUV420 frame against another as the reference's integration
+    tests measure it (integration_test.cpp:98-145): one mean square error
+    over the samples of all three planes, for the whole frame and for the
+    central third of each plane (borders excluded, where errors are
+    largest).  Returns (whole, central)."""
+    out = []
+    for central in (False, True):
+        sse, n = 0.0, 0
+        for a, b in zip(actual, reference):
+            h, w = a.shape
+            rows, cols = (slice(h // 3, 2 * h // 3), slice(w // 3, 2 * w // 3)) if central else (slice(0, h), slice(0, w))
+            d = a[rows, cols].astype(np.float64) - b[rows, cols].astype(np.float64)
+            sse += float((d * d).sum())
+            n += d.size
+        peak = (1 << bits) - 1
+        out.append(float("inf") if sse == 0 else 10 * np.log10(peak * peak / (sse / n)))
+    return tuple(out)
+
+
 def parity_report(gpu_yuv, cpu_yuv):
     """PSNR per plane and the fraction of samples differing by more than 2 codes."""
     out = {}
