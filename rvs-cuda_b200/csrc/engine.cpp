@@ -488,10 +488,17 @@ float pixels_per_radian(const rvsb_camera& c) {
 // many small triangles per tile, and the 32x32 tiles of variant 2 (also
 // 1024-thread CTAs) rasterise it faster: 4 x 1920x1080 into 960x540 (m =
 // 0.5) 0.450 -> 0.406 ms, into 640x360 (m = 0.33) 0.521 -> 0.440 ms; at m =
-// 0.67 variant 4 is ahead again (0.452 against 0.466).
+// 0.67 variant 4 is ahead again (0.452 against 0.466).  A batch of many
+// slots has tiles enough that the last wave does not matter, and there two
+// 512-thread CTAs per SM, one working while the other waits at a barrier,
+// do better: variant 1 (64x32 tiles of two views) runs 16 poses of the
+// 1080p scene at 1806 views/s and the 64-target mixed batch at 771,
+// against 755 for variant 4.
 constexpr int kMagnifiedVariant = 7;
 constexpr int kDefaultVariant = 4;
 constexpr int kMinifiedVariant = 2;
+constexpr int kBatchVariant = 1;
+constexpr int kBatchVariantMinSlots = 8;
 static_assert(kRasterVariants[kMagnifiedVariant].med > kRasterVariants[kMagnifiedVariant].small,
               "the magnified default has the medium-triangle path");
 static_assert(kRasterVariants[kDefaultVariant].tw == 64 && kRasterVariants[kDefaultVariant].vg == 4 &&
@@ -499,6 +506,8 @@ static_assert(kRasterVariants[kDefaultVariant].tw == 64 && kRasterVariants[kDefa
               "the default holds 64x32 tiles of four views in 1024-thread CTAs");
 static_assert(kRasterVariants[kMinifiedVariant].tw == 32 && kRasterVariants[kMinifiedVariant].threads == 1024,
               "the minified default holds 32x32 tiles in 1024-thread CTAs");
+static_assert(kRasterVariants[kBatchVariant].threads == 512 && kRasterVariants[kBatchVariant].med == 0,
+              "the batch default runs two CTAs per SM");
 
 int default_variant(const SlotRequest* reqs, int n) {
     float m = 0.f;
@@ -517,7 +526,7 @@ int default_variant(const SlotRequest* reqs, int n) {
     }
     if (m > 1.1f) return kMagnifiedVariant;
     if (!erp_out && m <= 0.6f) return kMinifiedVariant;
-    return kDefaultVariant;
+    return n >= kBatchVariantMinSlots ? kBatchVariant : kDefaultVariant;
 }
 
 }  // namespace

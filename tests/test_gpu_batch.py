@@ -144,7 +144,7 @@ def test_default_raster_variant_follows_magnification(ctx):
     four views, 1024-thread CTAs), a 3x magnified one variant 7 (the
     medium-triangle path) and a perspective one minified 3x variant 2
     (32x32 tiles, 1024-thread CTAs); each gives the bytes of another
-    variant."""
+    variant.  A batch of 8 or more unmagnified views runs variant 1."""
     import torch
     wl = scenes.random_pose_small(n_views=2, w=64, h=36, seed=5)
     sc = _upload(ctx, wl)
@@ -178,6 +178,22 @@ def test_default_raster_variant_follows_magnification(ctx):
         for x, y in zip(got, _yuv(out2, cam)):
             np.testing.assert_array_equal(x, y)
     b.close()
+    # A batch of 8 unmagnified views runs variant 1 (two 512-thread CTAs
+    # per SM); its outputs are those of the single-view calls.
+    b8 = rvsb.Batch(sc, 8)
+    outs = [yuv_planes_torch(same.width, same.height) for _ in range(8)]
+    b8.synthesize([same] * 8, p, outs)
+    torch.cuda.synchronize()
+    assert b8.last_raster_variant() == 1
+    b1 = rvsb.Batch(sc, 1)
+    alone = yuv_planes_torch(same.width, same.height)
+    b1.synthesize([same], p, [alone])
+    torch.cuda.synchronize()
+    for o in outs:
+        for x, y in zip(_yuv(o, same), _yuv(alone, same)):
+            np.testing.assert_array_equal(x, y)
+    b8.close()
+    b1.close()
 
 
 @pytest.mark.parametrize("name,n,picks", [("batched_erp", 32, (0, 4, 9, 13, 18, 22, 27, 31)),
