@@ -1,5 +1,5 @@
 """Synthesis quality against ground truth, the way the reference's
-integration tests judge it (integration_test.cpp:98-154, 179-484): the
+integration tests measure it (integration_test.cpp:98-154, 179-484): the
 synthesised view is compared with a capture of the same camera by the
 two-region PSNR (whole frame, central third).  The reference's test
 content is not available; the seeded scenes stand in for it, and their
