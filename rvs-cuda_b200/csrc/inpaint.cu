@@ -334,27 +334,26 @@ __device__ __forceinline__ uint64_t ds_at(const uint64_t* DS, const Region& rg, 
 // Sweep 1 seeds of region pixel (x, y): T(q) = best of stay (D0(q), S0(q)),
 // left (D0+1, S0 of left), up (D0+1, S0 of up) with priority stay > left >
 // up; T'(q) the same without stay.  Non-holes: (0, q).  Stores both and
-// returns T(q).
-__device__ __forceinline__ uint64_t seed1_at(const uint8_t* __restrict__ holes, const uint64_t* __restrict__ DS,
-                                             uint64_t* __restrict__ Tq, uint64_t* __restrict__ Tp,
-                                             const Region& rg, int wo, int x, int y) {
-    const size_t o = (size_t)y * wo + x;
-    if (!holes[o]) {
-        const uint64_t self = pack_dxy(0, x, y);
-        Tq[o] = self;
-        Tp[o] = self;
-        return self;
+// returns T(q).  `self`, `left` and `up` are the (D0, S0) words of the
+// pixel and its neighbours (ds_at), read by the caller for a hole only.
+__device__ __forceinline__ uint64_t seed1_from(bool hole, uint64_t self, uint64_t left, uint64_t up,
+                                               uint64_t* __restrict__ Tq, uint64_t* __restrict__ Tp, int x, int y,
+                                               size_t o) {
+    if (!hole) {
+        const uint64_t own = pack_dxy(0, x, y);
+        Tq[o] = own;
+        Tp[o] = own;
+        return own;
     }
-    const uint64_t self = DS[o];
     uint64_t best = self;
     uint64_t bp = ~0ull;
     if (x > 0) {
-        const uint64_t c = ds_at(DS, rg, wo, x - 1, y) + (1ull << 32);
+        const uint64_t c = left + (1ull << 32);
         if ((c >> 32) < (best >> 32)) best = c;
         bp = c;
     }
     if (y > 0) {
-        const uint64_t c = ds_at(DS, rg, wo, x, y - 1) + (1ull << 32);
+        const uint64_t c = up + (1ull << 32);
         if ((c >> 32) < (best >> 32)) best = c;
         if (bp == ~0ull || (c >> 32) < (bp >> 32)) bp = c;
     }
@@ -391,12 +390,31 @@ __global__ void __launch_bounds__(32 * ROW_WARPS) inpaint_row1_kernel(const __gr
         const int base = (seg0 + warp) * SEG;
         unsigned long long excl[CB];
         unsigned long long local = kEmptyKey;
+        // The chunks' hole flags, then the words their seeds read, before
+        // any arithmetic: the dependent loads of the CB chunks overlap.
+        bool hole[CB];
+        uint64_t self[CB], left[CB], up[CB];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+            const int x = rg.x1 - (base + 32 * c + (31 - lane));
+            hole[c] = x >= rg.x0 && holes[(size_t)y * wo + x];
+        }
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+            const int x = rg.x1 - (base + 32 * c + (31 - lane));
+            self[c] = left[c] = up[c] = 0;
+            if (hole[c]) {
+                self[c] = DS[(size_t)y * wo + x];
+                if (x > 0) left[c] = ds_at(DS, rg, wo, x - 1, y);
+                if (y > 0) up[c] = ds_at(DS, rg, wo, x, y - 1);
+            }
+        }
 #pragma unroll
         for (int c = 0; c < CB; ++c) {
             const int x = rg.x1 - (base + 32 * c + (31 - lane));
             unsigned long long key = kEmptyKey;
             if (x >= rg.x0) {
-                const uint64_t t = seed1_at(holes, DS, Tq, Tp, rg, wo, x, y);
+                const uint64_t t = seed1_from(hole[c], self[c], left[c], up[c], Tq, Tp, x, y, (size_t)y * wo + x);
                 key = ((unsigned long long)((t >> 32) + (uint64_t)x) << 16) | (unsigned long long)x;
             }
             const unsigned long long incl = umin64(warp_incl_min_rev(key, lane), local);
